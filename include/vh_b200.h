@@ -1,0 +1,203 @@
+/*
+ * vh_b200.h -- C ABI of the B200 implementation of the cpu-vh hot path
+ * (Kurganov-Tadmor RK2 evolution of T^{tau mu}, pi^{mu nu}, Pi and the
+ * Cornelius freezeout-surface search).
+ *
+ * Plain pointers and sizes only.  Every call returns an int status (VH_OK on
+ * success).  An event handle owns its device buffers and one CUDA stream; calls
+ * on different handles may run from different host threads.  Host arrays are
+ * caller-owned.
+ *
+ * Lattice layout shared with the reference: SoA arrays over the padded grid
+ * ncx*ncy*ncz = (nx+4)(ny+4)(nz+4), index i + ncx*(j + ncy*k), two ghost
+ * cells per side (DynamicalVariables.cpp:35-41, LatticeParameters.h:13-15).
+ * "Interior" arrays are nx*ny*nz with index i + nx*(j + ny*k).
+ *
+ * Units follow the reference: lengths in fm, energy densities in fm^-4,
+ * temperatures in fm^-1, except where a name ends in _GeV.
+ */
+#ifndef VH_B200_H
+#define VH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define VH_OK              0
+#define VH_ERR_ARG         1   /* bad argument / size / null pointer                     */
+#define VH_ERR_CUDA        2   /* a CUDA runtime call failed (message: vh_last_error)     */
+#define VH_ERR_NOMEM       3   /* device allocation failed                                */
+#define VH_ERR_NAN         4   /* NaN energy density, Newton f/fp or regulation factor:   */
+                               /* the reference prints and exit(-1)s here                 */
+                               /* (EnergyMomentumTensor.cpp:42, :197-203;                 */
+                               /*  FullyDiscreteKurganovTadmorScheme.cpp:849, :854)       */
+#define VH_ERR_CORNELIUS   5   /* Cornelius edge/polygon construction error (cornelius.cpp:1250-1252, :1589-1591) */
+#define VH_ERR_CAPACITY    6   /* caller buffer too small (the count is still returned)   */
+#define VH_ERR_NODEVICE    7   /* no CUDA device / the CUDA path is not available         */
+#define VH_ERR_STATE       8   /* call out of order (e.g. step before set_initial)        */
+
+/* EoS kinds (EquationOfState.h:13-15) */
+#define VH_EOS_CONFORMAL   0   /* e = a T^4, p = e/3                                      */
+#define VH_EOS_TABLE       1   /* uniform-in-e table, EquationOfState.cpp:292-360         */
+
+/* bulk viscosity laws zeta/s(T) */
+#define VH_ZETA_REFERENCE  0   /* SourceTerms.cpp:40-48                                   */
+#define VH_ZETA_GAUSSIAN   1   /* zeta_norm * exp(-((T_GeV - zeta_T0_GeV)/zeta_width_GeV)^2) */
+
+/* arithmetic modes */
+#define VH_PREC_FP64       0   /* FP64 throughout, op-for-op with the reference (parity)  */
+#define VH_PREC_MIXED      1   /* FP32 limiter/flux/source arithmetic and FP32 storage of  */
+                               /* e, p, u; FP64 conserved accumulation and root solve      */
+
+/* field ids for vh_event_get_field / vh_event_set_field */
+#define VH_F_Q0            0   /* 0..14: ttt ttx tty ttn pitt pitx pity pitn pixx pixy pixn piyy piyn pinn Pi */
+#define VH_F_UT          100   /* 100..103: u^tau u^x u^y u^eta  */
+#define VH_F_UPT         110   /* 110..113: previous-step u (the reference's `up`) */
+#define VH_F_E           200
+#define VH_F_P           201
+
+/* columns of one freezeout element, the 20 columns of surface.dat
+ * (FreezeOut.cpp:265-270): tau x y eta  ds0 ds1 ds2 ds3  ux uy un  e T P
+ * pixx pixy pixn piyy piyn  Pi */
+#define VH_FO_COLUMNS     20
+
+typedef struct vh_config {
+    int nx, ny, nz;            /* interior lattice points (LatticeParameters.h:19-21)            */
+    double dx, dy, dz;         /* lattice spacings [fm], [fm], [1] (LatticeParameters.h:28-30)   */
+    double dt;                 /* time step [fm/c] (LatticeParameters.h:31)                      */
+    double t0;                 /* initial proper time [fm/c] (HydroParameters.h:17)              */
+    double etabar;             /* eta/s (HydroParameters.h:18)                                   */
+    double T_freezeout_GeV;    /* HydroParameters.h:19                                           */
+    double T_reg_GeV;          /* regulation temperature (HydroParameters.h:21)                  */
+    int fo_factor;             /* coarseProperTimeFOFactor (LatticeParameters.h:26)              */
+    double theta;              /* minmod limiter theta (FluxLimiter.h:13)                        */
+    int eos_kind;              /* VH_EOS_*                                                       */
+    double eos_factor;         /* a of the conformal EoS (EquationOfState.h:19)                  */
+    int bulk;                  /* 1: evolve Pi (DynamicalVariables.h:14, `PI`)                   */
+    int zeta_law;              /* VH_ZETA_*                                                      */
+    double zeta_norm, zeta_T0_GeV, zeta_width_GeV;
+    int precision;             /* VH_PREC_*                                                      */
+} vh_config;
+
+typedef struct vh_event vh_event;
+
+/* ------------------------------------------------------------- library */
+/* The reference's shipped settings: rhic-conf properties defaults plus the
+ * compile-time macros THETA 1.1, CONFORMAL_EOS, EOS_FACTOR 13.8997, PIMUNU on,
+ * PI off. */
+int vh_config_default(vh_config *cfg);
+
+/* Number of conserved components evolved for cfg (14 or 15). */
+int vh_config_nq(const vh_config *cfg);
+
+/* Last error message of the calling thread ("" if none). */
+const char *vh_last_error(void);
+
+/* 1 if a CUDA device is usable, else 0. */
+int vh_device_available(void);
+
+/* ---------------------------------------------------------- event API */
+/* Create an event on the current CUDA device.  For VH_EOS_TABLE, eos_rows holds
+ * eos_nrows rows of (e [GeV/fm^3], P [GeV/fm^3], s [fm^-3], T [GeV]) on a
+ * uniform e grid -- the record layout of EoS/hrg_hotqcd_eos_binary.dat
+ * (EquationOfState.cpp:308-324); nrows in [2, 100000]. */
+int vh_event_create(const vh_config *cfg, const double *eos_rows, int eos_nrows, vh_event **out);
+int vh_event_destroy(vh_event *ev);
+
+/* Replaces the state with an initial condition given over the interior:
+ * e, p [fm^-4]; u as 4 planes (ut, ux, uy, un); pi as 10 planes
+ * (pitt pitx pity pitn pixx pixy pixn piyy piyn pinn) or NULL for zero; Pi or
+ * NULL.  Builds T^{tau mu} (DynamicalVariables.cpp:169-218) and the ghost
+ * cells (DynamicalVariables.cpp:220-378) on the device; the previous-step
+ * velocity is set equal to u.  Resets the step counter to 0 and t to t0. */
+int vh_event_set_initial(vh_event *ev, const double *e, const double *p, const double *u,
+                         const double *pi, const double *Pi);
+
+/* Same, from device pointers (already resident in HBM). */
+int vh_event_set_initial_device(vh_event *ev, const double *d_e, const double *d_p, const double *d_u,
+                                const double *d_pi, const double *d_Pi);
+
+/* Advance nsteps RK2 steps (rungeKutta2 + q<->Q swap + t = t0 + n dt,
+ * FullyDiscreteKurganovTadmorScheme.cpp:867-924, HydroPlugin.cpp:292-307).
+ * Asynchronous on the event's stream; errors detected on the device are
+ * reported by vh_event_status or by the next synchronising call. */
+int vh_event_step(vh_event *ev, int nsteps);
+
+/* Wait for the event's stream; returns VH_ERR_NAN etc. if the device flagged
+ * an error, with the step and cell index in *err_step, *err_cell (nullable). */
+int vh_event_status(vh_event *ev, int *err_step, long long *err_cell);
+
+/* Completed steps and current proper time. */
+int vh_event_progress(vh_event *ev, int *steps_done, double *t);
+
+/* Copy one padded field (ncx*ncy*ncz doubles) to host memory. */
+int vh_event_get_field(vh_event *ev, int field, double *host_out);
+
+/* One freezeout block of the driver loop (HydroPlugin.cpp:242-266) at loop
+ * index n = steps_done + 1: shift the coarse time slabs, find the surface
+ * elements of every (hyper)cube between the previous and the current slab
+ * (callFOFinder2p1D / callFOFinder3p1D, FreezeOut.cpp:200-361) and count the
+ * interior cells above the freezeout energy density (FreezeOut.cpp:364-381).
+ * The elements stay on the device; *n_elements (nullable) and *n_above
+ * (nullable) are written.  Order of elements: ix, iy, iz, element index --
+ * the order in which the reference writes them. */
+int vh_event_freezeout(vh_event *ev, int *n_elements, int *n_above);
+
+/* Copy the elements of the last freezeout block to host memory, VH_FO_COLUMNS
+ * doubles per element.  Returns VH_ERR_CAPACITY if cap_elements is too small. */
+int vh_event_fetch_surface(vh_event *ev, double *host_out, int cap_elements, int *n_elements);
+
+/* The CUDA stream (cudaStream_t) the event's work is queued on. */
+int vh_event_stream(vh_event *ev, void **stream);
+
+/* Device pointer of a padded field (for zero-copy inspection / timing). */
+int vh_event_device_field(vh_event *ev, int field, double **d_ptr);
+
+/* Energy density [fm^-4] for temperature T [fm^-1] with the event's EoS
+ * (EquationOfState.cpp:201-290); used for e_F and e_reg. */
+int vh_event_energy_of_T(vh_event *ev, double T, double *e_out);
+
+/* ------------------------------------------------ host-side helpers */
+/* Synthetic crossover EoS table in the binary record layout above:
+ * cs^2(T) = 1/3 - dip * exp(-((T - Tc)/w)^2) integrated from T_lo_GeV,
+ * tabulated on nrows points uniform in e from e(T_lo) to e_max_GeV. */
+int vh_eos_synthetic_table(int nrows, double T_lo_GeV, double e_max_GeV, double a_conformal,
+                           double dip, double Tc_GeV, double w_GeV, double *rows);
+
+/* Host copy of the reference EoS functions for a given configuration and
+ * table (EquationOfState.cpp:44-290). what: 0 p(e), 1 cs2(e), 2 T(e), 3 e(T). */
+double vh_eos_eval(const vh_config *cfg, const double *eos_rows, int eos_nrows, int what, double x);
+
+/* Viscous Gubser flow at proper time t0 (2+1D, nz = 1): e, p [fm^-4],
+ * u (4 planes), pi (10 planes, Navier-Stokes value 2 eta sigma^{mu nu}).
+ * T0_GeV is the temperature at the origin, q the Gubser scale [fm^-1]. */
+int vh_ic_gubser(const vh_config *cfg, double q, double T0_GeV,
+                 double *e, double *p, double *u, double *pi);
+
+/* Optical-Glauber event: e = e0 * n_part(x,y)/max n_part * L(eta) + 1e-3
+ * (the reference adds 1e-3 fm^-4, InitialConditions.cpp:1093), Woods-Saxon
+ * (R, a, n0 = 0.17 fm^-3), sigma_NN [fm^2], impact parameter b [fm];
+ * L(eta) = plateau |eta| < eta_flat/2 with Gaussian tails of width eta_sigma
+ * (InitialConditions.cpp:1046-1063).  u at rest, pi = Pi = 0. */
+int vh_ic_glauber(const vh_config *cfg, const double *eos_rows, int eos_nrows,
+                  double R, double a, double sigma_nn, double b, double e0_GeV,
+                  double eta_flat, double eta_sigma,
+                  double *e, double *p, double *u);
+
+/* Lumpy 2+1D event: sum of Gaussian hotspots (width w [fm]); the number is
+ * Poisson(mean_spots), amplitudes Gamma(k_gamma) scaled so their mean is
+ * amp_mean_GeV, centres drawn from the b = 0 Woods-Saxon overlap density;
+ * all draws come from a counter-based generator keyed by `seed`. */
+int vh_ic_hotspots(const vh_config *cfg, const double *eos_rows, int eos_nrows,
+                   uint64_t seed, double mean_spots, double w, double k_gamma, double amp_mean_GeV,
+                   double R, double a, double *e, double *p, double *u);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VH_B200_H */

@@ -1,0 +1,46 @@
+# ref.mk -- TEST INFRASTRUCTURE ONLY: builds the reference's own hot path.
+#
+# Compiles the unmodified cpu-vh sources where they lie (REF, read-only) into
+# shared libraries under oracle/_ref/, together with oracle/ref_harness.cpp.
+# Nothing is copied out of REF.  The physics macros that the reference fixes
+# inside its headers are overridden by force-including oracle/ref_shim.h.
+#
+#   make -f oracle/ref.mk                 # all variants
+#   make -f oracle/ref.mk REF=/path/to/cpu-vh
+#
+# Variants (one library each, since the reference keeps its state in globals):
+#   conf  : conformal EoS a=15.6269, theta=1.8, shear only  (Gubser 2+1D workload)
+#   table : tabulated EoS, theta=1.8, shear + bulk (-DPI)   (Glauber 3+1D workload)
+#   stock : the shipped macros (conformal a=13.8997, theta=1.1, shear only)
+#
+# Flags: the shipped ones (CMakeLists.txt:14, -O3 -fopenmp -std=c++11) with
+# -ffp-contract=off so the arithmetic is the literal IEEE program of the source
+# (GCC would otherwise fuse multiply-adds of its own choosing), and a portable
+# x86-64-v3 target instead of -march=native so the binary runs on any AVX2 host.
+REF ?= /root/reference
+OUT ?= oracle/_ref
+HOSTCXX ?= g++
+CXXFLAGS_BASE = -O3 -fopenmp -std=c++11 -march=x86-64-v3 -ffp-contract=off -fPIC -w \
+                -I$(REF)/rhic/include -I$(REF)/freezeout -include oracle/ref_shim.h
+LDFLAGS = -shared -fopenmp -Wl,-Bsymbolic
+
+SRC_NAMES = DynamicalVariables EnergyMomentumTensor EquationOfState FileIO FluxFunctions \
+            FluxLimiter FullyDiscreteKurganovTadmorScheme HalfSiteExtrapolation HydroPlugin \
+            LocalPropagationSpeed SemiDiscreteKurganovTadmorScheme SourceTerms SpectralRadius \
+            Vorticity FiniteDifference
+SRCS = $(addprefix $(REF)/rhic/src/,$(addsuffix .cpp,$(SRC_NAMES))) oracle/ref_harness.cpp
+
+DEFS_conf  = -DVH_THETA=1.8 -DVH_EOS_FACTOR=15.6269
+DEFS_table = -DVH_THETA=1.8 -DVH_EOS_FACTOR=15.6269 -DVH_EOS_TABLE -DPI
+DEFS_stock = -DVH_THETA=1.1 -DVH_EOS_FACTOR=13.8997
+
+all: $(OUT)/libvhref_conf.so $(OUT)/libvhref_table.so $(OUT)/libvhref_stock.so
+
+$(OUT)/libvhref_%.so: $(SRCS) oracle/ref_shim.h oracle/ref.mk
+	@mkdir -p $(OUT)
+	$(HOSTCXX) $(CXXFLAGS_BASE) $(DEFS_$*) $(SRCS) $(LDFLAGS) -o $@
+
+clean:
+	rm -f $(OUT)/libvhref_*.so
+
+.PHONY: all clean
