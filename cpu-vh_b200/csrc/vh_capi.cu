@@ -1,0 +1,451 @@
+/*
+ * vh_capi.cu -- the C ABI event implementation (include/vh_b200.h).
+ *
+ * An event owns one device allocation holding every plane of its state:
+ *   q[3]  : NQ planes each -- current q, next Q, stage qS
+ *           (the reference's q, Q, qS, DynamicalVariables.cpp:21)
+ *   ep[2] : (e, p) twice -- read by one stage, written by the other
+ *   u[3]  : 4 planes each -- u, up, uS (DynamicalVariables.cpp:23)
+ * Planes are padded to a multiple of 32 doubles so every plane starts on a
+ * 256-byte boundary.  One RK2 step is two launches of the fused stage kernel;
+ * buffer roles rotate by index on the host, exactly as the reference swaps
+ * pointers (setCurrentConservedVariables, swapFluidVelocity).
+ */
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "vh_b200.h"
+#include "vh_internal.h"
+#include "vh_kernels.h"
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+#define CUDA_TRY(x)                                                                                   \
+    do {                                                                                              \
+        cudaError_t e__ = (x);                                                                        \
+        if (e__ != cudaSuccess) return fail(e__ == cudaErrorMemoryAllocation ? VH_ERR_NOMEM : VH_ERR_CUDA, \
+                                            std::string(#x) + ": " + cudaGetErrorString(e__));        \
+    } while (0)
+
+namespace {
+
+/* host-exact powf table, uploaded once per device */
+struct DevPowf {
+    unsigned *keys = nullptr;
+    float *vals = nullptr;
+    unsigned *bucket = nullptr;
+    unsigned hb0 = 0, hb1 = 0;
+};
+std::mutex g_powf_mu;
+std::map<int, DevPowf> g_powf;
+
+int device_powf(int dev, DevPowf *out)
+{
+    std::lock_guard<std::mutex> lk(g_powf_mu);
+    auto it = g_powf.find(dev);
+    if (it != g_powf.end()) { *out = it->second; return VH_OK; }
+    const vh::PowfQuarterTable &T = vh::powf_quarter_table();
+    DevPowf d;
+    unsigned lob, hib;
+    std::memcpy(&lob, &T.lo, 4);
+    std::memcpy(&hib, &T.hi, 4);
+    d.hb0 = lob >> 16;
+    d.hb1 = hib >> 16;
+    size_t nk = std::max<size_t>(T.keys.size(), 1);
+    CUDA_TRY(cudaMalloc(&d.keys, nk * sizeof(unsigned)));
+    CUDA_TRY(cudaMalloc(&d.vals, nk * sizeof(float)));
+    CUDA_TRY(cudaMalloc(&d.bucket, T.bucket.size() * sizeof(unsigned)));
+    if (!T.keys.empty()) {
+        CUDA_TRY(cudaMemcpy(d.keys, T.keys.data(), T.keys.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+        CUDA_TRY(cudaMemcpy(d.vals, T.vals.data(), T.vals.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    CUDA_TRY(cudaMemcpy(d.bucket, T.bucket.data(), T.bucket.size() * sizeof(unsigned), cudaMemcpyHostToDevice));
+    g_powf[dev] = d;
+    *out = d;
+    return VH_OK;
+}
+
+} // namespace
+
+struct vh_event {
+    vh_config cfg;
+    int nq = 14;
+    int ncx = 0, ncy = 0, ncz = 0;
+    long long L = 0;          /* plane stride (padded) */
+    long long N = 0;          /* interior cells */
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    double *slab = nullptr;
+    double *q[3] = {nullptr, nullptr, nullptr};
+    double *ep[2] = {nullptr, nullptr};   /* e plane; p plane follows at +L */
+    double *u[3] = {nullptr, nullptr, nullptr};
+    int qc = 0, qn = 1, qs = 2;          /* current q, next Q, stage qS */
+    int ec = 0;                           /* e/p buffer holding the current state */
+    int uc = 0, up = 1, us = 2;           /* u, up, uS */
+    double *tables = nullptr;             /* p_tb then T_tb */
+    int *err = nullptr;                   /* [0] code, [1] step */
+    long long *err_cell = nullptr;
+    unsigned long long *powf_miss = nullptr;
+    double *ic = nullptr;                 /* interior staging: e, p, u(4), pi(10), Pi */
+    vh::HostEos heos;
+    DevPowf powf;
+    double e_reg = 0, e_fo = 0;
+    int n = 0;
+    double t = 0;
+    bool initialised = false;
+    /* freezeout */
+    double *fo_slabs = nullptr;           /* 2 x 11 x N */
+    int fo_prev = 0;                      /* which half is the previous slab */
+    int *fo_scratch = nullptr;
+    size_t fo_scratch_ints = 0;
+    double *fo_elems = nullptr;
+    int fo_cap = 0;
+    int fo_count = 0;
+};
+
+static vh::DevEos dev_eos(const vh_event *ev)
+{
+    vh::DevEos E;
+    E.kind = ev->cfg.eos_kind;
+    E.a = ev->cfg.eos_factor;
+    E.p_tb = ev->tables;
+    E.T_tb = ev->tables ? ev->tables + ev->heos.e_length : nullptr;
+    E.e_length = ev->heos.e_length;
+    E.e_min = ev->heos.e_min;
+    E.e_spacing = ev->heos.e_spacing;
+    E.pq.keys = ev->powf.keys;
+    E.pq.vals = ev->powf.vals;
+    E.pq.bucket = ev->powf.bucket;
+    E.pq.hb0 = ev->powf.hb0;
+    E.pq.hb1 = ev->powf.hb1;
+    E.pq.miss = ev->powf_miss;
+    return E;
+}
+
+extern "C" {
+
+const char *vh_last_error(void) { return g_err.c_str(); }
+
+int vh_device_available(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return n > 0 ? 1 : 0;
+}
+
+int vh_event_destroy(vh_event *ev)
+{
+    if (!ev) return VH_OK;
+    if (ev->stream) cudaStreamSynchronize(ev->stream);
+    cudaFree(ev->slab);
+    cudaFree(ev->tables);
+    cudaFree(ev->err);
+    cudaFree(ev->err_cell);
+    cudaFree(ev->powf_miss);
+    cudaFree(ev->ic);
+    cudaFree(ev->fo_slabs);
+    cudaFree(ev->fo_scratch);
+    cudaFree(ev->fo_elems);
+    if (ev->stream) cudaStreamDestroy(ev->stream);
+    delete ev;
+    return VH_OK;
+}
+
+int vh_event_create(const vh_config *cfg, const double *eos_rows, int eos_nrows, vh_event **out)
+{
+    if (!cfg || !out) return fail(VH_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (cfg->nx < 2 || cfg->ny < 2 || cfg->nz < 1) return fail(VH_ERR_ARG, "lattice must be at least 2x2x1");
+    if (!(cfg->dx > 0 && cfg->dy > 0 && cfg->dz > 0 && cfg->dt > 0 && cfg->t0 > 0))
+        return fail(VH_ERR_ARG, "spacings and t0 must be positive");
+    if (cfg->eos_kind == VH_EOS_TABLE && (!eos_rows || eos_nrows < 2 || eos_nrows > 100000))
+        return fail(VH_ERR_ARG, "tabulated EoS needs 2..100000 rows");
+    if (cfg->precision != VH_PREC_FP64) return fail(VH_ERR_ARG, "only VH_PREC_FP64 is available on this build path");
+    if (!vh_device_available()) return fail(VH_ERR_NODEVICE, "no CUDA device");
+    vh_event *ev = new vh_event();
+    ev->cfg = *cfg;
+    ev->nq = cfg->bulk ? 15 : 14;
+    ev->ncx = cfg->nx + 4; ev->ncy = cfg->ny + 4; ev->ncz = cfg->nz + 4;
+    long long len = (long long)ev->ncx * ev->ncy * ev->ncz;
+    ev->L = (len + 31) / 32 * 32;
+    ev->N = (long long)cfg->nx * cfg->ny * cfg->nz;
+    ev->heos.init(*cfg, eos_rows, eos_nrows);
+    ev->e_reg = ev->heos.energy_of_T(cfg->T_reg_GeV / vh::kHbarc);
+    ev->e_fo = ev->heos.energy_of_T(cfg->T_freezeout_GeV / vh::kHbarc);
+    int rc;
+#define TRY(x) do { cudaError_t e__ = (x); if (e__ != cudaSuccess) { rc = fail(e__ == cudaErrorMemoryAllocation ? VH_ERR_NOMEM : VH_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e__)); vh_event_destroy(ev); return rc; } } while (0)
+    TRY(cudaGetDevice(&ev->device));
+    TRY(cudaStreamCreateWithFlags(&ev->stream, cudaStreamNonBlocking));
+    const long long planes = 3LL * ev->nq + 2 * 2 + 3 * 4;
+    TRY(cudaMalloc(&ev->slab, (size_t)(planes * ev->L) * sizeof(double)));
+    TRY(cudaMemsetAsync(ev->slab, 0, (size_t)(planes * ev->L) * sizeof(double), ev->stream));
+    double *p = ev->slab;
+    for (int b = 0; b < 3; ++b) { ev->q[b] = p; p += ev->nq * ev->L; }
+    for (int b = 0; b < 2; ++b) { ev->ep[b] = p; p += 2 * ev->L; }
+    for (int b = 0; b < 3; ++b) { ev->u[b] = p; p += 4 * ev->L; }
+    if (cfg->eos_kind == VH_EOS_TABLE) {
+        TRY(cudaMalloc(&ev->tables, 2 * (size_t)eos_nrows * sizeof(double)));
+        TRY(cudaMemcpyAsync(ev->tables, ev->heos.p_tb.data(), eos_nrows * sizeof(double), cudaMemcpyHostToDevice, ev->stream));
+        TRY(cudaMemcpyAsync(ev->tables + eos_nrows, ev->heos.T_tb.data(), eos_nrows * sizeof(double), cudaMemcpyHostToDevice, ev->stream));
+    } else {
+        rc = device_powf(ev->device, &ev->powf);
+        if (rc != VH_OK) { vh_event_destroy(ev); return rc; }
+    }
+    TRY(cudaMalloc(&ev->err, 2 * sizeof(int)));
+    TRY(cudaMalloc(&ev->err_cell, sizeof(long long)));
+    TRY(cudaMalloc(&ev->powf_miss, sizeof(unsigned long long)));
+    TRY(cudaMemsetAsync(ev->err, 0, 2 * sizeof(int), ev->stream));
+    TRY(cudaMemsetAsync(ev->err_cell, 0, sizeof(long long), ev->stream));
+    TRY(cudaMemsetAsync(ev->powf_miss, 0, sizeof(unsigned long long), ev->stream));
+    TRY(cudaMalloc(&ev->ic, (size_t)(17 * ev->N) * sizeof(double)));
+    TRY(cudaStreamSynchronize(ev->stream));
+#undef TRY
+    *out = ev;
+    return VH_OK;
+}
+
+static int do_init(vh_event *ev, const double *d_e, const double *d_p, const double *d_u, const double *d_pi, const double *d_Pi)
+{
+    vh::InitArgs a;
+    a.e = d_e; a.p = d_p; a.u = d_u; a.pi = d_pi; a.Pi = d_Pi;
+    ev->qc = 0; ev->qn = 1; ev->qs = 2; ev->ec = 0; ev->uc = 0; ev->up = 1; ev->us = 2;
+    a.q = ev->q[ev->qc];
+    a.eo = ev->ep[ev->ec];
+    a.po = ev->ep[ev->ec] + ev->L;
+    a.uo = ev->u[ev->uc];
+    a.upo = ev->u[ev->up];
+    a.L = ev->L;
+    a.nx = ev->cfg.nx; a.ny = ev->cfg.ny; a.nz = ev->cfg.nz;
+    a.ncx = ev->ncx; a.ncy = ev->ncy; a.nq = ev->nq;
+    vh::launch_init(a, ev->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemsetAsync(ev->err, 0, 2 * sizeof(int), ev->stream));
+    CUDA_TRY(cudaMemsetAsync(ev->err_cell, 0, sizeof(long long), ev->stream));
+    if (ev->fo_slabs) CUDA_TRY(cudaMemsetAsync(ev->fo_slabs, 0, (size_t)(2 * 11 * ev->N) * sizeof(double), ev->stream));
+    ev->fo_prev = 0;
+    ev->fo_count = 0;
+    ev->n = 0;
+    ev->t = ev->cfg.t0;
+    ev->initialised = true;
+    return VH_OK;
+}
+
+int vh_event_set_initial(vh_event *ev, const double *e, const double *p, const double *u, const double *pi, const double *Pi)
+{
+    if (!ev || !e || !p || !u) return fail(VH_ERR_ARG, "null argument");
+    const size_t N = (size_t)ev->N, B = N * sizeof(double);
+    double *d = ev->ic;
+    CUDA_TRY(cudaMemcpyAsync(d, e, B, cudaMemcpyHostToDevice, ev->stream));
+    CUDA_TRY(cudaMemcpyAsync(d + N, p, B, cudaMemcpyHostToDevice, ev->stream));
+    CUDA_TRY(cudaMemcpyAsync(d + 2 * N, u, 4 * B, cudaMemcpyHostToDevice, ev->stream));
+    if (pi) CUDA_TRY(cudaMemcpyAsync(d + 6 * N, pi, 10 * B, cudaMemcpyHostToDevice, ev->stream));
+    if (Pi) CUDA_TRY(cudaMemcpyAsync(d + 16 * N, Pi, B, cudaMemcpyHostToDevice, ev->stream));
+    return do_init(ev, d, d + N, d + 2 * N, pi ? d + 6 * N : nullptr, Pi ? d + 16 * N : nullptr);
+}
+
+int vh_event_set_initial_device(vh_event *ev, const double *d_e, const double *d_p, const double *d_u, const double *d_pi, const double *d_Pi)
+{
+    if (!ev || !d_e || !d_p || !d_u) return fail(VH_ERR_ARG, "null argument");
+    return do_init(ev, d_e, d_p, d_u, d_pi, d_Pi);
+}
+
+int vh_event_step(vh_event *ev, int nsteps)
+{
+    if (!ev || nsteps < 0) return fail(VH_ERR_ARG, "bad argument");
+    if (!ev->initialised) return fail(VH_ERR_STATE, "vh_event_step before vh_event_set_initial");
+    const vh_config &c = ev->cfg;
+    vh::StageArgs A;
+    A.L = ev->L;
+    A.nx = c.nx; A.ny = c.ny; A.nz = c.nz; A.ncx = ev->ncx; A.ncy = ev->ncy;
+    A.dt = c.dt; A.dx = c.dx; A.dy = c.dy; A.dz = c.dz; A.theta = c.theta; A.etabar = c.etabar;
+    A.e_reg = ev->e_reg;
+    A.eos = dev_eos(ev);
+    A.zeta.law = c.zeta_law; A.zeta.norm = c.zeta_norm; A.zeta.T0 = c.zeta_T0_GeV; A.zeta.w = c.zeta_width_GeV;
+    A.err.code = ev->err; A.err.step = ev->err + 1; A.err.cell = ev->err_cell;
+    for (int it = 0; it < nsteps; ++it) {
+        const double t = ev->t;
+        const double t1 = t + c.dt;           /* `t += dt` of rungeKutta2 */
+        A.step = ev->n;
+        /* stage 1: q -> qS, (e,p)[ec] -> (e,p)[1-ec], u/up -> uS */
+        A.qin = ev->q[ev->qc]; A.qout = ev->q[ev->qs]; A.qbase = nullptr;
+        A.ein = ev->ep[ev->ec]; A.pin = ev->ep[ev->ec] + ev->L;
+        A.eout = ev->ep[1 - ev->ec]; A.pout = ev->ep[1 - ev->ec] + ev->L;
+        A.uin = ev->u[ev->uc]; A.upin = ev->u[ev->up]; A.uout = ev->u[ev->us];
+        A.t = t; A.t2pow = pow(t, 2); A.t_inf = t1;
+        vh::launch_stage(A, ev->nq, c.eos_kind, ev->stream);
+        /* stage 2: qS -> Q, convex with q; u(new) goes to the old up buffer */
+        A.qin = ev->q[ev->qs]; A.qout = ev->q[ev->qn]; A.qbase = ev->q[ev->qc];
+        A.ein = ev->ep[1 - ev->ec]; A.pin = ev->ep[1 - ev->ec] + ev->L;
+        A.eout = ev->ep[ev->ec]; A.pout = ev->ep[ev->ec] + ev->L;
+        A.uin = ev->u[ev->us]; A.upin = ev->u[ev->uc]; A.uout = ev->u[ev->up];
+        A.t = t1; A.t2pow = pow(t1, 2); A.t_inf = t1;
+        vh::launch_stage(A, ev->nq, c.eos_kind, ev->stream);
+        std::swap(ev->qc, ev->qn);
+        std::swap(ev->uc, ev->up);
+        ev->n += 1;
+        ev->t = c.t0 + ev->n * c.dt;
+    }
+    CUDA_TRY(cudaGetLastError());
+    return VH_OK;
+}
+
+int vh_event_status(vh_event *ev, int *err_step, long long *err_cell)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    CUDA_TRY(cudaStreamSynchronize(ev->stream));
+    int h[2];
+    long long cell;
+    CUDA_TRY(cudaMemcpy(h, ev->err, sizeof(h), cudaMemcpyDeviceToHost));
+    CUDA_TRY(cudaMemcpy(&cell, ev->err_cell, sizeof(cell), cudaMemcpyDeviceToHost));
+    if (err_step) *err_step = h[1];
+    if (err_cell) *err_cell = cell;
+    if (h[0] != 0) {
+        char buf[160];
+        std::snprintf(buf, sizeof buf, "device error %d at step %d, cell %lld", h[0], h[1], cell);
+        return fail(h[0], buf);
+    }
+    return VH_OK;
+}
+
+int vh_event_progress(vh_event *ev, int *steps_done, double *t)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    if (steps_done) *steps_done = ev->n;
+    if (t) *t = ev->t;
+    return VH_OK;
+}
+
+static const double *field_ptr(const vh_event *ev, int field)
+{
+    if (field >= 0 && field < ev->nq) return ev->q[ev->qc] + (long long)field * ev->L;
+    if (field >= VH_F_UT && field < VH_F_UT + 4) return ev->u[ev->uc] + (long long)(field - VH_F_UT) * ev->L;
+    if (field >= VH_F_UPT && field < VH_F_UPT + 4) return ev->u[ev->up] + (long long)(field - VH_F_UPT) * ev->L;
+    if (field == VH_F_E) return ev->ep[ev->ec];
+    if (field == VH_F_P) return ev->ep[ev->ec] + ev->L;
+    return nullptr;
+}
+
+int vh_event_get_field(vh_event *ev, int field, double *host_out)
+{
+    if (!ev || !host_out) return fail(VH_ERR_ARG, "null argument");
+    const double *src = field_ptr(ev, field);
+    if (!src) return fail(VH_ERR_ARG, "unknown field id");
+    size_t len = (size_t)ev->ncx * ev->ncy * ev->ncz;
+    CUDA_TRY(cudaMemcpyAsync(host_out, src, len * sizeof(double), cudaMemcpyDeviceToHost, ev->stream));
+    CUDA_TRY(cudaStreamSynchronize(ev->stream));
+    return VH_OK;
+}
+
+int vh_event_device_field(vh_event *ev, int field, double **d_ptr)
+{
+    if (!ev || !d_ptr) return fail(VH_ERR_ARG, "null argument");
+    const double *src = field_ptr(ev, field);
+    if (!src) return fail(VH_ERR_ARG, "unknown field id");
+    *d_ptr = const_cast<double *>(src);
+    return VH_OK;
+}
+
+int vh_event_stream(vh_event *ev, void **stream)
+{
+    if (!ev || !stream) return fail(VH_ERR_ARG, "null argument");
+    *stream = (void *)ev->stream;
+    return VH_OK;
+}
+
+int vh_event_energy_of_T(vh_event *ev, double T, double *e_out)
+{
+    if (!ev || !e_out) return fail(VH_ERR_ARG, "null argument");
+    *e_out = ev->heos.energy_of_T(T);
+    return VH_OK;
+}
+
+/* powf calibration diagnostics: inputs seen outside the calibrated range */
+int vh_event_powf_misses(vh_event *ev, unsigned long long *misses)
+{
+    if (!ev || !misses) return fail(VH_ERR_ARG, "null argument");
+    CUDA_TRY(cudaMemcpy(misses, ev->powf_miss, sizeof(*misses), cudaMemcpyDeviceToHost));
+    return VH_OK;
+}
+
+/* ------------------------------------------------------------ freezeout */
+int vh_event_freezeout(vh_event *ev, int *n_elements, int *n_above)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    if (!ev->initialised) return fail(VH_ERR_STATE, "freezeout before vh_event_set_initial");
+    const vh_config &c = ev->cfg;
+    const size_t N = (size_t)ev->N;
+    if (!ev->fo_slabs) {
+        CUDA_TRY(cudaMalloc(&ev->fo_slabs, 2 * 11 * N * sizeof(double)));
+        CUDA_TRY(cudaMemsetAsync(ev->fo_slabs, 0, 2 * 11 * N * sizeof(double), ev->stream));
+        ev->fo_scratch_ints = vh::freezeout_scratch_ints(c.nx, c.ny, c.nz);
+        CUDA_TRY(cudaMalloc(&ev->fo_scratch, ev->fo_scratch_ints * sizeof(int)));
+    }
+    vh::FoArgs a;
+    a.q = ev->q[ev->qc]; a.e = ev->ep[ev->ec]; a.u = ev->u[ev->uc];
+    a.L = ev->L; a.nx = c.nx; a.ny = c.ny; a.nz = c.nz; a.ncx = ev->ncx; a.ncy = ev->ncy; a.nq = ev->nq;
+    a.slab_prev = ev->fo_slabs + (size_t)ev->fo_prev * 11 * N;
+    a.slab_cur = ev->fo_slabs + (size_t)(1 - ev->fo_prev) * 11 * N;
+    a.eF = ev->e_fo;
+    a.dtau_c = c.dt * c.fo_factor; a.dx = c.dx; a.dy = c.dy; a.dz = c.dz;
+    a.t0 = c.t0; a.dt = c.dt; a.t = ev->t; a.n = ev->n + 1;
+    a.eos = dev_eos(ev);
+    a.err.code = ev->err; a.err.step = ev->err + 1; a.err.cell = ev->err_cell;
+    /* scratch: [counts: ncubes+1][block sums][n_above][n_total] */
+    a.counts = ev->fo_scratch;
+    a.block_sums = nullptr;
+    a.n_above = nullptr;
+    a.n_total = nullptr;
+    a.elems = ev->fo_elems;
+    a.cap = ev->fo_cap;
+    /* first pass: counts and the total; grows the element buffer if needed */
+    int total = 0, above = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        a.elems = ev->fo_elems;
+        a.cap = ev->fo_cap;
+        vh::launch_freezeout(a, ev->stream);
+        CUDA_TRY(cudaGetLastError());
+        int hdr[2];
+        size_t sc = ev->fo_scratch_ints;
+        CUDA_TRY(cudaMemcpyAsync(hdr, ev->fo_scratch + sc - 2, sizeof(hdr), cudaMemcpyDeviceToHost, ev->stream));
+        CUDA_TRY(cudaStreamSynchronize(ev->stream));
+        above = hdr[0];
+        total = hdr[1];
+        if (total <= ev->fo_cap) break;
+        /* not enough room: re-run with a larger buffer from the same slabs */
+        cudaFree(ev->fo_elems);
+        ev->fo_cap = total + total / 4 + 1024;
+        CUDA_TRY(cudaMalloc(&ev->fo_elems, (size_t)ev->fo_cap * VH_FO_COLUMNS * sizeof(double)));
+        a.slab_prev = ev->fo_slabs + (size_t)ev->fo_prev * 11 * N;   /* unchanged: the shift is idempotent */
+    }
+    ev->fo_prev = 1 - ev->fo_prev;
+    ev->fo_count = total;
+    if (n_elements) *n_elements = total;
+    if (n_above) *n_above = above;
+    return VH_OK;
+}
+
+int vh_event_fetch_surface(vh_event *ev, double *host_out, int cap_elements, int *n_elements)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    if (n_elements) *n_elements = ev->fo_count;
+    if (ev->fo_count > cap_elements) return fail(VH_ERR_CAPACITY, "surface buffer too small");
+    if (ev->fo_count == 0) return VH_OK;
+    if (!host_out) return fail(VH_ERR_ARG, "null output");
+    CUDA_TRY(cudaMemcpyAsync(host_out, ev->fo_elems, (size_t)ev->fo_count * VH_FO_COLUMNS * sizeof(double),
+                             cudaMemcpyDeviceToHost, ev->stream));
+    CUDA_TRY(cudaStreamSynchronize(ev->stream));
+    return VH_OK;
+}
+
+} /* extern "C" */

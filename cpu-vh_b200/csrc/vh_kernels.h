@@ -1,0 +1,79 @@
+/*
+ * vh_kernels.h -- launch interface between the C ABI (vh_capi.cu) and the
+ * kernels (vh_kt.cu, vh_fo.cu).  Internal to the library.
+ */
+#ifndef VH_KERNELS_H
+#define VH_KERNELS_H
+
+#include <cuda_runtime.h>
+#include "vh_physics.cuh"
+
+namespace vh {
+
+/* Arguments of one fused RK stage (FullyDiscreteKurganovTadmorScheme.cpp:895-906
+ * for stage 1, :912-923 for stage 2). */
+struct StageArgs {
+    const double *qin;     /* conserved variables the stage differentiates (NQ planes) */
+    double *qout;          /* updated conserved variables (NQ planes)                  */
+    const double *qbase;   /* stage 2: q^n for the convex combination; stage 1: null   */
+    const double *ein, *pin;
+    double *eout, *pout;
+    const double *uin;     /* 4 planes, read on the 7-point stencil                    */
+    const double *upin;    /* 4 planes, previous velocity, read at the centre          */
+    double *uout;          /* 4 planes                                                 */
+    long long L;           /* plane stride in doubles                                  */
+    int nx, ny, nz, ncx, ncy;
+    double t;              /* time the stage's fluxes and sources are evaluated at     */
+    double t2pow;          /* pow(t, 2) from the host libm (SourceTerms.cpp:415, :587) */
+    double t_inf;          /* time of the inference and regulation (t after t += dt)   */
+    double dt, dx, dy, dz, theta, etabar, e_reg;
+    int step;              /* step index for error reports                             */
+    DevEos eos;
+    Zeta zeta;
+    DevErr err;
+};
+
+/* Interior initial condition -> padded state (DynamicalVariables.cpp:169-218
+ * and the ghost faces). */
+struct InitArgs {
+    const double *e, *p, *u, *pi, *Pi;   /* interior planes, u: 4, pi: 10 (pi, Pi nullable) */
+    double *q, *eo, *po, *uo, *upo;      /* padded planes */
+    long long L;
+    int nx, ny, nz, ncx, ncy, nq;
+};
+
+void launch_init(const InitArgs &a, cudaStream_t s);
+void launch_stage(const StageArgs &a, int nq, int eos_kind, cudaStream_t s);
+
+/* ---- freezeout ---- */
+struct FoArgs {
+    /* current state (padded) */
+    const double *q;         /* NQ planes */
+    const double *e;
+    const double *u;         /* 4 planes */
+    long long L;
+    int nx, ny, nz, ncx, ncy, nq;
+    /* coarse slabs, interior layout i + nx*(j + ny*k): [2][11][N] = e, ux, uy, un, e, pixx, pixy, pixn, piyy, piyn, Pi */
+    double *slab_prev, *slab_cur;
+    double eF;
+    double dtau_c, dx, dy, dz;   /* lattice_spacing of HydroPlugin.cpp:137-152 */
+    double t0, dt, t;            /* cell_tau = t0 + n dt, normals scaled by t (FreezeOut.cpp:228, :243) */
+    int n;                       /* loop index of the freezeout block */
+    DevEos eos;
+    DevErr err;
+    int *counts;                 /* per (hyper)cube element counts, then offsets */
+    int *block_sums;
+    int *n_above;                /* cells above eF */
+    double *elems;               /* output, VH_FO_COLUMNS per element */
+    int cap;                     /* capacity of elems in elements */
+    int *n_total;
+};
+
+/* Runs the whole freezeout block; returns the number of elements through
+ * *a.n_total (device) and leaves elements in a.elems. */
+void launch_freezeout(const FoArgs &a, cudaStream_t s);
+size_t freezeout_scratch_ints(int nx, int ny, int nz);
+
+} // namespace vh
+
+#endif

@@ -1,0 +1,346 @@
+/*
+ * vh_kt.cu -- the Kurganov-Tadmor RK2 stage as one fused sm_100a kernel.
+ *
+ * The reference runs each RK stage as seven OpenMP loop nests over the lattice
+ * (source, x, y, eta flux passes, inference, regulation, ghost cells;
+ * FullyDiscreteKurganovTadmorScheme.cpp:895-923), each re-reading and
+ * re-writing the full state.  Here one thread owns one interior cell for the
+ * whole stage: it evaluates the source term, the six half-site fluxes and the
+ * direction sources, accumulates them in registers in the reference's order,
+ * applies the stage-2 convex combination, recovers (e, p, u) from the new
+ * T^{tau mu}, regulates pi^{mu nu} and Pi, and writes the cell and its ghost
+ * copies once.  e, p and u are double-buffered (read *_in, write *_out) so
+ * that no thread overwrites a value a neighbour still reads; that is what lets
+ * the inference move into the stencil kernel.  Per step the state crosses HBM
+ * twice (the algorithmic minimum for two stages), in 2 launches instead of 14
+ * loop nests.
+ *
+ * Arithmetic is the reference's, operation for operation, in FP64 with float
+ * truncations where the reference has them; the library is compiled with
+ * --fmad=false so no multiply-add is fused behind the reference's back.
+ */
+#include <cuda_runtime.h>
+#include "vh_kernels.h"
+
+namespace vh {
+
+/* Half-site states at the face between cells b and b+st (HalfSiteExtrapolation.cpp:12-26):
+ * for the forward face of cell s, b = s; for its backward face, b = s - st. */
+__device__ __forceinline__ void extrapolate(const double *__restrict__ qn, long long b, long long st, double th,
+                                            double &qR, double &qL)
+{
+    double A = __ldg(qn + b - st), B = __ldg(qn + b), C = __ldg(qn + b + st), D = __ldg(qn + b + 2 * st);
+    qR = C - approx_deriv(th, B, C, D) / 2;
+    qL = B + approx_deriv(th, A, B, C) / 2;
+}
+
+/* SemiDiscreteKurganovTadmorScheme.cpp:14-62 with LocalPropagationSpeed.cpp:14-22,
+ * SpectralRadius.cpp:14-24 and FluxFunctions.cpp:15-25.  FWD: r = -H, else r += H. */
+template <int NQ, int EOS, int DIR, bool FWD>
+__device__ __forceinline__ void face_flux(const StageArgs &A, long long b, long long st, double ePrev,
+                                          double *__restrict__ r, bool &bad)
+{
+    const double th = A.theta;
+    const long long L = A.L;
+    const double *__restrict__ q = A.qin;
+    double qRs[8], qLs[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) extrapolate(q + c * L, b, st, th, qRs[c], qLs[c]);
+    double PiR = 0, PiL = 0;
+    if (NQ == 15) extrapolate(q + 14 * L, b, st, th, PiR, PiL);
+    Prim R = infer<EOS>(A.eos, A.t, qRs[0] - qRs[4], qRs[1] - qRs[5], qRs[2] - qRs[6], qRs[3] - qRs[7], PiR, ePrev, bad);
+    Prim Lf = infer<EOS>(A.eos, A.t, qLs[0] - qLs[4], qLs[1] - qLs[5], qLs[2] - qLs[6], qLs[3] - qLs[7], PiL, ePrev, bad);
+    const double vR = (DIR == 1) ? R.ux : (DIR == 2) ? R.uy : R.un;
+    const double vL = (DIR == 1) ? Lf.ux : (DIR == 2) ? Lf.uy : Lf.un;
+    const double rhoLeft = fabs(vL / Lf.ut);
+    const double rhoRight = fabs(vR / R.ut);
+    const double a = fmax(rhoLeft, rhoRight);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) {
+        double qR, qL;
+        if (n < 8) { qR = qRs[n]; qL = qLs[n]; }
+        else if (n == 14) { qR = PiR; qL = PiL; }
+        else extrapolate(q + n * L, b, st, th, qR, qL);
+        double FqR = vR * qR / R.ut;
+        double FqL = vL * qL / Lf.ut;
+        double res = FqR + FqL - a * (qR - qL);
+        res /= 2;
+        if (FWD) r[n] = -res;
+        else r[n] += res;
+    }
+}
+
+/* SourceTerms.cpp:316-419: sources from d(pi^{tau mu})/dx^i of the T^{tau mu} rows. */
+template <int NQ, int DIR>
+__device__ __forceinline__ void dir_sources(const StageArgs &A, long long s, long long st, double d, double *S)
+{
+    const long long L = A.L;
+    const double *__restrict__ q = A.qin;
+    const double fac = 1 / d / 2;
+    const double ut = __ldg(A.uin + s);
+    const double v = __ldg(A.uin + DIR * L + s);
+    const double vv = v / ut;
+#define DER(n) ((__ldg(q + (n) * L + s + st) - __ldg(q + (n) * L + s - st)) * fac)
+    if (DIR == 1) {
+        double dpitt = DER(4), dpitx = DER(5), dpity = DER(6), dpitn = DER(7), dpixx = DER(8), dpixy = DER(9), dpixn = DER(10);
+        if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpitx - vv * dPi; S[1] = dpitx * vv - dpixx - dPi; }
+        else { S[0] = dpitt * vv - dpitx; S[1] = dpitx * vv - dpixx; }
+        S[2] = dpity * vv - dpixy;
+        S[3] = dpitn * vv - dpixn;
+    } else if (DIR == 2) {
+        double dpitt = DER(4), dpitx = DER(5), dpity = DER(6), dpitn = DER(7), dpixy = DER(9), dpiyy = DER(11), dpiyn = DER(12);
+        if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpity - vv * dPi; S[2] = dpity * vv - dpiyy - dPi; }
+        else { S[0] = dpitt * vv - dpity; S[2] = dpity * vv - dpiyy; }
+        S[1] = dpitx * vv - dpixy;
+        S[3] = dpitn * vv - dpiyn;
+    } else {
+        double dpitt = DER(4), dpitx = DER(5), dpity = DER(6), dpitn = DER(7), dpixn = DER(10), dpiyn = DER(12), dpinn = DER(13);
+        if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpitn - vv * dPi; S[3] = dpitn * vv - dpinn - dPi / A.t2pow; }
+        else { S[0] = dpitt * vv - dpitn; S[3] = dpitn * vv - dpinn; }
+        S[1] = dpitx * vv - dpixn;
+        S[2] = dpity * vv - dpiyn;
+    }
+#undef DER
+}
+
+/* One axis of eulerStepKernelX/Y/Z (FullyDiscreteKurganovTadmorScheme.cpp:300-634). */
+template <int NQ, int EOS, int DIR>
+__device__ __forceinline__ void axis_update(const StageArgs &A, long long s, double ePrev, double *__restrict__ acc, bool &bad)
+{
+    const long long st = (DIR == 1) ? 1 : (DIR == 2) ? (long long)A.ncx : (long long)A.ncx * A.ncy;
+    const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
+    double r[NQ];
+    face_flux<NQ, EOS, DIR, true>(A, s, st, ePrev, r, bad);
+    face_flux<NQ, EOS, DIR, false>(A, s - st, st, ePrev, r, bad);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) r[n] /= d;
+    double S[4];
+    dir_sources<NQ, DIR>(A, s, st, d, S);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) { r[n] += S[n]; r[n] *= A.dt; }
+#pragma unroll
+    for (int n = 4; n < NQ; ++n) r[n] *= A.dt;
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) acc[n] += r[n];
+}
+
+/* SourceTerms.cpp:421-612 (USE_APPROX_DERIVATIVE; the dynamical-source arrays
+ * are zero, DynamicalVariables.cpp:47-52), then Q + dt S
+ * (FullyDiscreteKurganovTadmorScheme.cpp:264-273). */
+template <int NQ, int EOS>
+__device__ __forceinline__ void source_update(const StageArgs &A, long long s, double *__restrict__ acc)
+{
+    const long long L = A.L;
+    const double th = A.theta;
+    const long long sx = 1, sy = A.ncx, sz = (long long)A.ncx * A.ncy;
+    double Qv[NQ];
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) Qv[n] = __ldg(A.qin + n * L + s);
+    const double Pi = (NQ == 15) ? Qv[14] : 0;
+    const double *__restrict__ utv = A.uin, *__restrict__ uxv = A.uin + L, *__restrict__ uyv = A.uin + 2 * L,
+                 *__restrict__ unv = A.uin + 3 * L, *__restrict__ pv = A.pin;
+    const double e = __ldg(A.ein + s), p = __ldg(pv + s);
+    const double ut = __ldg(utv + s), ux = __ldg(uxv + s), uy = __ldg(uyv + s), un = __ldg(unv + s);
+    const double dxut = approx_deriv(th, __ldg(utv + s - sx), ut, __ldg(utv + s + sx)) / A.dx;
+    const double dxux = approx_deriv(th, __ldg(uxv + s - sx), ux, __ldg(uxv + s + sx)) / A.dx;
+    const double dxuy = approx_deriv(th, __ldg(uyv + s - sx), uy, __ldg(uyv + s + sx)) / A.dx;
+    const double dxun = approx_deriv(th, __ldg(unv + s - sx), un, __ldg(unv + s + sx)) / A.dx;
+    const double dyut = approx_deriv(th, __ldg(utv + s - sy), ut, __ldg(utv + s + sy)) / A.dy;
+    const double dyux = approx_deriv(th, __ldg(uxv + s - sy), ux, __ldg(uxv + s + sy)) / A.dy;
+    const double dyuy = approx_deriv(th, __ldg(uyv + s - sy), uy, __ldg(uyv + s + sy)) / A.dy;
+    const double dyun = approx_deriv(th, __ldg(unv + s - sy), un, __ldg(unv + s + sy)) / A.dy;
+    const double dnut = approx_deriv(th, __ldg(utv + s - sz), ut, __ldg(utv + s + sz)) / A.dz;
+    const double dnux = approx_deriv(th, __ldg(uxv + s - sz), ux, __ldg(uxv + s + sz)) / A.dz;
+    const double dnuy = approx_deriv(th, __ldg(uyv + s - sz), uy, __ldg(uyv + s + sz)) / A.dz;
+    const double dnun = approx_deriv(th, __ldg(unv + s - sz), un, __ldg(unv + s + sz)) / A.dz;
+    const double dxp = approx_deriv(th, __ldg(pv + s - sx), p, __ldg(pv + s + sx)) / A.dx;
+    const double dyp = approx_deriv(th, __ldg(pv + s - sy), p, __ldg(pv + s + sy)) / A.dy;
+    const double dnp = approx_deriv(th, __ldg(pv + s - sz), p, __ldg(pv + s + sz)) / A.dz;
+    const double t = A.t;
+    /* Tnn(e, p + Pi, un, pinn, t), EnergyMomentumTensor.cpp:328-330 */
+    const double pP = p + Pi;
+    const double tnn = (e + pP) * un * un + pP / t / t + Qv[13];
+    const double vx = ux / ut, vy = uy / ut, vn = un / ut;
+    const double dxvx = (dxux - vx * dxut) / ut;
+    const double dyvy = (dyuy - vy * dyut) / ut;
+    const double dnvn = (dnun - vn * dnut) / ut;
+    const double dkvk = dxvx + dyvy + dnvn;
+    double S[NQ];
+    S[0] = 0.0 - (Qv[0] / t + t * tnn) + dkvk * (Qv[4] - p - Pi) - vx * dxp - vy * dyp - vn * dnp;
+    S[1] = 0.0 - Qv[1] / t - dxp + dkvk * Qv[5];
+    S[2] = 0.0 - Qv[2] / t - dyp + dkvk * Qv[6];
+    S[3] = 0.0 - 3 * Qv[3] / t - dnp / A.t2pow + dkvk * Qv[7];
+    pimunu_rhs<EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, e, p, ut, ux, uy, un,
+                              __ldg(A.upin + s), __ldg(A.upin + L + s), __ldg(A.upin + 2 * L + s), __ldg(A.upin + 3 * L + s),
+                              Qv + 4, Pi, dxut, dyut, dnut, dxux, dyux, dnux, dxuy, dyuy, dnuy, dxun, dyun, dnun, dkvk,
+                              A.etabar, A.dt);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) acc[n] = Qv[n] + A.dt * S[n];
+}
+
+/* regulateDissipativeCurrents, REG_SCHEME_1 (FullyDiscreteKurganovTadmorScheme.cpp:690-859).
+ * When e > e_reg both factors are exactly 1 and the reference's multiplies are
+ * identities, so the block is skipped. */
+template <int NQ>
+__device__ __forceinline__ void regulate(const StageArgs &A, double *__restrict__ acc, const Prim &P, bool &bad)
+{
+    if (P.e > A.e_reg) return;
+    const double t = A.t_inf, t2 = t * t;
+    const double pitt = acc[4], pitx = acc[5], pity = acc[6], pitn = acc[7], pixx = acc[8];
+    const double pixy = acc[9], pixn = acc[10], piyy = acc[11], piyn = acc[12], pinn = acc[13];
+    const double Pi = (NQ == 15) ? acc[14] : 0;
+    const double ut = P.ut, ux = P.ux, uy = P.uy, un = P.un;
+    const double xi0 = 0.1, rhomax = 1.0;
+    double pipi = pitt * pitt - 2 * pitx * pitx - 2 * pity * pity + pixx * pixx + 2 * pixy * pixy + piyy * piyy - 2 * pitn * pitn * t2 + 2 * pixn * pixn * t2 + 2 * piyn * piyn * t2 + pinn * pinn * t2 * t2;
+    double spipi = sqrt(fabs(pipi));
+    double pimumu = pitt - pixx - piyy - pinn * t * t;
+    double piu0 = -(pitn * t2 * un) + pitt * ut - pitx * ux - pity * uy;
+    double piu1 = -(pixn * t2 * un) + pitx * ut - pixx * ux - pixy * uy;
+    double piu2 = -(piyn * t2 * un) + pity * ut - pixy * ux - piyy * uy;
+    double piu3 = -(pinn * t2 * un) + pitn * ut - pixn * ux - piyn * uy;
+    double a1 = spipi / rhomax / (double)sqrtf(__double2float_rn(P.e * P.e + 3 * P.p * P.p));
+    double a2 = pimumu / xi0 / rhomax / spipi;
+    double a3 = piu0 / xi0 / rhomax / spipi;
+    double a4 = piu1 / xi0 / rhomax / spipi;
+    double a5 = piu2 / xi0 / rhomax / spipi;
+    double a6 = piu3 / xi0 / rhomax / spipi;
+    double a12 = fmax(a1, a2), a34 = fmax(a3, a4), a56 = fmax(a5, a6), a3456 = fmax(a34, a56);
+    double rho = fmax(a12, a3456);
+    double facShear = vh_tanh(rho) / rho;
+    if (fabs(rho) < 1.e-7) facShear = 1.0;
+#pragma unroll
+    for (int n = 4; n < 14; ++n) acc[n] *= facShear;
+    if (isnan(facShear)) bad = true;
+    if (NQ == 15) {
+        double rhoBulk = fabs(Pi) / P.p;
+        double facBulk = vh_tanh(rhoBulk) / rhoBulk;
+        if (fabs(rhoBulk) < 1.e-7) facBulk = 1.0;
+        acc[14] *= facBulk;
+        if (isnan(facBulk)) bad = true;
+    }
+}
+
+template <int NQ>
+__device__ __forceinline__ void put_cell(const StageArgs &A, long long d, const double *__restrict__ acc, const Prim &P)
+{
+    const long long L = A.L;
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) A.qout[n * L + d] = acc[n];
+    A.eout[d] = P.e;
+    A.pout[d] = P.p;
+    A.uout[d] = P.ut;
+    A.uout[L + d] = P.ux;
+    A.uout[2 * L + d] = P.uy;
+    A.uout[3 * L + d] = P.un;
+}
+
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
+__global__ void __launch_bounds__(128) kt_stage_kernel(const __grid_constant__ StageArgs A)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    const int k = blockIdx.z + 2;
+    if (i >= A.nx + 2 || j >= A.ny + 2) return;
+    const long long sxy = (long long)A.ncx * A.ncy;
+    const long long s = i + (long long)A.ncx * j + sxy * k;
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    double acc[NQ];
+    source_update<NQ, EOS>(A, s, acc);
+    axis_update<NQ, EOS, 1>(A, s, ePrev, acc, bad);
+    axis_update<NQ, EOS, 2>(A, s, ePrev, acc, bad);
+    if (HAS_Z) {
+        axis_update<NQ, EOS, 3>(A, s, ePrev, acc, bad);
+    } else {
+        /* nz = 1: the eta ghosts equal the cell, every eta slope is 0 and the
+         * reference's eta pass adds exactly +0.0 (which turns a -0 into +0). */
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) acc[n] += 0.0;
+    }
+    if (STAGE2) {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) { acc[n] += __ldg(A.qbase + n * A.L + s); acc[n] /= 2; }
+    }
+    /* setInferredVariablesKernel (EnergyMomentumTensor.cpp:235-287) with ePrev = e[s] */
+    Prim P = infer<EOS>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
+                        (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
+    regulate<NQ>(A, acc, P, bad);
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+    put_cell<NQ>(A, s, acc, P);
+    /* zero-gradient ghost faces (DynamicalVariables.cpp:220-378) */
+    if (i == 2) { put_cell<NQ>(A, s - 1, acc, P); put_cell<NQ>(A, s - 2, acc, P); }
+    if (i == A.nx + 1) { put_cell<NQ>(A, s + 1, acc, P); put_cell<NQ>(A, s + 2, acc, P); }
+    if (j == 2) { put_cell<NQ>(A, s - A.ncx, acc, P); put_cell<NQ>(A, s - 2 * A.ncx, acc, P); }
+    if (j == A.ny + 1) { put_cell<NQ>(A, s + A.ncx, acc, P); put_cell<NQ>(A, s + 2 * A.ncx, acc, P); }
+    if (k == 2) { put_cell<NQ>(A, s - sxy, acc, P); put_cell<NQ>(A, s - 2 * sxy, acc, P); }
+    if (k == A.nz + 1) { put_cell<NQ>(A, s + sxy, acc, P); put_cell<NQ>(A, s + 2 * sxy, acc, P); }
+}
+
+/* DynamicalVariables.cpp:169-218 (T^{tau mu} from e, p+Pi, u, pi) and the
+ * ghost faces; the previous-step velocity starts equal to u. */
+__global__ void init_kernel(const __grid_constant__ InitArgs A)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= A.nx || j >= A.ny) return;
+    const long long N = (long long)A.nx * A.ny * A.nz;
+    const long long m = i + (long long)A.nx * (j + (long long)A.ny * k);
+    const long long L = A.L, sxy = (long long)A.ncx * A.ncy;
+    const long long s = (i + 2) + (long long)A.ncx * (j + 2) + sxy * (k + 2);
+    double qv[15];
+    const double e = A.e[m], p = A.p[m];
+    const double ut = A.u[m], ux = A.u[N + m], uy = A.u[2 * N + m], un = A.u[3 * N + m];
+    for (int c = 0; c < 10; ++c) qv[4 + c] = A.pi ? A.pi[c * N + m] : 0.0;
+    const double Pi = (A.nq == 15 && A.Pi) ? A.Pi[m] : 0.0;
+    if (A.nq == 15) qv[14] = Pi;
+    const double P = p + Pi;
+    qv[0] = (e + P) * ut * ut - P + qv[4];
+    qv[1] = (e + P) * ut * ux + qv[5];
+    qv[2] = (e + P) * ut * uy + qv[6];
+    qv[3] = (e + P) * ut * un + qv[7];
+    auto put = [&](long long d) {
+        for (int n = 0; n < A.nq; ++n) A.q[n * L + d] = qv[n];
+        A.eo[d] = e; A.po[d] = p;
+        A.uo[d] = ut; A.uo[L + d] = ux; A.uo[2 * L + d] = uy; A.uo[3 * L + d] = un;
+    };
+    put(s);
+    A.upo[s] = ut; A.upo[L + s] = ux; A.upo[2 * L + s] = uy; A.upo[3 * L + s] = un;
+    const int ii = i + 2, jj = j + 2, kk = k + 2;
+    if (ii == 2) { put(s - 1); put(s - 2); }
+    if (ii == A.nx + 1) { put(s + 1); put(s + 2); }
+    if (jj == 2) { put(s - A.ncx); put(s - 2 * A.ncx); }
+    if (jj == A.ny + 1) { put(s + A.ncx); put(s + 2 * A.ncx); }
+    if (kk == 2) { put(s - sxy); put(s - 2 * sxy); }
+    if (kk == A.nz + 1) { put(s + sxy); put(s + 2 * sxy); }
+}
+
+void launch_init(const InitArgs &a, cudaStream_t s)
+{
+    dim3 block(32, 4, 1);
+    dim3 grid((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
+    init_kernel<<<grid, block, 0, s>>>(a);
+}
+
+template <int NQ, int EOS>
+static void launch_stage_t(const StageArgs &a, cudaStream_t s)
+{
+    dim3 block(32, 4, 1);
+    dim3 grid((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
+    const bool z = a.nz > 1, st2 = a.qbase != nullptr;
+    if (z && st2) kt_stage_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
+    else if (z) kt_stage_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
+    else if (st2) kt_stage_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);
+    else kt_stage_kernel<NQ, EOS, false, false><<<grid, block, 0, s>>>(a);
+}
+
+void launch_stage(const StageArgs &a, int nq, int eos_kind, cudaStream_t s)
+{
+    if (nq == 15) {
+        if (eos_kind == 1) launch_stage_t<15, 1>(a, s); else launch_stage_t<15, 0>(a, s);
+    } else {
+        if (eos_kind == 1) launch_stage_t<14, 1>(a, s); else launch_stage_t<14, 0>(a, s);
+    }
+}
+
+} // namespace vh

@@ -1,0 +1,308 @@
+/*
+ * vh_physics.cuh -- per-cell device physics of the KT RK2 step, in FP64 and in
+ * the reference's floating-point operation order (the library is compiled
+ * with --fmad=false, so nothing below is fused unless written as fma()).
+ *
+ * Each function names the reference code it reproduces (file:line in
+ * derekeverett/cpu-vh).  The state lives in padded SoA arrays (stride L
+ * doubles between components) indexed i + ncx*(j + ncy*k).
+ */
+#ifndef VH_PHYSICS_CUH
+#define VH_PHYSICS_CUH
+
+#include "vh_math.cuh"
+
+namespace vh {
+
+/* error codes raised on the device (match VH_ERR_* in vh_b200.h) */
+constexpr int kErrNan = 4;
+
+struct DevEos {
+    int kind;                 /* 0 conformal, 1 table */
+    double a;                 /* conformal e = a T^4 */
+    const double *p_tb;       /* tabulated P(e) [fm^-4] */
+    const double *T_tb;       /* tabulated T(e) [fm^-1] */
+    int e_length;
+    double e_min, e_spacing;
+    PowfTab pq;               /* host-exact powf(x, 0.25) */
+};
+
+struct DevErr {
+    int *code;                /* first error code, 0 if none */
+    long long *cell;          /* padded index of the first failing cell */
+    int *step;                /* step counter at the time */
+};
+
+__device__ __forceinline__ void raise_error(const DevErr &E, int code, long long cell, int step)
+{
+    if (atomicCAS(E.code, 0, code) == 0) { *E.cell = cell; *E.step = step; }
+}
+
+/* ------------------------------------------------------------------ EoS */
+/* EquationOfState.cpp:329-360 */
+__device__ __forceinline__ double eos_interp(const DevEos &E, double ed, const double *tb)
+{
+    int idx = (int)((ed - E.e_min) / E.e_spacing);
+    idx = (E.e_length - 2 < idx) ? E.e_length - 2 : idx;   /* std::min(N_e - 2, idx) */
+    idx = (idx < 0) ? 0 : idx;                              /* std::max(0, idx)       */
+    const double frac = (ed - (idx * E.e_spacing + E.e_min)) / E.e_spacing;
+    return __ldg(tb + idx) * (1. - frac) + __ldg(tb + idx + 1) * frac;
+}
+/* std::max(1.e-15, f): (1e-15 < f) ? f : 1e-15 */
+__device__ __forceinline__ double floor15(double f) { return (1.e-15 < f) ? f : 1.e-15; }
+
+template <int EOS>
+__device__ __forceinline__ double eos_p(const DevEos &E, double ed)          /* EquationOfState.cpp:44-107 */
+{
+    if (EOS == 1) return floor15(eos_interp(E, ed, E.p_tb));
+    return ed / 3.;
+}
+template <int EOS>
+__device__ __forceinline__ double eos_cs2(const DevEos &E, double ed)        /* EquationOfState.cpp:109-160 */
+{
+    if (EOS == 1) {
+        const double v_min = 0.01, v_max = 1. / 3.;
+        double pp = eos_p<1>(E, ed);
+        double p_r = eos_p<1>(E, ed + E.e_spacing);
+        double v = E.e_spacing / (p_r - pp);
+        v = (v < v_max) ? v : v_max;            /* std::min(v_max, v) */
+        return (v_min < v) ? v : v_min;         /* std::max(v_min, v) */
+    }
+    return 1. / 3.;
+}
+template <int EOS>
+__device__ __forceinline__ double eos_T(const DevEos &E, double ed)          /* EquationOfState.cpp:162-199 */
+{
+    if (EOS == 1) return floor15(eos_interp(E, ed, E.T_tb));
+    return (double)powf_quarter(__double2float_rn(ed / E.a), E.pq);
+}
+
+/* --------------------------------------------------------- limiter */
+/* FluxLimiter.cpp:14-32, generalised minmod with sign(0) = +1 */
+__device__ __forceinline__ double minmod(double x, double y)
+{
+    int sx = (x < 0) ? -1 : 1, sy = (y < 0) ? -1 : 1;
+    return (sx + sy) * fmin(fabs(x), fabs(y)) / 2.0;
+}
+__device__ __forceinline__ double approx_deriv(double th, double x, double y, double z)
+{
+    double l = th * (y - x);
+    double c = (z - x) / 2.0;
+    double r = th * (z - y);
+    return minmod(l, minmod(c, r));
+}
+
+/* -------------------------------------------------------- inversion */
+/* EnergyMomentumTensor.cpp:22-115: energy density from M0, M, Pi */
+template <int EOS>
+__device__ double e_from_conserved(const DevEos &E, double ePrev, double M0, double M, double Pi, bool &bad)
+{
+    if (EOS == 0) {
+        float h = sqrtf(fabsf(__double2float_rn(4 * M0 * M0 - 3 * M)));
+        return (double)fabsf(__double2float_rn((double)h - M0));
+    }
+    double e0 = ePrev;
+    for (int j = 0; j < 10000; ++j) {                              /* MAX_ITERS_NR */
+        double pp = eos_p<1>(E, e0);
+        double cs2 = eos_cs2<1>(E, e0);
+        double cst2 = pp / e0;
+        double A = M0 * (1.0 - cst2) + Pi;
+        double B = M0 * (M0 + Pi) - M;
+        double H = (double)sqrtf(fabsf(__double2float_rn(A * A + 4 * cst2 * B)));
+        double D = (A - H) / (2 * cst2);
+        double f = e0 + D;
+        double fp = 1.0 - ((cs2 - cst2) * (B + D * H - ((cs2 - cst2) * cst2 * D * M0) / e0)) / (cst2 * e0 * H);
+        if (isnan(f / fp)) { bad = true; return ePrev; }
+        double e = e0 - f / fp;
+        if ((double)fabsf(__double2float_rn(e - e0)) <= 1.0e-3 * (double)fabsf(__double2float_rn(e))) return e;
+        e0 = e;
+    }
+    /* bisection fallback, EnergyMomentumTensor.cpp:48-111 */
+    double e_lo = 0.0, e_mid = ePrev, e_hi = 2.0 * (ePrev + 1.0);
+    for (int j = 0; j < 1000000; ++j) {                            /* MAX_ITERS_BI */
+        double p_lo = eos_p<1>(E, e_lo), p_mid = eos_p<1>(E, e_mid), p_hi = eos_p<1>(E, e_hi);
+        double c_lo = p_lo / e_lo, c_mid = p_mid / e_mid, c_hi = p_hi / e_hi;
+        double A_lo = M0 * (1.0 - c_lo) + Pi, A_mid = M0 * (1.0 - c_mid) + Pi, A_hi = M0 * (1.0 - c_hi) + Pi;
+        double B = M0 * (M0 + Pi) - M;
+        double H_lo = (double)sqrtf(fabsf(__double2float_rn(A_lo * A_lo + 4 * c_lo * B)));
+        double H_mid = (double)sqrtf(fabsf(__double2float_rn(A_mid * A_mid + 4 * c_mid * B)));
+        double H_hi = (double)sqrtf(fabsf(__double2float_rn(A_hi * A_hi + 4 * c_hi * B)));
+        double f_lo = e_lo + (A_lo - H_lo) / (2 * c_lo);
+        double f_mid = e_mid + (A_mid - H_mid) / (2 * c_mid);
+        double f_hi = e_hi + (A_hi - H_hi) / (2 * c_hi);
+        if ((e_hi - e_lo) < (1.0e-3 * e_hi) / 2.0) return e_mid;
+        if (f_lo * f_mid < 0.0) { e_hi = e_mid; e_mid = (e_lo + e_hi) / 2.0; }
+        else if (f_mid * f_hi < 0.0) { e_lo = e_mid; e_mid = (e_lo + e_hi) / 2.0; }
+    }
+    return ePrev;
+}
+
+struct Prim { double e, p, ut, ux, uy, un; };
+
+/* EnergyMomentumTensor.cpp:117-233, from the five combinations it uses
+ * (M0 = ttt - pitt, M1..M3 = tt^i - pit^i, Pi). */
+template <int EOS>
+__device__ __forceinline__ Prim infer(const DevEos &E, double t, double M0, double M1, double M2, double M3,
+                                      double Pi, double ePrev, bool &bad)
+{
+    Prim r;
+    double M = M1 * M1 + M2 * M2 + t * t * M3 * M3;
+    if (ePrev <= 0.1) r.e = M0 - M / M0;
+    else r.e = e_from_conserved<EOS>(E, ePrev, M0, M, Pi, bad);
+    if (isnan(r.e)) bad = true;
+    r.p = eos_p<EOS>(E, r.e);
+    if (r.e < 1.e-7) { r.e = 1.e-7; r.p = 1.e-7; }
+    double P = r.p + Pi;
+    double Einv = 1.0 / (r.e + P);
+    r.ut = (double)sqrtf(fabsf(__double2float_rn((M0 + P) * Einv)));
+    double E2 = Einv / r.ut;
+    r.ux = M1 * E2;
+    r.uy = M2 * E2;
+    r.un = M3 * E2;
+    if (r.ut > 1.0e3) { r.ut = 1.0; r.ux = 0.0; r.uy = 0.0; r.un = 0.0; }
+    return r;
+}
+
+/* --------------------------------------------------- bulk viscosity */
+struct Zeta { int law; double norm, T0, w; };
+
+/* SourceTerms.cpp:40-48 (T in fm^-1) or a Gaussian in T [GeV] */
+__device__ __forceinline__ double zeta_over_s(const Zeta &Z, double T)
+{
+    if (Z.law == 1) {
+        double z = (T * 0.197326938 - Z.T0) / Z.w;
+        return Z.norm * exp(-(z * z));
+    }
+    double x = T / 1.01355;
+    if (x > 1.05) return 0.9 * exp(-(x - 1) / 0.025) + 0.25 * exp(-(x - 1) / 0.13) + 0.001;
+    else if (x < 0.995) return 0.9 * exp((x - 1) / 0.0025) + 0.22 * exp((x - 1) / 0.022) + 0.03;
+    return -13.77 * x * x + 27.55 * x - 13.45;
+}
+
+/* SourceTerms.cpp:55-313, the right-hand side of the pi^{mu nu} (and Pi)
+ * relaxation equations divided by u^tau. */
+template <int EOS, bool BULK>
+__device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, double *rhs, double t, double e, double p,
+    double ut, double ux, double uy, double un, double utp, double uxp, double uyp, double unp,
+    const double *pv, double Pi,
+    double dxut, double dyut, double dnut, double dxux, double dyux, double dnux,
+    double dxuy, double dyuy, double dnuy, double dxun, double dyun, double dnun, double dkvk,
+    double d_etabar, double d_dt)
+{
+    const double delta_pipi = 1.33333, tau_pipi = 1.42857, delta_PiPi = 0.666667, lambda_piPi = 1.2;
+    const double pitt = pv[0], pitx = pv[1], pity = pv[2], pitn = pv[3], pixx = pv[4];
+    const double pixy = pv[5], pixn = pv[6], piyy = pv[7], piyn = pv[8], pinn = pv[9];
+    double T = eos_T<EOS>(E, e);
+    double taupiInv = T / 5 / d_etabar;
+    double beta_pi = (e + p) / 5;
+    double cs2 = eos_cs2<EOS>(E, e);
+    double a = 1.0 / 3.0 - cs2;
+    double a2 = a * a;
+    double beta_Pi = 15 * a2 * (e + p);
+    double lambda_Pipi = 8 * a / 5;
+    double tauPiInv = 0.0;
+    if (BULK) tauPiInv = 15 * a2 * T / zeta_over_s(Z, T);
+    double ut2 = ut * ut, un2 = un * un, t2 = t * t, t3 = t * t2;
+    double dtut = (ut - utp) / d_dt, dtux = (ux - uxp) / d_dt, dtuy = (uy - uyp) / d_dt, dtun = (un - unp) / d_dt;
+    double Dut = ut * dtut + ux * dxut + uy * dyut + un * dnut + t * un * un;
+    double DuxUpper = ut * dtux + ux * dxux + uy * dyux + un * dnux;
+    double Dux = -DuxUpper;
+    double DuyUpper = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
+    double Duy = -DuyUpper;
+    double DunUpper = ut * dtun + ux * dxun + uy * dyun + un * dnun + 2 * ut * un / t;
+    double Dun = -t2 * DunUpper;
+    double dut = Dut - t * un * un;
+    double dux = ut * dtux + ux * dxux + uy * dyux + un * dnux;
+    double duy = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
+    double dun = ut * dtun + ux * dxun + uy * dyun + un * dnun;
+    double theta = ut / t + dtut + dxux + dyuy + dnun;
+    double stt = -t * ut * un2 + (dtut - ut * dut) + (ut2 - 1) * theta / 3.0;
+    double stx = -(t * un2 * ux) / 2.0 + (dtux - dxut) / 2.0 - (ux * dut + ut * dux) / 2.0 + ut * ux * theta / 3.0;
+    double sty = -(t * un2 * uy) / 2.0 + (dtuy - dyut) / 2.0 - (uy * dut + ut * duy) / 2.0 + ut * uy * theta / 3.0;
+    double stn = -un * (2.0 * ut2 + t2 * un2) / (2.0 * t) + (dtun - dnut / t2) / 2.0 - (un * dut + ut * dun) / 2.0 + ut * un * theta / 3.0;
+    double sxx = -(dxux + ux * dux) + (1.0 + ux * ux) * theta / 3.0;
+    double sxy = -(dxuy + dyux) / 2.0 - (uy * dux + ux * duy) / 2.0 + ux * uy * theta / 3.0;
+    double sxn = -ut * ux * un / t - (dxun + dnux / t2) / 2.0 - (un * dux + ux * dun) / 2.0 + ux * un * theta / 3.0;
+    double syy = -(dyuy + uy * duy) + (1.0 + uy * uy) * theta / 3.0;
+    double syn = -ut * uy * un / t - (dyun + dnuy / t2) / 2.0 - (un * duy + uy * dun) / 2.0 + uy * un * theta / 3.0;
+    double snn = -ut * (1.0 + 2.0 * t2 * un2) / t3 - dnun / t2 - un * dun + (1.0 / t2 + un2) * theta / 3.0;
+    double wtx = (-dtux - dxut + ut * dux - ux * dut - t * un2 * ux) / 2.0;
+    double wty = (-dtuy - dyut + ut * duy - uy * dut - t * un2 * uy) / 2.0;
+    double wtn = (-t2 * dtun - 2.0 * t * un - dnut - ut * Dun - t2 * un * dut - t3 * un * un2) / 2.0;
+    double wxy = (dxuy - dyux + ux * duy - uy * dux) / 2.0;
+    double wxn = (t2 * dxun - dnux - ux * Dun - t2 * un * dux) / 2.0;
+    double wyn = (t2 * dyun - dnuy - uy * Dun - t2 * un * duy) / 2.0;
+    double wxt = wtx, wyt = wty, wnt = wtn / t2, wyx = -wxy, wnx = -wxn / t2, wny = -wyn / t2;
+    double I1tt = 2.0 * ut * (pitt * Dut + pitx * Dux + pity * Duy + pitn * Dun);
+    double I1tx = (pitt * ux + pitx * ut) * Dut + (pitx * ux + pixx * ut) * Dux + (pity * ux + pixy * ut) * Duy + (pitn * ux + pixn * ut) * Dun;
+    double I1ty = (pitt * uy + pity * ut) * Dut + (pitx * uy + pixy * ut) * Dux + (pity * uy + piyy * ut) * Duy + (pitn * uy + piyn * ut) * Dun;
+    double I1tn = (pitt * un + pitn * ut) * Dut + (pitx * un + pixn * ut) * Dux + (pity * un + piyn * ut) * Duy + (pitn * un + pinn * ut) * Dun;
+    double I1xx = 2.0 * ux * (pitx * Dut + pixx * Dux + pixy * Duy + pixn * Dun);
+    double I1xy = (pitx * uy + pity * ux) * Dut + (pixx * uy + pixy * ux) * Dux + (pixy * uy + piyy * ux) * Duy + (pixn * uy + piyn * ux) * Dun;
+    double I1xn = (pitx * un + pitn * ux) * Dut + (pixx * un + pixn * ux) * Dux + (pixy * un + piyn * ux) * Duy + (pixn * un + pinn * ux) * Dun;
+    double I1yy = 2.0 * uy * (pity * Dut + pixy * Dux + piyy * Duy + piyn * Dun);
+    double I1yn = (pity * un + pitn * uy) * Dut + (pixy * un + pixn * uy) * Dux + (piyy * un + piyn * uy) * Duy + (piyn * un + pinn * uy) * Dun;
+    double I1nn = 2.0 * un * (pitn * Dut + pixn * Dux + piyn * Duy + pinn * Dun);
+    double I2tt = theta * pitt, I2tx = theta * pitx, I2ty = theta * pity, I2tn = theta * pitn, I2xx = theta * pixx;
+    double I2xy = theta * pixy, I2xn = theta * pixn, I2yy = theta * piyy, I2yn = theta * piyn, I2nn = theta * pinn;
+    double I3tt = 2.0 * (pitx * wtx + pity * wty + pitn * wtn);
+    double I3tx = pitt * wxt + pity * wxy + pitn * wxn + pixx * wtx + pixy * wty + pixn * wtn;
+    double I3ty = pitt * wyt + pitx * wyx + pitn * wyn + pixy * wtx + piyy * wty + piyn * wtn;
+    double I3tn = pitt * wnt + pitx * wnx + pity * wny + pixn * wtx + piyn * wty + pinn * wtn;
+    double I3xx = 2.0 * (pitx * wxt + pixy * wxy + pixn * wxn);
+    double I3xy = pitx * wyt + pity * wxt + pixx * wyx + piyy * wxy + pixn * wyn + piyn * wxn;
+    double I3xn = pitx * wnt + pitn * wxt + pixx * wnx + pixy * wny + piyn * wxy + pinn * wxn;
+    double I3yy = 2.0 * (pity * wyt + pixy * wyx + piyn * wyn);
+    double I3yn = pity * wnt + pitn * wyt + pixy * wnx + pixn * wyx + piyy * wny + pinn * wyn;
+    double I3nn = 2.0 * (pitn * wnt + pixn * wnx + piyn * wny);
+    double ux2 = ux * ux, uy2 = uy * uy;
+    double ps = pitt * stt - 2.0 * pitx * stx - 2.0 * pity * sty + pixx * sxx + 2.0 * pixy * sxy + piyy * syy - 2.0 * pitn * stn * t2 + 2.0 * pixn * sxn * t2 + 2.0 * piyn * syn * t2 + pinn * snn * t2 * t2;
+    double I4tt = (pitt * stt - pitx * stx - pity * sty - t2 * pitn * stn) - (1.0 - ut2) * ps / 3.0;
+    double I4tx = (pitt * stx + pitx * stt) / 2.0 - (pitx * sxx + pixx * stx) / 2.0 - (pity * sxy + pixy * sty) / 2.0 - t2 * (pitn * sxn + pixn * stn) / 2.0 + (ut * ux) * ps / 3.0;
+    double I4ty = (pitt * sty + pity * stt) / 2.0 - (pitx * sxy + pixy * stx) / 2.0 - (pity * syy + piyy * sty) / 2.0 - t2 * (pitn * syn + piyn * stn) / 2.0 + (ut * uy) * ps / 3.0;
+    double I4tn = (pitt * stn + pitn * stt) / 2.0 - (pitx * sxn + pixn * stx) / 2.0 - (pity * syn + piyn * sty) / 2.0 - t2 * (pitn * snn + pinn * stn) / 2.0 + (ut * un) * ps / 3.0;
+    double I4xx = (pitx * stx - pixx * sxx - pixy * sxy - t2 * pixn * sxn) + (1.0 + ux2) * ps / 3.0;
+    double I4xy = (pitx * sty + pity * stx) / 2.0 - (pixx * sxy + pixy * sxx) / 2.0 - (pixy * syy + piyy * sxy) / 2.0 - t2 * (pixn * syn + piyn * sxn) / 2.0 + (ux * uy) * ps / 3.0;
+    double I4xn = (pitx * stn + pitn * stx) / 2.0 - (pixx * sxn + pixn * sxx) / 2.0 - (pixy * syn + piyn * sxy) / 2.0 - t2 * (pixn * snn + pinn * sxn) / 2.0 + (ux * un) * ps / 3.0;
+    double I4yy = (pity * sty - pixy * sxy - piyy * syy - t2 * piyn * syn) + (1.0 + uy2) * ps / 3.0;
+    double I4yn = (pity * stn + pitn * sty) / 2.0 - (pixy * sxn + pixn * sxy) / 2.0 - (piyy * syn + piyn * syy) / 2.0 - t2 * (piyn * snn + pinn * syn) / 2.0 + (uy * un) * ps / 3.0;
+    double I4nn = (pitn * stn - pixn * sxn - piyn * syn - t2 * pinn * snn) + (1.0 / t2 + un2) * ps / 3.0;
+    double Itt = I1tt + delta_pipi * I2tt - I3tt + tau_pipi * I4tt - lambda_piPi * Pi * stt;
+    double Itx = I1tx + delta_pipi * I2tx - I3tx + tau_pipi * I4tx - lambda_piPi * Pi * stx;
+    double Ity = I1ty + delta_pipi * I2ty - I3ty + tau_pipi * I4ty - lambda_piPi * Pi * sty;
+    double Itn = I1tn + delta_pipi * I2tn - I3tn + tau_pipi * I4tn - lambda_piPi * Pi * stn;
+    double Ixx = I1xx + delta_pipi * I2xx - I3xx + tau_pipi * I4xx - lambda_piPi * Pi * sxx;
+    double Ixy = I1xy + delta_pipi * I2xy - I3xy + tau_pipi * I4xy - lambda_piPi * Pi * sxy;
+    double Ixn = I1xn + delta_pipi * I2xn - I3xn + tau_pipi * I4xn - lambda_piPi * Pi * sxn;
+    double Iyy = I1yy + delta_pipi * I2yy - I3yy + tau_pipi * I4yy - lambda_piPi * Pi * syy;
+    double Iyn = I1yn + delta_pipi * I2yn - I3yn + tau_pipi * I4yn - lambda_piPi * Pi * syn;
+    double Inn = I1nn + delta_pipi * I2nn - I3nn + tau_pipi * I4nn - lambda_piPi * Pi * snn;
+    double dpitt = 2.0 * beta_pi * stt - pitt * taupiInv - Itt - 2.0 * un * t * pitn;
+    double dpitx = 2.0 * beta_pi * stx - pitx * taupiInv - Itx - un * t * pixn;
+    double dpity = 2.0 * beta_pi * sty - pity * taupiInv - Ity - un * t * piyn;
+    double dpitn = 2.0 * beta_pi * stn - pitn * taupiInv - Itn - un * t * pinn - (ut * pitn + un * pitt) / t;
+    double dpixx = 2.0 * beta_pi * sxx - pixx * taupiInv - Ixx;
+    double dpixy = 2.0 * beta_pi * sxy - pixy * taupiInv - Ixy;
+    double dpixn = 2.0 * beta_pi * sxn - pixn * taupiInv - Ixn - (ut * pixn + un * pitx) / t;
+    double dpiyy = 2.0 * beta_pi * syy - piyy * taupiInv - Iyy;
+    double dpiyn = 2.0 * beta_pi * syn - piyn * taupiInv - Iyn - (ut * piyn + un * pity) / t;
+    double dpinn = 2.0 * beta_pi * snn - pinn * taupiInv - Inn - 2 * (ut * pinn + un * pitn) / t;
+    rhs[0] = dpitt / ut + pitt * dkvk;
+    rhs[1] = dpitx / ut + pitx * dkvk;
+    rhs[2] = dpity / ut + pity * dkvk;
+    rhs[3] = dpitn / ut + pitn * dkvk;
+    rhs[4] = dpixx / ut + pixx * dkvk;
+    rhs[5] = dpixy / ut + pixy * dkvk;
+    rhs[6] = dpixn / ut + pixn * dkvk;
+    rhs[7] = dpiyy / ut + piyy * dkvk;
+    rhs[8] = dpiyn / ut + piyn * dkvk;
+    rhs[9] = dpinn / ut + pinn * dkvk;
+    if (BULK) {
+        double dPi = -beta_Pi * theta - Pi * tauPiInv - delta_PiPi * Pi * theta + lambda_Pipi * ps;
+        rhs[10] = dPi / ut + Pi * dkvk;
+    }
+}
+
+} // namespace vh
+
+#endif

@@ -1,0 +1,175 @@
+"""TEST INFRASTRUCTURE ONLY: Python access to the CPU oracles.
+
+* OracleEvent wraps liboracle_vh.so, the C restatement of the cpu-vh hot path
+  (vh_oracle.c, cornelius_oracle.c).  It is built from this directory's
+  sources by `make -C oracle` (the tests build it on demand with gcc).
+* RefEvent wraps oracle/_ref/libvhref_<variant>.so, the reference's own
+  sources compiled in place by oracle/ref.mk; it exists only where the
+  reference tree was available at build time.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may use
+this module, and only as the checker or the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle_vh.so")
+REF_DIR = os.path.join(HERE, "_ref")
+_dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+
+def build_oracle(force: bool = False) -> str:
+    srcs = [os.path.join(HERE, f) for f in ("vh_oracle.c", "cornelius_oracle.c") if os.path.exists(os.path.join(HERE, f))]
+    newest = max(os.path.getmtime(s) for s in srcs)
+    if force or not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < newest:
+        subprocess.run(["make", "-s", "-C", HERE, "liboracle_vh.so", "CC_HOST=gcc"], check=True)
+    return ORACLE_LIB
+
+
+_olib = None
+
+
+def oracle_lib():
+    global _olib
+    if _olib is None:
+        _olib = C.CDLL(build_oracle())
+        L = _olib
+        L.vho_create.restype = C.c_void_p
+        L.vho_create.argtypes = [C.c_int] * 3 + [C.c_double] * 7 + [C.c_int, C.c_double, C.c_double, C.c_int]
+        L.vho_set_conformal.argtypes = [C.c_void_p, C.c_double]
+        L.vho_set_zeta.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.vho_set_table.argtypes = [C.c_void_p, _dp, C.c_int]
+        L.vho_set_ic.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_void_p, C.c_void_p]
+        L.vho_step.argtypes = [C.c_void_p, C.c_int]
+        L.vho_get.argtypes = [C.c_void_p, C.c_int, _dp]
+        L.vho_destroy.argtypes = [C.c_void_p]
+        for f in ("vho_eos_p", "vho_eos_T", "vho_eos_cs2", "vho_eos_e"):
+            getattr(L, f).argtypes = [C.c_void_p, C.c_double]
+            getattr(L, f).restype = C.c_double
+        L.vho_fo_eF.argtypes = [C.c_void_p]
+        L.vho_fo_eF.restype = C.c_double
+        L.vho_time.argtypes = [C.c_void_p]
+        L.vho_time.restype = C.c_double
+        L.vho_steps_done.argtypes = [C.c_void_p]
+        if hasattr(L, "vho_freezeout"):
+            L.vho_freezeout.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+            L.vho_freezeout.restype = C.c_int
+    return _olib
+
+
+def _p(a):
+    return None if a is None else np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(C.c_void_p)
+
+
+class OracleEvent:
+    """The C restatement driven like vh.Event (same config structure)."""
+
+    def __init__(self, cfg, eos_rows=None):
+        L = oracle_lib()
+        self.L, self.cfg = L, cfg
+        self.h = L.vho_create(cfg.nx, cfg.ny, cfg.nz, cfg.dx, cfg.dy, cfg.dz, cfg.dt, cfg.t0, cfg.etabar, cfg.theta,
+                              cfg.bulk, cfg.T_reg_GeV, cfg.T_freezeout_GeV, cfg.fo_factor)
+        if cfg.eos_kind == 1:
+            rows = np.ascontiguousarray(eos_rows, dtype=np.float64)
+            L.vho_set_table(self.h, rows, len(rows))
+        else:
+            L.vho_set_conformal(self.h, cfg.eos_factor)
+        L.vho_set_zeta(self.h, cfg.zeta_law, cfg.zeta_norm, cfg.zeta_T0_GeV, cfg.zeta_width_GeV)
+        self.nq = 15 if cfg.bulk else 14
+
+    def set_initial(self, st):
+        self._keep = [np.ascontiguousarray(x, dtype=np.float64) if x is not None else None
+                      for x in (st.e, st.p, np.asarray(st.u).reshape(-1), None if st.pi is None else np.asarray(st.pi).reshape(-1), st.Pi)]
+        e, p, u, pi, Pi = self._keep
+        self.L.vho_set_ic(self.h, e, p, u, _p(pi) if pi is not None else None, _p(Pi) if Pi is not None else None)
+
+    def step(self, n=1):
+        return self.L.vho_step(self.h, n)
+
+    def field(self, fid):
+        ncx, ncy, ncz = self.cfg.nx + 4, self.cfg.ny + 4, self.cfg.nz + 4
+        out = np.zeros(ncx * ncy * ncz)
+        rc = self.L.vho_get(self.h, fid, out)
+        assert rc == 0, fid
+        return out
+
+    def freezeout(self, cap=None):
+        n_el, n_ab = C.c_int(), C.c_int()
+        cap = cap or max(1024, 40 * self.cfg.nx * self.cfg.ny * max(1, self.cfg.nz))
+        buf = np.zeros((cap, 20))
+        rc = self.L.vho_freezeout(self.h, buf.ctypes.data_as(C.c_void_p), cap, C.byref(n_el), C.byref(n_ab))
+        assert rc == 0, rc
+        return buf[:n_el.value].copy(), n_ab.value
+
+    def close(self):
+        if self.h:
+            self.L.vho_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def ref_available(variant: str) -> bool:
+    return os.path.exists(os.path.join(REF_DIR, f"libvhref_{variant}.so"))
+
+
+class RefEvent:
+    """The reference's own code (oracle/_ref), single-threaded unless asked.
+
+    The reference keeps its state in process globals, so only one RefEvent per
+    variant library may be live at a time."""
+
+    def __init__(self, variant, cfg, eos_rows=None, threads=1):
+        path = os.path.join(REF_DIR, f"libvhref_{variant}.so")
+        L = C.CDLL(path)
+        self.L, self.cfg = L, cfg
+        L.vhref_threads.argtypes = [C.c_int]
+        L.vhref_threads(threads)
+        L.vhref_setup.argtypes = [C.c_int] * 5 + [C.c_double] * 8 + [C.c_int]
+        L.vhref_setup(cfg.nx, cfg.ny, cfg.nz, 100000, cfg.fo_factor, cfg.dx, cfg.dy, cfg.dz, cfg.dt, cfg.t0, cfg.etabar,
+                      cfg.T_freezeout_GeV, cfg.T_reg_GeV, 0)
+        if eos_rows is not None:
+            L.vhref_load_eos_table.argtypes = [_dp, C.c_int]
+            rows = np.ascontiguousarray(eos_rows, dtype=np.float64)
+            L.vhref_load_eos_table(rows, len(rows))
+        L.vhref_set_ic_arrays.argtypes = [_dp] * 5
+        L.vhref_get.argtypes = [C.c_int, _dp]
+        L.vhref_step.argtypes = [C.c_int]
+        L.vhref_time_steps.argtypes = [C.c_int]
+        L.vhref_time_steps.restype = C.c_double
+        L.vhref_freezeout.argtypes = [C.c_char_p]
+        L.vhref_run_full.argtypes = [C.c_char_p]
+        L.vhref_theta.restype = C.c_double
+        for f in ("vhref_eos_pressure", "vhref_eos_temperature", "vhref_eos_cs2", "vhref_eos_energy"):
+            getattr(L, f).argtypes = [C.c_double]
+            getattr(L, f).restype = C.c_double
+
+    def set_initial(self, st):
+        N = self.cfg.nx * self.cfg.ny * self.cfg.nz
+        pi = np.zeros(10 * N) if st.pi is None else np.ascontiguousarray(st.pi, dtype=np.float64).reshape(-1)
+        Pi = np.zeros(N) if st.Pi is None else np.ascontiguousarray(st.Pi, dtype=np.float64)
+        self.L.vhref_set_ic_arrays(np.ascontiguousarray(st.e), np.ascontiguousarray(st.p),
+                                   np.ascontiguousarray(st.u, dtype=np.float64).reshape(-1), pi, Pi)
+        self.L.vhref_init()
+
+    def step(self, n=1):
+        self.L.vhref_step(n)
+
+    def time_steps(self, n):
+        return self.L.vhref_time_steps(n)
+
+    def field(self, fid):
+        ncx, ncy, ncz = self.cfg.nx + 4, self.cfg.ny + 4, self.cfg.nz + 4
+        out = np.zeros(ncx * ncy * ncz)
+        assert self.L.vhref_get(fid, out) == 0, fid
+        return out
+
+    def freezeout(self, path):
+        return self.L.vhref_freezeout(path.encode())
