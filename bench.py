@@ -1,0 +1,313 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 KT RK2 step (cell-updates/s).
+
+Workload (default): the 3+1D optical-Glauber event, 131x131x61 cells,
+dx=dy=0.15 fm, deta=0.2, tau0=0.6 fm/c, dtau=0.015 fm/c, 2000-row synthetic
+crossover EoS table, eta/s=0.08, Gaussian zeta/s (bulk evolved, 15 conserved
+components), FP64 in the reference's operation order.  One "step" is one RK2
+step over the whole lattice.  Synthetic seeded inputs stand in for physics
+event generators (none are public for this path).
+
+  value  cell-updates/s with the state resident in HBM, CUDA events on the
+         event's stream around K steps (the state, ~580 MB, is larger than
+         the 126 MB L2, so no flush is needed between steps)
+  e2e    the same metric through the C ABI with pinned host buffers: upload of
+         the initial condition, K steps, download of the energy density, timed
+         on the host clock
+  roofline  dominant kernel = the fused stage kernel; algorithmic bytes per
+         launch = 428 B/cell (mean of the 368 B and 488 B the two stages must
+         move), peak = measured HBM copy bandwidth
+  cpu_baseline  the reference's own sources (oracle/_ref, OpenMP over all host
+         cores) on a bounded sample of the same workload
+
+`--impl reference` times the reference CPU implementation instead (rank 0).
+Multi-GPU: independent replicas (events share nothing), max time over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cpu-vh_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+BYTES_PER_CELL_STEP = 856          # (5*Nq + 32) * 8 with Nq = 15
+BYTES_PER_CELL_LAUNCH = 428        # stage 1: 46 words, stage 2: 61 words; mean
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="glauber_3p1d", choices=["glauber_3p1d", "gubser_2p1d"])
+    ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    return ap.parse_args()
+
+
+def workload(name):
+    import vh
+    if name == "gubser_2p1d":
+        cfg = vh.gubser_config()
+        return cfg, None, vh.gubser_ic(cfg), "conf", (
+            "gubser_2p1d: 101x101x1, dx=0.1 fm, tau0=1.0, dtau=0.01, conformal a=15.6269, eta/s=0.2, "
+            "theta=1.8, T0=0.3 GeV, pi at Navier-Stokes")
+    cfg = vh.glauber_config()
+    rows = vh.synthetic_eos_table()
+    return cfg, rows, vh.glauber_ic(cfg, rows), "table", (
+        "glauber_3p1d: 131x131x61, dx=dy=0.15 fm, deta=0.2, tau0=0.6, dtau=0.015, Au+Au optical Glauber b=7 fm, "
+        "peak 30 GeV/fm^3, 2000-row synthetic crossover EoS, eta/s=0.08, Gaussian zeta/s (bulk on), FP64")
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(cfg, rows, st, variant, steps=2):
+    """The reference's own code (oracle/_ref) on all host cores, `steps` RK2 steps."""
+    import oracle as O
+    threads = os.cpu_count() or 1
+    N = cfg.nx * cfg.ny * cfg.nz
+    if O.ref_available(variant):
+        ref = O.RefEvent(variant, cfg, rows, threads=threads)
+        kind = "reference"
+    else:
+        ref = O.OracleEvent(cfg, rows)
+        threads = 1
+        kind = "port"
+    ref.set_initial(st)
+    if kind == "reference":
+        ref.time_steps(1)                      # warm-up step
+        secs = ref.time_steps(steps)
+    else:
+        ref.step(1)
+        t0 = time.perf_counter()
+        ref.step(steps)
+        secs = time.perf_counter() - t0
+    return {"value": N * steps / secs, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+            "sample": f"{steps} RK2 steps of the same {cfg.nx}x{cfg.ny}x{cfg.nz} event after 1 warm-up step, "
+                      f"{threads} OpenMP threads" + (" (reference sources, -O3 -ffp-contract=off)" if kind == "reference"
+                                                      else " (C restatement, 1 thread)"),
+            "seconds": secs}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cfg, rows, st, variant, desc = workload(args.workload)
+    import oracle as O
+    N = cfg.nx * cfg.ny * cfg.nz
+    threads = os.cpu_count() or 1
+    if O.ref_available(variant):
+        ref, kind = O.RefEvent(variant, cfg, rows, threads=threads), "reference"
+    else:
+        ref, kind, threads = O.OracleEvent(cfg, rows), "port", 1
+    ref.set_initial(st)
+    # bounded sample: at most ~150 s of timed CPU work
+    t0 = time.perf_counter()
+    ref.step(1)
+    est = time.perf_counter() - t0
+    warm = max(0, min(args.warmup, int(30.0 / max(est, 1e-3))) - 1)
+    if warm:
+        ref.step(warm)
+    k = max(1, min(args.steps, int(150.0 / max(est, 1e-3))))
+    t0 = time.perf_counter()
+    ref.step(k)
+    secs = time.perf_counter() - t0
+    v = N * k / secs
+    line = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / k * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": desc, "cells": N, "timed_steps": k},
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": kind,
+                             "sample": f"{k} RK2 steps timed of {args.steps} requested (bounded to ~150 s), "
+                                       f"{threads} OpenMP threads"},
+            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    import vh
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    cfg, rows, st, variant, desc = workload(args.workload)
+    N = cfg.nx * cfg.ny * cfg.nz
+    ev = vh.Event(cfg, rows)
+    ev.set_initial(st)
+    stream = torch.cuda.ExternalStream(ev.stream())
+    ev.step(args.warmup)
+    ev.sync()
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    ev.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    rc, _, _ = ev.status()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    vh.check(rc, "timed steps")
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    ms_step = ms / args.steps
+    value = N * args.steps * world / (ms / 1e3)
+    launch_s = ms / 1e3 / (2 * args.steps)
+    peak, peak_kind = measured_peaks()
+    achieved = BYTES_PER_CELL_LAUNCH * N / launch_s / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        # pinned host buffers; one event = upload IC, K steps, download e
+        nq_in = 17
+        pin = torch.empty((nq_in, N), dtype=torch.float64, pin_memory=True)
+        h = pin.numpy()
+        h[0], h[1], h[2:6] = st.e, st.p, st.u
+        h[6:16] = 0.0 if st.pi is None else st.pi
+        h[16] = 0.0 if st.Pi is None else st.Pi
+        outp = torch.empty(ev.cfg.padded()[0] * ev.cfg.padded()[1] * ev.cfg.padded()[2], dtype=torch.float64,
+                           pin_memory=True).numpy()
+        init = vh.InitialState(h[0], h[1], h[2:6], h[6:16], h[16] if cfg.bulk else None)
+        ev.set_initial(init)
+        ev.step(1)
+        ev.sync()
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ev.set_initial(init)
+        ev.step(args.steps)
+        vh.check(vh.lib.vh_event_get_field(ev.h, vh.VH_F_E, outp), "vh_event_get_field")
+        rc, _, _ = ev.status()
+        t1 = time.perf_counter()
+        barrier()
+        vh.check(rc, "e2e steps")
+        secs = max_over_ranks(t1 - t0)
+        h2d = (6 * N + 10 * N + (N if cfg.bulk else 0)) * 8
+        e2e = {"value": N * args.steps * world / secs, "unit": "cell-updates/s",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": outp.nbytes / args.steps,
+               "timer": "host wall clock, pinned buffers, IC upload + K steps + e download"}
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_baseline:
+        base = cpu_baseline(cfg, rows, st, variant)
+
+    if rank == 0:
+        line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": desc, "cells": N, "parallelism": f"replicas x{world}",
+                           "l2": "state ~580 MB > 126 MB L2, no flush"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None,
+                             "note": f"peak {peak_kind}; algorithmic {BYTES_PER_CELL_LAUNCH} B/cell per launch; "
+                                     "the FP64 step is bound by the FP64 pipe, not HBM"},
+                "clocks": clk, "gpu_launches": 2 * args.steps}
+        if e2e:
+            line["e2e"] = e2e
+        if base:
+            line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line), flush=True)
+    ev.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -35,10 +35,13 @@ __device__ __forceinline__ void extrapolate(const double *__restrict__ qn, long 
 }
 
 /* SemiDiscreteKurganovTadmorScheme.cpp:14-62 with LocalPropagationSpeed.cpp:14-22,
- * SpectralRadius.cpp:14-24 and FluxFunctions.cpp:15-25.  FWD: r = -H, else r += H. */
-template <int NQ, int EOS, int DIR, bool FWD>
-__device__ __forceinline__ void face_flux(const StageArgs &A, long long b, long long st, double ePrev,
-                                          double *__restrict__ r, bool &bad)
+ * SpectralRadius.cpp:14-24 and FluxFunctions.cpp:15-25, for the face between
+ * cells b and b+st along axis dir (1 x, 2 y, 3 eta).  fwd: r = -H, else r += H.
+ * dir and fwd are runtime values so that the six faces of a cell share one copy
+ * of this code (the fully unrolled form overflowed the instruction cache). */
+template <int NQ, int EOS>
+__device__ __forceinline__ void face_flux(const StageArgs &A, long long b, long long st, int dir, bool fwd,
+                                          double ePrev, double *__restrict__ r, bool &bad)
 {
     const double th = A.theta;
     const long long L = A.L;
@@ -50,8 +53,8 @@ __device__ __forceinline__ void face_flux(const StageArgs &A, long long b, long 
     if (NQ == 15) extrapolate(q + 14 * L, b, st, th, PiR, PiL);
     Prim R = infer<EOS>(A.eos, A.t, qRs[0] - qRs[4], qRs[1] - qRs[5], qRs[2] - qRs[6], qRs[3] - qRs[7], PiR, ePrev, bad);
     Prim Lf = infer<EOS>(A.eos, A.t, qLs[0] - qLs[4], qLs[1] - qLs[5], qLs[2] - qLs[6], qLs[3] - qLs[7], PiL, ePrev, bad);
-    const double vR = (DIR == 1) ? R.ux : (DIR == 2) ? R.uy : R.un;
-    const double vL = (DIR == 1) ? Lf.ux : (DIR == 2) ? Lf.uy : Lf.un;
+    const double vR = (dir == 1) ? R.ux : (dir == 2) ? R.uy : R.un;
+    const double vL = (dir == 1) ? Lf.ux : (dir == 2) ? Lf.uy : Lf.un;
     const double rhoLeft = fabs(vL / Lf.ut);
     const double rhoRight = fabs(vR / R.ut);
     const double a = fmax(rhoLeft, rhoRight);
@@ -65,36 +68,36 @@ __device__ __forceinline__ void face_flux(const StageArgs &A, long long b, long 
         double FqL = vL * qL / Lf.ut;
         double res = FqR + FqL - a * (qR - qL);
         res /= 2;
-        if (FWD) r[n] = -res;
-        else r[n] += res;
+        r[n] = fwd ? -res : r[n] + res;
     }
 }
 
 /* SourceTerms.cpp:316-419: sources from d(pi^{tau mu})/dx^i of the T^{tau mu} rows. */
-template <int NQ, int DIR>
-__device__ __forceinline__ void dir_sources(const StageArgs &A, long long s, long long st, double d, double *S)
+template <int NQ>
+__device__ __forceinline__ void dir_sources(const StageArgs &A, long long s, long long st, double d, int dir, double *S)
 {
     const long long L = A.L;
     const double *__restrict__ q = A.qin;
     const double fac = 1 / d / 2;
     const double ut = __ldg(A.uin + s);
-    const double v = __ldg(A.uin + DIR * L + s);
+    const double v = __ldg(A.uin + dir * L + s);
     const double vv = v / ut;
 #define DER(n) ((__ldg(q + (n) * L + s + st) - __ldg(q + (n) * L + s - st)) * fac)
-    if (DIR == 1) {
-        double dpitt = DER(4), dpitx = DER(5), dpity = DER(6), dpitn = DER(7), dpixx = DER(8), dpixy = DER(9), dpixn = DER(10);
+    const double dpitt = DER(4), dpitx = DER(5), dpity = DER(6), dpitn = DER(7);
+    if (dir == 1) {
+        double dpixx = DER(8), dpixy = DER(9), dpixn = DER(10);
         if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpitx - vv * dPi; S[1] = dpitx * vv - dpixx - dPi; }
         else { S[0] = dpitt * vv - dpitx; S[1] = dpitx * vv - dpixx; }
         S[2] = dpity * vv - dpixy;
         S[3] = dpitn * vv - dpixn;
-    } else if (DIR == 2) {
-        double dpitt = DER(4), dpitx = DER(5), dpity = DER(6), dpitn = DER(7), dpixy = DER(9), dpiyy = DER(11), dpiyn = DER(12);
+    } else if (dir == 2) {
+        double dpixy = DER(9), dpiyy = DER(11), dpiyn = DER(12);
         if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpity - vv * dPi; S[2] = dpity * vv - dpiyy - dPi; }
         else { S[0] = dpitt * vv - dpity; S[2] = dpity * vv - dpiyy; }
         S[1] = dpitx * vv - dpixy;
         S[3] = dpitn * vv - dpiyn;
     } else {
-        double dpitt = DER(4), dpitx = DER(5), dpity = DER(6), dpitn = DER(7), dpixn = DER(10), dpiyn = DER(12), dpinn = DER(13);
+        double dpixn = DER(10), dpiyn = DER(12), dpinn = DER(13);
         if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpitn - vv * dPi; S[3] = dpitn * vv - dpinn - dPi / A.t2pow; }
         else { S[0] = dpitt * vv - dpitn; S[3] = dpitn * vv - dpinn; }
         S[1] = dpitx * vv - dpixn;
@@ -103,25 +106,29 @@ __device__ __forceinline__ void dir_sources(const StageArgs &A, long long s, lon
 #undef DER
 }
 
-/* One axis of eulerStepKernelX/Y/Z (FullyDiscreteKurganovTadmorScheme.cpp:300-634). */
-template <int NQ, int EOS, int DIR>
-__device__ __forceinline__ void axis_update(const StageArgs &A, long long s, double ePrev, double *__restrict__ acc, bool &bad)
+/* eulerStepKernelX/Y/Z (FullyDiscreteKurganovTadmorScheme.cpp:300-634), the
+ * axes in the reference's order x, y, eta. */
+template <int NQ, int EOS, bool HAS_Z>
+__device__ __forceinline__ void flux_update(const StageArgs &A, long long s, double ePrev, double *__restrict__ acc, bool &bad)
 {
-    const long long st = (DIR == 1) ? 1 : (DIR == 2) ? (long long)A.ncx : (long long)A.ncx * A.ncy;
-    const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
-    double r[NQ];
-    face_flux<NQ, EOS, DIR, true>(A, s, st, ePrev, r, bad);
-    face_flux<NQ, EOS, DIR, false>(A, s - st, st, ePrev, r, bad);
+#pragma unroll 1
+    for (int dir = 1; dir <= (HAS_Z ? 3 : 2); ++dir) {
+        const long long st = (dir == 1) ? 1 : (dir == 2) ? (long long)A.ncx : (long long)A.ncx * A.ncy;
+        const double d = (dir == 1) ? A.dx : (dir == 2) ? A.dy : A.dz;
+        double r[NQ];
+#pragma unroll 1
+        for (int f = 0; f < 2; ++f) face_flux<NQ, EOS>(A, f == 0 ? s : s - st, st, dir, f == 0, ePrev, r, bad);
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) r[n] /= d;
-    double S[4];
-    dir_sources<NQ, DIR>(A, s, st, d, S);
+        for (int n = 0; n < NQ; ++n) r[n] /= d;
+        double S[4];
+        dir_sources<NQ>(A, s, st, d, dir, S);
 #pragma unroll
-    for (int n = 0; n < 4; ++n) { r[n] += S[n]; r[n] *= A.dt; }
+        for (int n = 0; n < 4; ++n) { r[n] += S[n]; r[n] *= A.dt; }
 #pragma unroll
-    for (int n = 4; n < NQ; ++n) r[n] *= A.dt;
+        for (int n = 4; n < NQ; ++n) r[n] *= A.dt;
 #pragma unroll
-    for (int n = 0; n < NQ; ++n) acc[n] += r[n];
+        for (int n = 0; n < NQ; ++n) acc[n] += r[n];
+    }
 }
 
 /* SourceTerms.cpp:421-612 (USE_APPROX_DERIVATIVE; the dynamical-source arrays
@@ -234,8 +241,12 @@ __device__ __forceinline__ void put_cell(const StageArgs &A, long long d, const 
     A.uout[3 * L + d] = P.un;
 }
 
+#ifndef VH_STAGE_MIN_BLOCKS
+#define VH_STAGE_MIN_BLOCKS 4   /* 128 registers: 16 warps/SM; measured faster than 2-3 blocks at 168-255 */
+#endif
+
 template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
-__global__ void __launch_bounds__(128) kt_stage_kernel(const __grid_constant__ StageArgs A)
+__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_stage_kernel(const __grid_constant__ StageArgs A)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
     const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
@@ -247,11 +258,8 @@ __global__ void __launch_bounds__(128) kt_stage_kernel(const __grid_constant__ S
     bool bad = false;
     double acc[NQ];
     source_update<NQ, EOS>(A, s, acc);
-    axis_update<NQ, EOS, 1>(A, s, ePrev, acc, bad);
-    axis_update<NQ, EOS, 2>(A, s, ePrev, acc, bad);
-    if (HAS_Z) {
-        axis_update<NQ, EOS, 3>(A, s, ePrev, acc, bad);
-    } else {
+    flux_update<NQ, EOS, HAS_Z>(A, s, ePrev, acc, bad);
+    if (!HAS_Z) {
         /* nz = 1: the eta ghosts equal the cell, every eta slope is 0 and the
          * reference's eta pass adds exactly +0.0 (which turns a -0 into +0). */
 #pragma unroll

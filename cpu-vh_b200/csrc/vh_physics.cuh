@@ -93,14 +93,12 @@ __device__ __forceinline__ double approx_deriv(double th, double x, double y, do
 }
 
 /* -------------------------------------------------------- inversion */
-/* EnergyMomentumTensor.cpp:22-115: energy density from M0, M, Pi */
-template <int EOS>
-__device__ double e_from_conserved(const DevEos &E, double ePrev, double M0, double M, double Pi, bool &bad)
+/* EnergyMomentumTensor.cpp:22-111, the tabulated-EoS root solve: Newton from
+ * ePrev, bisection if Newton does not converge.  Kept out of line: it is
+ * called thirteen times per cell and stage, and inlining the loop that often
+ * overflows the instruction cache. */
+static __device__ __noinline__ double e_newton_table(const DevEos &E, double ePrev, double M0, double M, double Pi, bool &bad)
 {
-    if (EOS == 0) {
-        float h = sqrtf(fabsf(__double2float_rn(4 * M0 * M0 - 3 * M)));
-        return (double)fabsf(__double2float_rn((double)h - M0));
-    }
     double e0 = ePrev;
     for (int j = 0; j < 10000; ++j) {                              /* MAX_ITERS_NR */
         double pp = eos_p<1>(E, e0);
@@ -135,6 +133,18 @@ __device__ double e_from_conserved(const DevEos &E, double ePrev, double M0, dou
         else if (f_mid * f_hi < 0.0) { e_lo = e_mid; e_mid = (e_lo + e_hi) / 2.0; }
     }
     return ePrev;
+}
+
+/* EnergyMomentumTensor.cpp:22-115: energy density from M0, M, Pi; the
+ * conformal closed form (:113) truncates through float. */
+template <int EOS>
+__device__ __forceinline__ double e_from_conserved(const DevEos &E, double ePrev, double M0, double M, double Pi, bool &bad)
+{
+    if (EOS == 0) {
+        float h = sqrtf(fabsf(__double2float_rn(4 * M0 * M0 - 3 * M)));
+        return (double)fabsf(__double2float_rn((double)h - M0));
+    }
+    return e_newton_table(E, ePrev, M0, M, Pi, bad);
 }
 
 struct Prim { double e, p, ut, ux, uy, un; };

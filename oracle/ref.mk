@@ -36,11 +36,21 @@ DEFS_stock = -DVH_THETA=1.1 -DVH_EOS_FACTOR=13.8997
 
 all: $(OUT)/libvhref_conf.so $(OUT)/libvhref_table.so $(OUT)/libvhref_stock.so
 
+# DynamicalVariables.cpp is compiled with its setGhostCells renamed away: the
+# reference's version declares its loop indices outside `omp parallel for`
+# (DynamicalVariables.cpp:290-291, :324-325, :358-359), a data race that
+# corrupts cells when more than one thread runs.  ref_harness.cpp supplies the
+# same three loop nests with private indices, so any thread count reproduces
+# the single-thread reference exactly.
+DV = $(REF)/rhic/src/DynamicalVariables.cpp
+SRCS_NO_DV = $(filter-out $(DV),$(SRCS))
+
 $(OUT)/libvhref_%.so: $(SRCS) oracle/ref_shim.h oracle/ref.mk
-	@mkdir -p $(OUT)
-	$(HOSTCXX) $(CXXFLAGS_BASE) $(DEFS_$*) $(SRCS) $(LDFLAGS) -o $@
+	@mkdir -p $(OUT)/obj_$*
+	$(HOSTCXX) $(CXXFLAGS_BASE) $(DEFS_$*) -DsetGhostCells=vhref_setGhostCells_racy -c $(DV) -o $(OUT)/obj_$*/dv.o
+	$(HOSTCXX) $(CXXFLAGS_BASE) $(DEFS_$*) -DVH_RACE_FREE_GHOSTS $(SRCS_NO_DV) $(OUT)/obj_$*/dv.o $(LDFLAGS) -o $@
 
 clean:
-	rm -f $(OUT)/libvhref_*.so
+	rm -rf $(OUT)/libvhref_*.so $(OUT)/obj_*
 
 .PHONY: all clean

@@ -202,6 +202,49 @@ void readInSource(int n, void *latticeParams, void *initCondParams, void *hydroP
 }
 void noSource(void *latticeParams, void *initCondParams) { (void)latticeParams; (void)initCondParams; }
 
+#ifdef VH_RACE_FREE_GHOSTS
+/* DynamicalVariables.cpp:229-276, unchanged, compiled in that file */
+void setGhostCellVars(CONSERVED_VARIABLES *const __restrict__ q, PRECISION *const __restrict__ e,
+                      PRECISION *const __restrict__ p, FLUID_VELOCITY *const __restrict__ u, int s, int sBC);
+
+/* DynamicalVariables.cpp:220-378 with the loop indices private to each
+ * iteration (the original shares s, sBC and iBC/jBC/kBC across OpenMP
+ * threads).  Same loop ranges and order, so the result equals the reference
+ * run on one thread. */
+void setGhostCells(CONSERVED_VARIABLES *const __restrict__ q, PRECISION *const __restrict__ e,
+                   PRECISION *const __restrict__ p, FLUID_VELOCITY *const __restrict__ u, void *latticeParams)
+{
+    struct LatticeParameters *lattice = (struct LatticeParameters *)latticeParams;
+    int nx = lattice->numLatticePointsX, ny = lattice->numLatticePointsY, nz = lattice->numLatticePointsRapidity;
+    int ncx = lattice->numComputationalLatticePointsX, ncy = lattice->numComputationalLatticePointsY;
+    int ncz = lattice->numComputationalLatticePointsRapidity;
+#pragma omp parallel for
+    for (int j = 2; j < ncy; ++j)
+        for (int k = 2; k < ncz; ++k) {
+            for (int i = 0; i <= 1; ++i)
+                setGhostCellVars(q, e, p, u, columnMajorLinearIndex(i, j, k, ncx, ncy, ncz), columnMajorLinearIndex(2, j, k, ncx, ncy, ncz));
+            for (int i = nx + 2; i <= nx + 3; ++i)
+                setGhostCellVars(q, e, p, u, columnMajorLinearIndex(i, j, k, ncx, ncy, ncz), columnMajorLinearIndex(nx + 1, j, k, ncx, ncy, ncz));
+        }
+#pragma omp parallel for
+    for (int i = 2; i < ncx; ++i)
+        for (int k = 2; k < ncz; ++k) {
+            for (int j = 0; j <= 1; ++j)
+                setGhostCellVars(q, e, p, u, columnMajorLinearIndex(i, j, k, ncx, ncy, ncz), columnMajorLinearIndex(i, 2, k, ncx, ncy, ncz));
+            for (int j = ny + 2; j <= ny + 3; ++j)
+                setGhostCellVars(q, e, p, u, columnMajorLinearIndex(i, j, k, ncx, ncy, ncz), columnMajorLinearIndex(i, ny + 1, k, ncx, ncy, ncz));
+        }
+#pragma omp parallel for
+    for (int i = 2; i < ncx; ++i)
+        for (int j = 2; j < ncy; ++j) {
+            for (int k = 0; k <= 1; ++k)
+                setGhostCellVars(q, e, p, u, columnMajorLinearIndex(i, j, k, ncx, ncy, ncz), columnMajorLinearIndex(i, j, 2, ncx, ncy, ncz));
+            for (int k = nz + 2; k <= nz + 3; ++k)
+                setGhostCellVars(q, e, p, u, columnMajorLinearIndex(i, j, k, ncx, ncy, ncz), columnMajorLinearIndex(i, j, nz + 1, ncx, ncy, ncz));
+        }
+}
+#endif
+
 extern "C" {
 
 int vhref_nq(void) { return NUMBER_CONSERVED_VARIABLES; }
