@@ -44,9 +44,9 @@ typedef struct {
     double t;
     double e_reg;
     int nan_flag;
-    /* freezeout slabs */
-    double *fo_e[2], *fo_h[10][2];
-    int fo_calls;
+    /* freezeout slabs: 2 x [11][N] (e, ux, uy, un, e, pixx, pixy, pixn, piyy, piyn, Pi) */
+    double *slab[2];
+    int fo_prev;
 } vho_t;
 
 /* ------------------------------------------------------------------ EoS */
@@ -625,10 +625,7 @@ vho_t *vho_create(int nx, int ny, int nz, double dx, double dy, double dz, doubl
         h->u[c] = (double *)calloc(len, 8); h->up[c] = (double *)calloc(len, 8); h->uS[c] = (double *)calloc(len, 8);
     }
     size_t N = (size_t)nx * ny * nz;
-    for (int s = 0; s < 2; ++s) {
-        h->fo_e[s] = (double *)calloc(N, 8);
-        for (int v = 0; v < 10; ++v) h->fo_h[v][s] = (double *)calloc(N, 8);
-    }
+    for (int s = 0; s < 2; ++s) h->slab[s] = (double *)calloc(11 * N, 8);
     return h;
 }
 
@@ -686,11 +683,8 @@ void vho_set_ic(vho_t *h, const double *e, const double *p, const double *u, con
     ghosts(h, h->q, h->u);
     h->n = 0; h->t = h->t0;
     h->e_reg = eos_e_of_T(h, h->T_reg_GeV / HBARC);
-    h->fo_calls = 0;
-    for (int s = 0; s < 2; ++s) {
-        memset(h->fo_e[s], 0, 8 * N);
-        for (int v = 0; v < 10; ++v) memset(h->fo_h[v][s], 0, 8 * N);
-    }
+    h->fo_prev = 0;
+    for (int s = 0; s < 2; ++s) memset(h->slab[s], 0, 8 * 11 * N);
 }
 
 /* HydroPlugin.cpp:292-307 */
@@ -728,7 +722,7 @@ void vho_destroy(vho_t *h)
     for (int n = 0; n < h->nq; ++n) { free(h->q[n]); free(h->Q[n]); free(h->qS[n]); }
     free(h->e); free(h->p);
     for (int c = 0; c < 4; ++c) { free(h->u[c]); free(h->up[c]); free(h->uS[c]); }
-    for (int s = 0; s < 2; ++s) { free(h->fo_e[s]); for (int v = 0; v < 10; ++v) free(h->fo_h[v][s]); }
+    for (int s = 0; s < 2; ++s) free(h->slab[s]);
     free(h->p_tb); free(h->T_tb);
     free(h);
 }
@@ -737,3 +731,30 @@ void vho_destroy(vho_t *h)
 double vho_fo_eF(vho_t *h) { return eos_e_of_T(h, h->T_fo_GeV / HBARC); }
 double vho_T_of_e(vho_t *h, double ed) { return eos_T(h, ed); }
 double vho_p_of_e(vho_t *h, double ed) { return eos_p(h, ed); }
+
+/* state view for the freezeout driver in cornelius_oracle.c */
+int vho_fo_view(vho_t *h, int *dims, double *spacing, double *t0dt_t, int *n_next, double **e, double **u,
+                double **q, int *nq, double **slabs_prev, double **slabs_cur, double *eF)
+{
+    dims[0] = h->nx; dims[1] = h->ny; dims[2] = h->nz;
+    spacing[0] = h->dt * h->fofac; spacing[1] = h->dx; spacing[2] = h->dy; spacing[3] = h->dz;
+    t0dt_t[0] = h->t0; t0dt_t[1] = h->dt; t0dt_t[2] = h->t;
+    *n_next = h->n + 1;
+    *e = h->e;
+    /* u and q planes are separate allocations; expose them through a packed copy */
+    size_t L = (size_t)h->ncx * h->ncy * h->ncz;
+    static __thread double *pack = NULL;
+    static __thread size_t packlen = 0;
+    size_t need = (4 + (size_t)h->nq) * L;
+    if (packlen < need) { free(pack); pack = (double *)malloc(8 * need); packlen = need; }
+    for (int c = 0; c < 4; ++c) memcpy(pack + c * L, h->u[c], 8 * L);
+    for (int n = 0; n < h->nq; ++n) memcpy(pack + (4 + n) * L, h->q[n], 8 * L);
+    *u = pack;
+    *q = pack + 4 * L;
+    *nq = h->nq;
+    *slabs_prev = h->slab[h->fo_prev];
+    *slabs_cur = h->slab[1 - h->fo_prev];
+    *eF = eos_e_of_T(h, h->T_fo_GeV / HBARC);
+    return 0;
+}
+void vho_fo_flip(vho_t *h) { h->fo_prev = 1 - h->fo_prev; }

@@ -1,0 +1,121 @@
+"""The C oracle against the reference's own sources (oracle/_ref) and
+against the reference's Cornelius known-answer files.
+
+Runs on CPU.  The reference libraries exist only where the reference tree was
+available when __graft_entry__.build() ran; those tests skip elsewhere.  The
+known-answer test uses the committed golden hashes and runs everywhere."""
+import ctypes as C
+import hashlib
+import json
+import os
+import sys
+import tempfile
+
+import numpy as np
+import pytest
+
+import vh
+import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import cornelius_kat as K  # noqa: E402
+
+FIELDS = lambda nq: list(range(nq)) + [100, 101, 102, 103, 200, 201]  # noqa: E731
+
+
+def _same(cfg, a, b):
+    A, B = vh.face_cells(cfg, a), vh.face_cells(cfg, b)
+    return int(np.count_nonzero(A.view(np.uint64) != B.view(np.uint64)))
+
+
+def small_glauber():
+    cfg = vh.glauber_config(21, 19, 7)
+    cfg.dx = cfg.dy = 0.6
+    cfg.dz = 0.5
+    cfg.dt = 0.05
+    rows = vh.synthetic_eos_table()
+    return cfg, rows, vh.glauber_ic(cfg, rows)
+
+
+def small_gubser():
+    cfg = vh.gubser_config(31, 27)
+    return cfg, None, vh.gubser_ic(cfg)
+
+
+@pytest.mark.parametrize("case,variant", [("gubser", "conf"), ("glauber", "table")])
+def test_kt_steps_bitexact_vs_reference(case, variant):
+    if not O.ref_available(variant):
+        pytest.skip("reference build not present")
+    cfg, rows, st = small_gubser() if case == "gubser" else small_glauber()
+    ref = O.RefEvent(variant, cfg, rows, threads=1)
+    orc = O.OracleEvent(cfg, rows)
+    ref.set_initial(st)
+    orc.set_initial(st)
+    for n in (1, 6):
+        ref.step(n)
+        assert orc.step(n) == 0
+        for f in FIELDS(orc.nq):
+            assert _same(cfg, ref.field(f), orc.field(f)) == 0, (case, f)
+
+
+def test_reference_threads_agree_after_ghost_fix():
+    if not O.ref_available("table"):
+        pytest.skip("reference build not present")
+    cfg, rows, st = small_glauber()
+    out = []
+    for th in (1, 4):
+        ref = O.RefEvent("table", cfg, rows, threads=th)
+        ref.set_initial(st)
+        ref.step(5)
+        out.append([ref.field(f) for f in FIELDS(15)])
+    for a, b in zip(*out):
+        assert _same(cfg, a, b) == 0
+
+
+def _parse_surface(path):
+    with open(path) as f:
+        rows = [list(map(float, ln.split())) for ln in f if ln.strip()]
+    return np.array(rows).reshape(-1, 20)
+
+
+@pytest.mark.parametrize("case,variant", [("gubser", "conf"), ("glauber", "table")])
+def test_freezeout_matches_reference(case, variant):
+    if not O.ref_available(variant):
+        pytest.skip("reference build not present")
+    cfg, rows, st = small_gubser() if case == "gubser" else small_glauber()
+    if case == "gubser":
+        cfg.T_freezeout_GeV = 0.2      # a surface that crosses the small grid
+    ref = O.RefEvent(variant, cfg, rows, threads=1)
+    orc = O.OracleEvent(cfg, rows)
+    ref.set_initial(st)
+    orc.set_initial(st)
+    with tempfile.TemporaryDirectory() as d:
+        for blk in range(3):
+            path = os.path.join(d, f"s{blk}.dat")
+            above_ref = ref.freezeout(path)
+            el_orc, above_orc = orc.freezeout()
+            el_ref = _parse_surface(path)
+            assert above_ref == above_orc
+            assert el_ref.shape == el_orc.shape, (blk, el_ref.shape, el_orc.shape)
+            assert el_ref.shape[0] > 0
+            np.testing.assert_array_equal(el_ref.view(np.uint64), el_orc.view(np.uint64))
+            ref.step(cfg.fo_factor)
+            orc.step(cfg.fo_factor)
+
+
+@pytest.mark.parametrize("dim", [3, 4])
+def test_cornelius_known_answers(dim):
+    with open(os.path.join(HERE, "golden", "cornelius_kat.json")) as f:
+        gold = json.load(f)[f"{dim}d"]
+    L = O.oracle_lib()
+    L.vho_cornelius_batch.argtypes = [C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+    cubes = K.random_cubes(dim)
+    out = np.zeros((40000, 2 * dim))
+    counts = np.zeros(len(cubes), dtype=np.int32)
+    dx = np.ones(4)
+    n = L.vho_cornelius_batch(dim, cubes.ctypes.data, len(cubes), 0.5, dx.ctypes.data, out.ctypes.data, len(out),
+                              counts.ctypes.data)
+    assert n == gold["elements"]
+    txt = K.format_elements(out[:n]).encode()
+    assert hashlib.sha256(txt).hexdigest() == gold["sha256"]
