@@ -448,4 +448,58 @@ int vh_event_fetch_surface(vh_event *ev, double *host_out, int cap_elements, int
     return VH_OK;
 }
 
+/* ------------------------------------------------- Cornelius service */
+int vh_cornelius_surfaces(int dim, const double *cubes, int n_cubes, double value0, const double *dx,
+                          double *elements, int cap_elements, int *counts, int *n_elements)
+{
+    if ((dim != 3 && dim != 4) || n_cubes < 0 || !cubes || !dx || !counts) return fail(VH_ERR_ARG, "bad argument");
+    if (n_elements) *n_elements = 0;
+    if (n_cubes == 0) return VH_OK;
+    if (!vh_device_available()) return fail(VH_ERR_NODEVICE, "no CUDA device");
+    const int per = dim == 3 ? 8 : 16;
+    const size_t slot_doubles = (size_t)n_cubes * 10 * 8;
+    double *d_cubes = nullptr, *d_slots = nullptr;
+    int *d_counts = nullptr, *d_err = nullptr;
+    cudaStream_t st = nullptr;
+    int rc = VH_OK;
+    std::vector<double> slots;
+    std::vector<int> cnt;
+#define GO(x) do { cudaError_t e__ = (x); if (e__ != cudaSuccess) { rc = fail(VH_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e__)); goto done; } } while (0)
+    GO(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    GO(cudaMalloc(&d_cubes, (size_t)n_cubes * per * sizeof(double)));
+    GO(cudaMalloc(&d_slots, slot_doubles * sizeof(double)));
+    GO(cudaMalloc(&d_counts, (size_t)n_cubes * sizeof(int)));
+    GO(cudaMalloc(&d_err, sizeof(int)));
+    GO(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+    GO(cudaMemcpyAsync(d_cubes, cubes, (size_t)n_cubes * per * sizeof(double), cudaMemcpyHostToDevice, st));
+    vh::launch_cornelius_batch(dim, d_cubes, n_cubes, value0, dx, d_slots, d_counts, d_err, st);
+    GO(cudaGetLastError());
+    slots.resize(slot_doubles);
+    cnt.resize(n_cubes);
+    int herr;
+    GO(cudaMemcpyAsync(slots.data(), d_slots, slot_doubles * sizeof(double), cudaMemcpyDeviceToHost, st));
+    GO(cudaMemcpyAsync(cnt.data(), d_counts, (size_t)n_cubes * sizeof(int), cudaMemcpyDeviceToHost, st));
+    GO(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GO(cudaStreamSynchronize(st));
+    if (herr) { rc = fail(VH_ERR_CORNELIUS, "Cornelius construction error"); goto done; }
+    {
+        int total = 0;
+        for (int c = 0; c < n_cubes; ++c) {
+            counts[c] = cnt[c];
+            for (int k = 0; k < cnt[c]; ++k) {
+                if (total < cap_elements && elements)
+                    std::memcpy(elements + (size_t)total * 2 * dim, slots.data() + ((size_t)c * 10 + k) * 8, 2 * dim * sizeof(double));
+                total++;
+            }
+        }
+        if (n_elements) *n_elements = total;
+        if (total > cap_elements) rc = fail(VH_ERR_CAPACITY, "element buffer too small");
+    }
+#undef GO
+done:
+    cudaFree(d_cubes); cudaFree(d_slots); cudaFree(d_counts); cudaFree(d_err);
+    if (st) cudaStreamDestroy(st);
+    return rc;
+}
+
 } /* extern "C" */

@@ -98,6 +98,7 @@ _sig("vh_event_stream", C.c_int, [_evp, C.POINTER(C.c_void_p)])
 _sig("vh_event_device_field", C.c_int, [_evp, C.c_int, C.POINTER(C.c_void_p)])
 _sig("vh_event_energy_of_T", C.c_int, [_evp, C.c_double, C.POINTER(C.c_double)])
 _sig("vh_event_powf_misses", C.c_int, [_evp, C.POINTER(C.c_ulonglong)])
+_sig("vh_cornelius_surfaces", C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)])
 _sig("vh_eos_synthetic_table", C.c_int, [C.c_int] + [C.c_double] * 6 + [_dp])
 _sig("vh_eos_eval", C.c_double, [_cfgp, C.c_void_p, C.c_int, C.c_int, C.c_double])
 _sig("vh_ic_gubser", C.c_int, [_cfgp, C.c_double, C.c_double, _dp, _dp, _dp, C.c_void_p])
@@ -286,6 +287,19 @@ class Event:
         e = C.c_double()
         check(lib.vh_event_energy_of_T(self.h, T, C.byref(e)), "vh_event_energy_of_T")
         return e.value
+
+
+def cornelius_surfaces(dim: int, cubes: np.ndarray, value0: float, dx) -> tuple[np.ndarray, np.ndarray]:
+    """Cornelius elements (centroid, normal) of each cube on the device."""
+    cubes = np.ascontiguousarray(cubes, dtype=np.float64).reshape(len(cubes), -1)
+    dxa = np.ascontiguousarray(dx, dtype=np.float64)
+    counts = np.zeros(len(cubes), dtype=np.int32)
+    n = C.c_int()
+    cap = 10 * len(cubes)
+    out = np.zeros((cap, 2 * dim))
+    check(lib.vh_cornelius_surfaces(dim, _ptr(cubes), len(cubes), value0, _ptr(dxa), _ptr(out), cap, _ptr(counts),
+                                    C.byref(n)), "vh_cornelius_surfaces")
+    return out[:n.value], counts
 
 
 def interior(cfg: VhConfig, a: np.ndarray) -> np.ndarray:

@@ -161,6 +161,21 @@ int vh_event_device_field(vh_event *ev, int field, double **d_ptr);
  * (EquationOfState.cpp:201-290); used for e_F and e_reg. */
 int vh_event_energy_of_T(vh_event *ev, double T, double *e_out);
 
+/* Cornelius surface elements of arbitrary cubes on the device, the routine
+ * the freezeout block applies to every lattice cube (freezeout/
+ * cornelius-c++-1.3/cornelius.cpp: Cornelius::find_surface_3d :2161-2237 and
+ * find_surface_4d :2248-2287).  dim 3: 8 corner values per cube in [t][x][y]
+ * order; dim 4: 16 values in [t][x][y][z] order; dx holds dim spacings.
+ * Writes, per element and in cube order, 2*dim doubles (centroid then normal,
+ * as get_centroid_elem/get_normal_elem return them), the element count of
+ * every cube into counts[n_cubes], and the total into *n_elements. */
+int vh_cornelius_surfaces(int dim, const double *cubes, int n_cubes, double value0, const double *dx,
+                          double *elements, int cap_elements, int *counts, int *n_elements);
+
+/* Inputs seen outside the calibrated powf range since creation (diagnostic;
+ * 0 means every temperature matched the host libm exactly). */
+int vh_event_powf_misses(vh_event *ev, unsigned long long *misses);
+
 /* ------------------------------------------------ host-side helpers */
 /* Synthetic crossover EoS table in the binary record layout above:
  * cs^2(T) = 1/3 - dip * exp(-((T - Tc)/w)^2) integrated from T_lo_GeV,
