@@ -31,6 +31,8 @@ static int fail(int code, const std::string &msg)
     g_err = msg;
     return code;
 }
+
+int vh::set_error(int code, const std::string &msg) { return fail(code, msg); }
 #define CUDA_TRY(x)                                                                                   \
     do {                                                                                              \
         cudaError_t e__ = (x);                                                                        \

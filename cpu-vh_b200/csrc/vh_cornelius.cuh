@@ -64,7 +64,7 @@ __device__ __forceinline__ void orient(double *n, const double *out)
 
 /* Square::construct_lines with ends_of_edge and find_outside
  * (cornelius.cpp:1134-1337); appends its lines to w.L. */
-__device__ void square_lines(Work &w, const double P[2][2], int c0, int c1, double v0_, double v1_, double E0, const double *dx)
+static __device__ void square_lines(Work &w, const double P[2][2], int c0, int c1, double v0_, double v1_, double E0, const double *dx)
 {
     int above = 0;
     for (int i = 0; i < 2; i++)
@@ -169,7 +169,7 @@ __device__ __forceinline__ bool poly_add_line(Work &w, Poly &p, int l, bool dono
 
 /* Polygon::calculate_centroid, cornelius.cpp:478-551 (pow(x, 2.0) is x*x:
  * the host libm returns the correctly rounded square) */
-__device__ const double *poly_centroid(Work &w, Poly &p)
+static __device__ const double *poly_centroid(Work &w, Poly &p)
 {
     if (p.have_cen) return p.cen;
     double mean[D] = {0, 0, 0, 0};
@@ -202,7 +202,7 @@ __device__ const double *poly_centroid(Work &w, Poly &p)
 }
 
 /* Polygon::calculate_normal, cornelius.cpp:559-617 */
-__device__ void poly_normal(Work &w, Poly &p, double *normal)
+static __device__ void poly_normal(Work &w, Poly &p, double *normal)
 {
     const double *cen = poly_centroid(w, p);
     for (int i = 0; i < D; i++) normal[i] = 0;
@@ -226,7 +226,7 @@ __device__ void poly_normal(Work &w, Poly &p, double *normal)
 /* Cube::split_to_squares + construct_polygons + check_ambiguous
  * (cornelius.cpp:1502-1650).  Returns the cube's number of lines; its
  * polygons are appended to w.poly, and *ambiguous reports the cube flag. */
-__device__ int cube_polygons(Work &w, const double cube[2][2][2], int const_i, double const_v, double E0,
+static __device__ int cube_polygons(Work &w, const double cube[2][2][2], int const_i, double const_v, double E0,
                              const double *dx, bool *ambiguous)
 {
     int x1 = -1, x2 = -1, x3 = -1;
@@ -278,7 +278,7 @@ __device__ int cube_polygons(Work &w, const double cube[2][2][2], int const_i, d
 /* Cornelius::find_surface_3d for a cube whose corner (i,j,k) spans
  * (tau, x, y); dx3 = {dtau, dx, dy} (cornelius.cpp:2161-2237, init :2087).
  * Element geometry is 4-vectors with component 0 unused. */
-__device__ int surface_3d(Work &w, const double cube[2][2][2], double E0, const double *dx3,
+static __device__ int surface_3d(Work &w, const double cube[2][2][2], double E0, const double *dx3,
                           double cen[][D], double nor[][D])
 {
     int above = 0;
@@ -357,7 +357,7 @@ __device__ __forceinline__ bool hedron_add(Work &w, Hedron &h, int pi, bool dono
 }
 
 /* Polyhedron::calculate_centroid and calculate_normal, cornelius.cpp:842-987 */
-__device__ void hedron_geometry(Work &w, const Hedron &h, double *centroid, double *normal)
+static __device__ void hedron_geometry(Work &w, const Hedron &h, double *centroid, double *normal)
 {
     double mean[D] = {0, 0, 0, 0};
     for (int i = 0; i < h.npoly; i++) {
@@ -406,7 +406,7 @@ __device__ void hedron_geometry(Work &w, const Hedron &h, double *centroid, doub
 
 /* Cornelius::find_surface_4d with the Hypercube construction
  * (cornelius.cpp:1778-1970, :2248-2287). */
-__device__ int surface_4d(Work &w, const double h[2][2][2][2], double E0, const double *dx,
+static __device__ int surface_4d(Work &w, const double h[2][2][2][2], double E0, const double *dx,
                           double cen[][D], double nor[][D])
 {
     int above = 0;

@@ -26,9 +26,6 @@
 
 namespace vh {
 
-constexpr int kScanThreads = 1024;
-constexpr int kScanItems = 4;
-constexpr int kScanChunk = kScanThreads * kScanItems;
 
 static long long cube_count(int nx, int ny, int nz)
 {
@@ -200,7 +197,7 @@ __global__ void scan_apply_kernel(int *data, long long n, const int *bsum, int *
     if (n == 0 && blockIdx.x == 0 && threadIdx.x == 0) { data[0] = 0; if (total) *total = 0; }
 }
 
-static void exclusive_scan(int *data, long long n, int *bsum, int *total, cudaStream_t st)
+void exclusive_scan(int *data, long long n, int *bsum, int *total, cudaStream_t st)
 {
     long long nb = (n + kScanChunk - 1) / kScanChunk;
     if (nb == 0) nb = 1;

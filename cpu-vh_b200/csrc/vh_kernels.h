@@ -77,6 +77,13 @@ void launch_cornelius_batch(int dim, const double *cubes, int n, double v0, cons
                             double *slots, int *counts, int *err, cudaStream_t st);
 size_t freezeout_scratch_ints(int nx, int ny, int nz);
 
+/* exclusive prefix sum of data[0..n) in place, data[n] = total (and *total
+ * if non-null); bsum needs (n + kScanChunk) / kScanChunk + 1 ints */
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanChunk = kScanThreads * kScanItems;
+void exclusive_scan(int *data, long long n, int *bsum, int *total, cudaStream_t st);
+
 } // namespace vh
 
 #endif

@@ -5,6 +5,7 @@
 #ifndef VH_INTERNAL_H
 #define VH_INTERNAL_H
 
+#include <string>
 #include <vector>
 #include "vh_b200.h"
 
@@ -42,6 +43,9 @@ struct PowfQuarterTable {
     std::vector<unsigned> bucket;   /* 65537 offsets into keys by (bits >> 16)    */
 };
 const PowfQuarterTable &powf_quarter_table();
+
+/* records msg as the calling thread's vh_last_error() and returns code */
+int set_error(int code, const std::string &msg);
 
 } // namespace vh
 

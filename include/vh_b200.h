@@ -172,6 +172,27 @@ int vh_event_energy_of_T(vh_event *ev, double T, double *e_out);
 int vh_cornelius_surfaces(int dim, const double *cubes, int n_cubes, double value0, const double *dx,
                           double *elements, int cap_elements, int *counts, int *n_elements);
 
+/* No counterpart in the reference.  The same surface elements as
+ * vh_cornelius_surfaces for callers that cannot let a library allocate device
+ * memory (a host framework whose pool owns the whole GPU, or a loop sharing
+ * the GPU where cudaMalloc's device-wide synchronisation would stall other
+ * streams).  Everything is caller-owned device memory: d_cubes (n_cubes cubes,
+ * layout as above), d_elements (cap_elements x 2*dim doubles, compacted in cube
+ * order), d_counts (n_cubes ints) and d_n_elements (one int: the total, or -1
+ * after a Cornelius construction error); dx is a host array of dim spacings.
+ * Work is queued on `stream` (a cudaStream_t, 0 for the legacy stream) and the
+ * call returns without waiting; read the outputs after synchronising.
+ * The library's working memory is a fixed device array of about 1 MiB held by
+ * every GPU that loads the library, so n_cubes is limited to
+ * VH_NOALLOC_MAX_CUBES (larger batches are rejected with VH_ERR_ARG).  The
+ * first call on each device looks up that array's address with that device
+ * current; make it before any stream capture.  All calls on a device share
+ * the array: calls that overlap on the GPU race. */
+#define VH_NOALLOC_MAX_CUBES 262144
+int vh_cornelius_surfaces_noalloc(int dim, const double *d_cubes, int n_cubes, double value0, const double *dx,
+                                  double *d_elements, int cap_elements, int *d_counts, int *d_n_elements,
+                                  void *stream);
+
 /* Inputs seen outside the calibrated powf range since creation (diagnostic;
  * 0 means every temperature matched the host libm exactly). */
 int vh_event_powf_misses(vh_event *ev, unsigned long long *misses);
