@@ -27,7 +27,7 @@ LDFLAGS = -shared -fopenmp -Wl,-Bsymbolic
 SRC_NAMES = DynamicalVariables EnergyMomentumTensor EquationOfState FileIO FluxFunctions \
             FluxLimiter FullyDiscreteKurganovTadmorScheme HalfSiteExtrapolation HydroPlugin \
             LocalPropagationSpeed SemiDiscreteKurganovTadmorScheme SourceTerms SpectralRadius \
-            Vorticity FiniteDifference
+            Vorticity FiniteDifference LatticeParameters HydroParameters InitialConditionParameters
 SRCS = $(addprefix $(REF)/rhic/src/,$(addsuffix .cpp,$(SRC_NAMES))) oracle/ref_harness.cpp
 
 DEFS_conf  = -DVH_THETA=1.8 -DVH_EOS_FACTOR=15.6269

@@ -41,6 +41,8 @@
 #include "FreezeOut.h"
 #include "HydroPlugin.h"
 #include "LatticeParameters.h"
+#include "HydroParameters.h"
+#include "InitialConditionParameters.h"
 
 /* Defined inside the HydroPlugin.cpp TU (FreezeOut.cpp and Memory.cpp are
  * #included there, HydroPlugin.cpp:21-22). */
@@ -423,6 +425,33 @@ int vhref_freezeout(const char *path)
         callFOFinder2p1D(dim, nx, ny, nz, n, t0, dt, g_t, dx, dy, dz, ls, eF, fo_hc4, fo_hc3, fo_e, fo_h, f, fo_surf, eqnOfState);
     f.close();
     return checkForCellsAboveTc(nx, ny, nz, eF, e);
+}
+
+/* The reference driver end to end from an energy-density vector, initial
+ * condition type 13 (HydroWrapper.cpp:20-23, InitialConditions.cpp:1593). */
+void vhref_run_vector(const char *outdir, const double *e_in, int n)
+{
+    HydroInitialTmunu tm;
+    tm.e_in.assign(e_in, e_in + n);
+    g_ic.initialConditionType = 13;
+    run(&g_lat, &g_ic, &g_hydro, ".", outdir, tm);
+}
+
+/* Loads the harness parameter structs with the reference's own parsers. */
+void vhref_load_conf(const char *dir)
+{
+    readLatticeParameters(dir, &g_lat);
+    readHydroParameters(dir, &g_hydro);
+    readInitialConditionParameters(dir, &g_ic);
+}
+
+/* The reference's own positional parsers (LatticeParameters.cpp:68-157,
+ * HydroParameters.cpp:207-263, InitialConditionParameters.cpp:65-149). */
+void vhref_read_parameters(const char *dir, void *lat, void *hyd, void *ic)
+{
+    readLatticeParameters(dir, lat);
+    readHydroParameters(dir, hyd);
+    readInitialConditionParameters(dir, ic);
 }
 
 /* The reference driver end to end (HydroPlugin.cpp:74-321) on the harness IC;

@@ -1,0 +1,134 @@
+"""Host-side pieces that need no GPU: the C ABI exports, the rhic-conf
+parsers of the C++ drop-in against the reference's own parsers, the host EoS
+against the oracle, and the initial-condition generators."""
+import ctypes as C
+import os
+import re
+import tempfile
+
+import numpy as np
+import pytest
+
+import vh
+import oracle as O
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+
+
+def _declared(header):
+    with open(os.path.join(ROOT, "include", header)) as f:
+        txt = re.sub(r"/\*.*?\*/", "", f.read(), flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(vh_\w+)\s*\(", txt, flags=re.M)))
+
+
+def test_c_abi_exports_every_declared_symbol():
+    names = _declared("vh_b200.h")
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(vh.lib, n)]
+    assert not missing, missing
+
+
+def test_event_create_without_device_fails_cleanly():
+    if vh.lib.vh_device_available():
+        pytest.skip("a GPU is present")
+    cfg = vh.gubser_config(9, 9)
+    with pytest.raises(vh.VhError) as ei:
+        vh.Event(cfg)
+    assert ei.value.code == 7   # VH_ERR_NODEVICE
+
+
+class Lat(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("nx", "ny", "nz", "ncx", "ncy", "ncz", "nt", "fo")] + \
+               [(n, C.c_double) for n in ("dx", "dy", "dz", "dt", "theta")]
+
+
+class Hyd(C.Structure):
+    _fields_ = [("t0", C.c_double), ("etabar", C.c_double), ("TF", C.c_double), ("piNS", C.c_int),
+                ("Treg", C.c_double), ("doFO", C.c_int)]
+
+
+class Ic(C.Structure):
+    _fields_ = [("type", C.c_int), ("A", C.c_int), ("nsrc", C.c_int)] + \
+               [(n, C.c_double) for n in ("e0", "snn", "b", "alpha", "var", "mean")] + [("src", C.c_int)]
+
+
+def _mine(d):
+    lib = C.CDLL(os.path.join(ROOT, "cpu-vh_b200", "libcpu-vh_lib.so"))
+    L, H, I = Lat(), Hyd(), Ic()
+    getattr(lib, "_Z21readLatticeParametersPKcPv")(d.encode(), C.byref(L))
+    getattr(lib, "_Z19readHydroParametersPKcPv")(d.encode(), C.byref(H))
+    getattr(lib, "_Z30readInitialConditionParametersPKcPv")(d.encode(), C.byref(I))
+    return bytes(L), bytes(H), bytes(I)
+
+
+def _theirs(d):
+    lib = C.CDLL(os.path.join(ROOT, "oracle", "_ref", "libvhref_stock.so"))
+    L, H, I = Lat(), Hyd(), Ic()
+    lib.vhref_read_parameters(d.encode(), C.byref(L), C.byref(H), C.byref(I))
+    return bytes(L), bytes(H), bytes(I)
+
+
+@pytest.mark.parametrize("case", ["dropin", "messy"])
+def test_properties_parsers_match_reference(case):
+    if not O.ref_available("stock"):
+        pytest.skip("reference build not present")
+    if case == "dropin":
+        d = os.path.join(HERE, "golden", "dropin_conf")
+        return_dir = d
+    else:
+        return_dir = tempfile.mkdtemp()
+        with open(os.path.join(return_dir, "lattice.properties"), "w") as f:
+            f.write("numLatticePointsX = 131\n  ny=\t131 \nnz=61\n300\ndx = 0.15\ndy=0.15\n\tdz=0.2\ndt=0.015\nFO = 3\nextra=1\n")
+        with open(os.path.join(return_dir, "hydro.properties"), "w") as f:
+            f.write("t0=0.6\r\netas=0.08\r\nTF=0.150\r\npiNS=1\r\nTreg=0.1\r\nFO=0\r\n")
+        with open(os.path.join(return_dir, "ic.properties"), "w") as f:
+            f.write("type=2\nn=0\nA=197\ne0=30\nsnn=42\nb=7.0\nalpha=0.5\nvar=1.69\nmean=3.0\n")
+    assert _mine(return_dir) == _theirs(return_dir)
+
+
+def test_host_eos_matches_oracle():
+    rows = vh.synthetic_eos_table()
+    cfg = vh.glauber_config(9, 9, 3)
+    orc = O.OracleEvent(cfg, rows)
+    xs = np.concatenate([np.geomspace(1e-6, 400.0, 2000), [0.0, 0.0643, 1e-15]])
+    for what, f in ((0, orc.L.vho_eos_p), (1, orc.L.vho_eos_cs2), (2, orc.L.vho_eos_T)):
+        a = np.array([vh.eos_eval(cfg, rows, what, x) for x in xs])
+        b = np.array([f(orc.h, x) for x in xs])
+        np.testing.assert_array_equal(a.view(np.uint64), b.view(np.uint64))
+    for T in (0.05, 0.5, 0.76, 1.2):
+        assert vh.eos_eval(cfg, rows, 3, T) == orc.L.vho_eos_e(orc.h, T)
+    conf = vh.gubser_config(9, 9)
+    oc = O.OracleEvent(conf)
+    for x in np.geomspace(1e-6, 300.0, 500):
+        assert vh.eos_eval(conf, None, 2, x) == oc.L.vho_eos_T(oc.h, x)
+
+
+def test_synthetic_table_is_monotone_and_crossover():
+    rows = vh.synthetic_eos_table()
+    e, p, s, T = rows.T
+    assert np.all(np.diff(e) > 0) and np.all(np.diff(p) > 0) and np.all(np.diff(T) > 0)
+    assert np.allclose(np.diff(e), np.diff(e)[0])
+    cs2 = np.gradient(p, e)
+    Tc = T[np.argmin(cs2[5:-5]) + 5]
+    assert 0.13 < Tc < 0.19 and cs2.min() < 0.2
+
+
+def test_initial_conditions():
+    cfg = vh.glauber_config(41, 41, 11)
+    rows = vh.synthetic_eos_table()
+    st = vh.glauber_ic(cfg, rows)
+    e = st.e.reshape(11, 41, 41)
+    assert np.all(np.isfinite(e)) and e.min() >= 1e-3
+    assert abs(e.max() - (30.0 / vh.HBARC + 1e-3)) < 1e-9
+    np.testing.assert_allclose(e, e[::-1, ::-1, ::-1], rtol=1e-12)   # b along x: point symmetric
+    g = vh.gubser_config(31, 31)
+    sg = vh.gubser_ic(g)
+    c = 15 + 31 * 15
+    T0 = vh.eos_eval(g, None, 2, sg.e[c]) * vh.HBARC
+    assert abs(T0 - 0.3) < 1e-6
+    assert np.all(np.isfinite(sg.pi)) and abs(sg.u[1][c]) == 0.0
+    h1 = vh.hotspot_ic(vh.gubser_config(61, 61), None, seed=7)
+    h2 = vh.hotspot_ic(vh.gubser_config(61, 61), None, seed=7)
+    h3 = vh.hotspot_ic(vh.gubser_config(61, 61), None, seed=8)
+    assert np.array_equal(h1.e, h2.e) and not np.array_equal(h1.e, h3.e)
