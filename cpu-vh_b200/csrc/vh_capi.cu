@@ -126,6 +126,7 @@ static vh::DevEos dev_eos(const vh_event *ev)
     E.e_length = ev->heos.e_length;
     E.e_min = ev->heos.e_min;
     E.e_spacing = ev->heos.e_spacing;
+    E.inv_spacing = 1.0 / ev->heos.e_spacing;
     E.pq.keys = ev->powf.keys;
     E.pq.vals = ev->powf.vals;
     E.pq.bucket = ev->powf.bucket;
@@ -271,6 +272,7 @@ int vh_event_step(vh_event *ev, int nsteps)
     A.L = ev->L;
     A.nx = c.nx; A.ny = c.ny; A.nz = c.nz; A.ncx = ev->ncx; A.ncy = ev->ncy;
     A.dt = c.dt; A.dx = c.dx; A.dy = c.dy; A.dz = c.dz; A.theta = c.theta; A.etabar = c.etabar;
+    A.inv_dx = 1.0 / c.dx; A.inv_dy = 1.0 / c.dy; A.inv_dz = 1.0 / c.dz;
     A.e_reg = ev->e_reg;
     A.eos = dev_eos(ev);
     A.zeta.law = c.zeta_law; A.zeta.norm = c.zeta_norm; A.zeta.T0 = c.zeta_T0_GeV; A.zeta.w = c.zeta_width_GeV;
@@ -284,14 +286,14 @@ int vh_event_step(vh_event *ev, int nsteps)
         A.ein = ev->ep[ev->ec]; A.pin = ev->ep[ev->ec] + ev->L;
         A.eout = ev->ep[1 - ev->ec]; A.pout = ev->ep[1 - ev->ec] + ev->L;
         A.uin = ev->u[ev->uc]; A.upin = ev->u[ev->up]; A.uout = ev->u[ev->us];
-        A.t = t; A.t2pow = pow(t, 2); A.t_inf = t1;
+        A.t = t; A.t2pow = pow(t, 2); A.t_inf = t1; A.inv_t = 1.0 / t;
         vh::launch_stage(A, ev->nq, c.eos_kind, ev->stream);
         /* stage 2: qS -> Q, convex with q; u(new) goes to the old up buffer */
         A.qin = ev->q[ev->qs]; A.qout = ev->q[ev->qn]; A.qbase = ev->q[ev->qc];
         A.ein = ev->ep[1 - ev->ec]; A.pin = ev->ep[1 - ev->ec] + ev->L;
         A.eout = ev->ep[ev->ec]; A.pout = ev->ep[ev->ec] + ev->L;
         A.uin = ev->u[ev->us]; A.upin = ev->u[ev->uc]; A.uout = ev->u[ev->up];
-        A.t = t1; A.t2pow = pow(t1, 2); A.t_inf = t1;
+        A.t = t1; A.t2pow = pow(t1, 2); A.t_inf = t1; A.inv_t = 1.0 / t1;
         vh::launch_stage(A, ev->nq, c.eos_kind, ev->stream);
         std::swap(ev->qc, ev->qn);
         std::swap(ev->uc, ev->up);
@@ -447,6 +449,36 @@ int vh_event_fetch_surface(vh_event *ev, double *host_out, int cap_elements, int
     CUDA_TRY(cudaMemcpyAsync(host_out, ev->fo_elems, (size_t)ev->fo_count * VH_FO_COLUMNS * sizeof(double),
                              cudaMemcpyDeviceToHost, ev->stream));
     CUDA_TRY(cudaStreamSynchronize(ev->stream));
+    return VH_OK;
+}
+
+/* ------------------------------------------------- device math check */
+int vh_device_math_check(int which, const double *a, const double *b, int n, double *out)
+{
+    if (which < 0 || which > 3 || n < 0 || !a || !out || ((which == 1 || which == 2) && !b)) return fail(VH_ERR_ARG, "bad argument");
+    if (n == 0) return VH_OK;
+    if (!vh_device_available()) return fail(VH_ERR_NODEVICE, "no CUDA device");
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    DevPowf pw;
+    vh::PowfTab pq{};
+    if (which == 3) {
+        int rc = device_powf(dev, &pw);
+        if (rc != VH_OK) return rc;
+        pq.keys = pw.keys; pq.vals = pw.vals; pq.bucket = pw.bucket; pq.hb0 = pw.hb0; pq.hb1 = pw.hb1; pq.miss = nullptr;
+    }
+    double *d = nullptr;
+    const size_t B = (size_t)n * sizeof(double);
+    CUDA_TRY(cudaMalloc(&d, 3 * B));
+    cudaError_t e = cudaMemcpy(d, a, B, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && b) e = cudaMemcpy(d + n, b, B, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        vh::launch_math_check(which, d, d + n, n, d + 2 * (size_t)n, pq, 0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + 2 * (size_t)n, B, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(VH_ERR_CUDA, std::string("vh_device_math_check: ") + cudaGetErrorString(e));
     return VH_OK;
 }
 

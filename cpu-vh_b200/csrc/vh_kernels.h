@@ -28,6 +28,8 @@ struct StageArgs {
     double t2pow;          /* pow(t, 2) from the host libm (SourceTerms.cpp:415, :587) */
     double t_inf;          /* time of the inference and regulation (t after t += dt)   */
     double dt, dx, dy, dz, theta, etabar, e_reg;
+    double inv_dx, inv_dy, inv_dz;   /* RN(1/dx) etc. for div_rcp                      */
+    double inv_t;          /* RN(1/t)                                                  */
     int step;              /* step index for error reports                             */
     DevEos eos;
     Zeta zeta;
@@ -44,6 +46,7 @@ struct InitArgs {
 };
 
 void launch_init(const InitArgs &a, cudaStream_t s);
+void launch_math_check(int which, const double *a, const double *b, int n, double *out, const PowfTab &pq, cudaStream_t s);
 void launch_stage(const StageArgs &a, int nq, int eos_kind, cudaStream_t s);
 
 /* ---- freezeout ---- */

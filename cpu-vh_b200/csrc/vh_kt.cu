@@ -58,14 +58,15 @@ __device__ __forceinline__ void face_flux(const StageArgs &A, long long b, long 
     const double rhoLeft = fabs(vL / Lf.ut);
     const double rhoRight = fabs(vR / R.ut);
     const double a = fmax(rhoLeft, rhoRight);
+    const double yR = 1.0 / R.ut, yL = 1.0 / Lf.ut;   /* one reciprocal per state, exact quotients via div_rcp */
 #pragma unroll
     for (int n = 0; n < NQ; ++n) {
         double qR, qL;
         if (n < 8) { qR = qRs[n]; qL = qLs[n]; }
         else if (n == 14) { qR = PiR; qL = PiL; }
         else extrapolate(q + n * L, b, st, th, qR, qL);
-        double FqR = vR * qR / R.ut;
-        double FqL = vL * qL / Lf.ut;
+        double FqR = div_rcp(vR * qR, R.ut, yR);
+        double FqL = div_rcp(vL * qL, Lf.ut, yL);
         double res = FqR + FqL - a * (qR - qL);
         res /= 2;
         r[n] = fwd ? -res : r[n] + res;
@@ -115,11 +116,12 @@ __device__ __forceinline__ void flux_update(const StageArgs &A, long long s, dou
     for (int dir = 1; dir <= (HAS_Z ? 3 : 2); ++dir) {
         const long long st = (dir == 1) ? 1 : (dir == 2) ? (long long)A.ncx : (long long)A.ncx * A.ncy;
         const double d = (dir == 1) ? A.dx : (dir == 2) ? A.dy : A.dz;
+        const double yd = (dir == 1) ? A.inv_dx : (dir == 2) ? A.inv_dy : A.inv_dz;
         double r[NQ];
 #pragma unroll 1
         for (int f = 0; f < 2; ++f) face_flux<NQ, EOS>(A, f == 0 ? s : s - st, st, dir, f == 0, ePrev, r, bad);
 #pragma unroll
-        for (int n = 0; n < NQ; ++n) r[n] /= d;
+        for (int n = 0; n < NQ; ++n) r[n] = div_rcp(r[n], d, yd);
         double S[4];
         dir_sources<NQ>(A, s, st, d, dir, S);
 #pragma unroll
@@ -148,35 +150,37 @@ __device__ __forceinline__ void source_update(const StageArgs &A, long long s, d
                  *__restrict__ unv = A.uin + 3 * L, *__restrict__ pv = A.pin;
     const double e = __ldg(A.ein + s), p = __ldg(pv + s);
     const double ut = __ldg(utv + s), ux = __ldg(uxv + s), uy = __ldg(uyv + s), un = __ldg(unv + s);
-    const double dxut = approx_deriv(th, __ldg(utv + s - sx), ut, __ldg(utv + s + sx)) / A.dx;
-    const double dxux = approx_deriv(th, __ldg(uxv + s - sx), ux, __ldg(uxv + s + sx)) / A.dx;
-    const double dxuy = approx_deriv(th, __ldg(uyv + s - sx), uy, __ldg(uyv + s + sx)) / A.dx;
-    const double dxun = approx_deriv(th, __ldg(unv + s - sx), un, __ldg(unv + s + sx)) / A.dx;
-    const double dyut = approx_deriv(th, __ldg(utv + s - sy), ut, __ldg(utv + s + sy)) / A.dy;
-    const double dyux = approx_deriv(th, __ldg(uxv + s - sy), ux, __ldg(uxv + s + sy)) / A.dy;
-    const double dyuy = approx_deriv(th, __ldg(uyv + s - sy), uy, __ldg(uyv + s + sy)) / A.dy;
-    const double dyun = approx_deriv(th, __ldg(unv + s - sy), un, __ldg(unv + s + sy)) / A.dy;
-    const double dnut = approx_deriv(th, __ldg(utv + s - sz), ut, __ldg(utv + s + sz)) / A.dz;
-    const double dnux = approx_deriv(th, __ldg(uxv + s - sz), ux, __ldg(uxv + s + sz)) / A.dz;
-    const double dnuy = approx_deriv(th, __ldg(uyv + s - sz), uy, __ldg(uyv + s + sz)) / A.dz;
-    const double dnun = approx_deriv(th, __ldg(unv + s - sz), un, __ldg(unv + s + sz)) / A.dz;
-    const double dxp = approx_deriv(th, __ldg(pv + s - sx), p, __ldg(pv + s + sx)) / A.dx;
-    const double dyp = approx_deriv(th, __ldg(pv + s - sy), p, __ldg(pv + s + sy)) / A.dy;
-    const double dnp = approx_deriv(th, __ldg(pv + s - sz), p, __ldg(pv + s + sz)) / A.dz;
+    const double dxut = div_rcp(approx_deriv(th, __ldg(utv + s - sx), ut, __ldg(utv + s + sx)), A.dx, A.inv_dx);
+    const double dxux = div_rcp(approx_deriv(th, __ldg(uxv + s - sx), ux, __ldg(uxv + s + sx)), A.dx, A.inv_dx);
+    const double dxuy = div_rcp(approx_deriv(th, __ldg(uyv + s - sx), uy, __ldg(uyv + s + sx)), A.dx, A.inv_dx);
+    const double dxun = div_rcp(approx_deriv(th, __ldg(unv + s - sx), un, __ldg(unv + s + sx)), A.dx, A.inv_dx);
+    const double dyut = div_rcp(approx_deriv(th, __ldg(utv + s - sy), ut, __ldg(utv + s + sy)), A.dy, A.inv_dy);
+    const double dyux = div_rcp(approx_deriv(th, __ldg(uxv + s - sy), ux, __ldg(uxv + s + sy)), A.dy, A.inv_dy);
+    const double dyuy = div_rcp(approx_deriv(th, __ldg(uyv + s - sy), uy, __ldg(uyv + s + sy)), A.dy, A.inv_dy);
+    const double dyun = div_rcp(approx_deriv(th, __ldg(unv + s - sy), un, __ldg(unv + s + sy)), A.dy, A.inv_dy);
+    const double dnut = div_rcp(approx_deriv(th, __ldg(utv + s - sz), ut, __ldg(utv + s + sz)), A.dz, A.inv_dz);
+    const double dnux = div_rcp(approx_deriv(th, __ldg(uxv + s - sz), ux, __ldg(uxv + s + sz)), A.dz, A.inv_dz);
+    const double dnuy = div_rcp(approx_deriv(th, __ldg(uyv + s - sz), uy, __ldg(uyv + s + sz)), A.dz, A.inv_dz);
+    const double dnun = div_rcp(approx_deriv(th, __ldg(unv + s - sz), un, __ldg(unv + s + sz)), A.dz, A.inv_dz);
+    const double dxp = div_rcp(approx_deriv(th, __ldg(pv + s - sx), p, __ldg(pv + s + sx)), A.dx, A.inv_dx);
+    const double dyp = div_rcp(approx_deriv(th, __ldg(pv + s - sy), p, __ldg(pv + s + sy)), A.dy, A.inv_dy);
+    const double dnp = div_rcp(approx_deriv(th, __ldg(pv + s - sz), p, __ldg(pv + s + sz)), A.dz, A.inv_dz);
     const double t = A.t;
     /* Tnn(e, p + Pi, un, pinn, t), EnergyMomentumTensor.cpp:328-330 */
     const double pP = p + Pi;
-    const double tnn = (e + pP) * un * un + pP / t / t + Qv[13];
-    const double vx = ux / ut, vy = uy / ut, vn = un / ut;
-    const double dxvx = (dxux - vx * dxut) / ut;
-    const double dyvy = (dyuy - vy * dyut) / ut;
-    const double dnvn = (dnun - vn * dnut) / ut;
+    const double yt = A.inv_t;
+    const double tnn = (e + pP) * un * un + div_rcp(div_rcp(pP, t, yt), t, yt) + Qv[13];
+    const double yut = 1.0 / ut;
+    const double vx = div_rcp(ux, ut, yut), vy = div_rcp(uy, ut, yut), vn = div_rcp(un, ut, yut);
+    const double dxvx = div_rcp(dxux - vx * dxut, ut, yut);
+    const double dyvy = div_rcp(dyuy - vy * dyut, ut, yut);
+    const double dnvn = div_rcp(dnun - vn * dnut, ut, yut);
     const double dkvk = dxvx + dyvy + dnvn;
     double S[NQ];
-    S[0] = 0.0 - (Qv[0] / t + t * tnn) + dkvk * (Qv[4] - p - Pi) - vx * dxp - vy * dyp - vn * dnp;
-    S[1] = 0.0 - Qv[1] / t - dxp + dkvk * Qv[5];
-    S[2] = 0.0 - Qv[2] / t - dyp + dkvk * Qv[6];
-    S[3] = 0.0 - 3 * Qv[3] / t - dnp / A.t2pow + dkvk * Qv[7];
+    S[0] = 0.0 - (div_rcp(Qv[0], t, yt) + t * tnn) + dkvk * (Qv[4] - p - Pi) - vx * dxp - vy * dyp - vn * dnp;
+    S[1] = 0.0 - div_rcp(Qv[1], t, yt) - dxp + dkvk * Qv[5];
+    S[2] = 0.0 - div_rcp(Qv[2], t, yt) - dyp + dkvk * Qv[6];
+    S[3] = 0.0 - div_rcp(3 * Qv[3], t, yt) - dnp / A.t2pow + dkvk * Qv[7];
     pimunu_rhs<EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, e, p, ut, ux, uy, un,
                               __ldg(A.upin + s), __ldg(A.upin + L + s), __ldg(A.upin + 2 * L + s), __ldg(A.upin + 3 * L + s),
                               Qv + 4, Pi, dxut, dyut, dnut, dxux, dyux, dnux, dxuy, dyuy, dnuy, dxun, dyun, dnun, dkvk,
@@ -321,6 +325,25 @@ __global__ void init_kernel(const __grid_constant__ InitArgs A)
     if (jj == A.ny + 1) { put(s + A.ncx); put(s + 2 * A.ncx); }
     if (kk == 2) { put(s - sxy); put(s - 2 * sxy); }
     if (kk == A.nz + 1) { put(s + sxy); put(s + 2 * sxy); }
+}
+
+/* device math self-check: 0 vh_tanh(a), 1 div_rcp(a, b, RN(1/b)), 2 IEEE a/b,
+ * 3 powf_quarter(float(a)) */
+__global__ void math_check_kernel(int which, const double *a, const double *b, int n, double *out, PowfTab pq)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double x = a[i], r;
+    if (which == 0) r = vh_tanh(x);
+    else if (which == 1) { double y = b[i]; r = div_rcp(x, y, 1.0 / y); }
+    else if (which == 2) r = x / b[i];
+    else r = (double)powf_quarter(__double2float_rn(x), pq);
+    out[i] = r;
+}
+
+void launch_math_check(int which, const double *a, const double *b, int n, double *out, const PowfTab &pq, cudaStream_t s)
+{
+    math_check_kernel<<<(n + 255) / 256, 256, 0, s>>>(which, a, b, n, out, pq);
 }
 
 void launch_init(const InitArgs &a, cudaStream_t s)

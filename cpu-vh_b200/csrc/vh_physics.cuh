@@ -24,6 +24,7 @@ struct DevEos {
     const double *T_tb;       /* tabulated T(e) [fm^-1] */
     int e_length;
     double e_min, e_spacing;
+    double inv_spacing;       /* RN(1/e_spacing), for div_rcp */
     PowfTab pq;               /* host-exact powf(x, 0.25) */
 };
 
@@ -38,14 +39,34 @@ __device__ __forceinline__ void raise_error(const DevErr &E, int code, long long
     if (atomicCAS(E.code, 0, code) == 0) { *E.cell = cell; *E.step = step; }
 }
 
+/* ---------------------------------------------- division, shared divisor */
+/* IEEE a/b, kept out of line: the fallback of div_rcp */
+static __device__ __noinline__ double div_ieee(double a, double b) { return a / b; }
+
+/* The correctly rounded quotient a/b given y = RN(1/b), by Markstein's
+ * theorem (P. Markstein, IBM J. Res. Dev. 34(1), 1990; Muller et al.,
+ * Handbook of Floating-Point Arithmetic, ch. 4): q0 = RN(a*y) is within one
+ * ulp of a/b, r = a - q0*b is exact with an FMA, and RN(q0 + r*y) = RN(a/b).
+ * One reciprocal then serves every division by the same b at the cost of a
+ * multiply and two FMAs each -- bit-identical to `a / b`.  Zero, non-finite,
+ * huge or near-subnormal operands, where the exactness argument needs more
+ * care, take the IEEE division. */
+__device__ __forceinline__ double div_rcp(double a, double b, double y)
+{
+    const double q0 = a * y;
+    if (!(fabs(q0) >= 0x1p-960 && fabs(q0) <= 0x1p1000 && fabs(a) >= 0x1p-960)) return div_ieee(a, b);
+    const double r = fma(-q0, b, a);
+    return fma(r, y, q0);
+}
+
 /* ------------------------------------------------------------------ EoS */
 /* EquationOfState.cpp:329-360 */
 __device__ __forceinline__ double eos_interp(const DevEos &E, double ed, const double *tb)
 {
-    int idx = (int)((ed - E.e_min) / E.e_spacing);
+    int idx = (int)div_rcp(ed - E.e_min, E.e_spacing, E.inv_spacing);
     idx = (E.e_length - 2 < idx) ? E.e_length - 2 : idx;   /* std::min(N_e - 2, idx) */
     idx = (idx < 0) ? 0 : idx;                              /* std::max(0, idx)       */
-    const double frac = (ed - (idx * E.e_spacing + E.e_min)) / E.e_spacing;
+    const double frac = div_rcp(ed - (idx * E.e_spacing + E.e_min), E.e_spacing, E.inv_spacing);
     return __ldg(tb + idx) * (1. - frac) + __ldg(tb + idx + 1) * frac;
 }
 /* std::max(1.e-15, f): (1e-15 < f) ? f : 1e-15 */
@@ -213,7 +234,8 @@ __device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, double *rhs, double t
     double tauPiInv = 0.0;
     if (BULK) tauPiInv = 15 * a2 * T / zeta_over_s(Z, T);
     double ut2 = ut * ut, un2 = un * un, t2 = t * t, t3 = t * t2;
-    double dtut = (ut - utp) / d_dt, dtux = (ux - uxp) / d_dt, dtuy = (uy - uyp) / d_dt, dtun = (un - unp) / d_dt;
+    const double kThird = 1.0 / 3.0, yut = 1.0 / ut, ydt = 1.0 / d_dt;
+    double dtut = div_rcp((ut - utp), d_dt, ydt), dtux = div_rcp((ux - uxp), d_dt, ydt), dtuy = div_rcp((uy - uyp), d_dt, ydt), dtun = div_rcp((un - unp), d_dt, ydt);
     double Dut = ut * dtut + ux * dxut + uy * dyut + un * dnut + t * un * un;
     double DuxUpper = ut * dtux + ux * dxux + uy * dyux + un * dnux;
     double Dux = -DuxUpper;
@@ -226,16 +248,16 @@ __device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, double *rhs, double t
     double duy = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
     double dun = ut * dtun + ux * dxun + uy * dyun + un * dnun;
     double theta = ut / t + dtut + dxux + dyuy + dnun;
-    double stt = -t * ut * un2 + (dtut - ut * dut) + (ut2 - 1) * theta / 3.0;
-    double stx = -(t * un2 * ux) / 2.0 + (dtux - dxut) / 2.0 - (ux * dut + ut * dux) / 2.0 + ut * ux * theta / 3.0;
-    double sty = -(t * un2 * uy) / 2.0 + (dtuy - dyut) / 2.0 - (uy * dut + ut * duy) / 2.0 + ut * uy * theta / 3.0;
-    double stn = -un * (2.0 * ut2 + t2 * un2) / (2.0 * t) + (dtun - dnut / t2) / 2.0 - (un * dut + ut * dun) / 2.0 + ut * un * theta / 3.0;
-    double sxx = -(dxux + ux * dux) + (1.0 + ux * ux) * theta / 3.0;
-    double sxy = -(dxuy + dyux) / 2.0 - (uy * dux + ux * duy) / 2.0 + ux * uy * theta / 3.0;
-    double sxn = -ut * ux * un / t - (dxun + dnux / t2) / 2.0 - (un * dux + ux * dun) / 2.0 + ux * un * theta / 3.0;
-    double syy = -(dyuy + uy * duy) + (1.0 + uy * uy) * theta / 3.0;
-    double syn = -ut * uy * un / t - (dyun + dnuy / t2) / 2.0 - (un * duy + uy * dun) / 2.0 + uy * un * theta / 3.0;
-    double snn = -ut * (1.0 + 2.0 * t2 * un2) / t3 - dnun / t2 - un * dun + (1.0 / t2 + un2) * theta / 3.0;
+    double stt = -t * ut * un2 + (dtut - ut * dut) + div_rcp((ut2 - 1) * theta, 3.0, kThird);
+    double stx = -(t * un2 * ux) / 2.0 + (dtux - dxut) / 2.0 - (ux * dut + ut * dux) / 2.0 + div_rcp(ut * ux * theta, 3.0, kThird);
+    double sty = -(t * un2 * uy) / 2.0 + (dtuy - dyut) / 2.0 - (uy * dut + ut * duy) / 2.0 + div_rcp(ut * uy * theta, 3.0, kThird);
+    double stn = -un * (2.0 * ut2 + t2 * un2) / (2.0 * t) + (dtun - dnut / t2) / 2.0 - (un * dut + ut * dun) / 2.0 + div_rcp(ut * un * theta, 3.0, kThird);
+    double sxx = -(dxux + ux * dux) + div_rcp((1.0 + ux * ux) * theta, 3.0, kThird);
+    double sxy = -(dxuy + dyux) / 2.0 - (uy * dux + ux * duy) / 2.0 + div_rcp(ux * uy * theta, 3.0, kThird);
+    double sxn = -ut * ux * un / t - (dxun + dnux / t2) / 2.0 - (un * dux + ux * dun) / 2.0 + div_rcp(ux * un * theta, 3.0, kThird);
+    double syy = -(dyuy + uy * duy) + div_rcp((1.0 + uy * uy) * theta, 3.0, kThird);
+    double syn = -ut * uy * un / t - (dyun + dnuy / t2) / 2.0 - (un * duy + uy * dun) / 2.0 + div_rcp(uy * un * theta, 3.0, kThird);
+    double snn = -ut * (1.0 + 2.0 * t2 * un2) / t3 - dnun / t2 - un * dun + div_rcp((1.0 / t2 + un2) * theta, 3.0, kThird);
     double wtx = (-dtux - dxut + ut * dux - ux * dut - t * un2 * ux) / 2.0;
     double wty = (-dtuy - dyut + ut * duy - uy * dut - t * un2 * uy) / 2.0;
     double wtn = (-t2 * dtun - 2.0 * t * un - dnut - ut * Dun - t2 * un * dut - t3 * un * un2) / 2.0;
@@ -267,16 +289,16 @@ __device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, double *rhs, double t
     double I3nn = 2.0 * (pitn * wnt + pixn * wnx + piyn * wny);
     double ux2 = ux * ux, uy2 = uy * uy;
     double ps = pitt * stt - 2.0 * pitx * stx - 2.0 * pity * sty + pixx * sxx + 2.0 * pixy * sxy + piyy * syy - 2.0 * pitn * stn * t2 + 2.0 * pixn * sxn * t2 + 2.0 * piyn * syn * t2 + pinn * snn * t2 * t2;
-    double I4tt = (pitt * stt - pitx * stx - pity * sty - t2 * pitn * stn) - (1.0 - ut2) * ps / 3.0;
-    double I4tx = (pitt * stx + pitx * stt) / 2.0 - (pitx * sxx + pixx * stx) / 2.0 - (pity * sxy + pixy * sty) / 2.0 - t2 * (pitn * sxn + pixn * stn) / 2.0 + (ut * ux) * ps / 3.0;
-    double I4ty = (pitt * sty + pity * stt) / 2.0 - (pitx * sxy + pixy * stx) / 2.0 - (pity * syy + piyy * sty) / 2.0 - t2 * (pitn * syn + piyn * stn) / 2.0 + (ut * uy) * ps / 3.0;
-    double I4tn = (pitt * stn + pitn * stt) / 2.0 - (pitx * sxn + pixn * stx) / 2.0 - (pity * syn + piyn * sty) / 2.0 - t2 * (pitn * snn + pinn * stn) / 2.0 + (ut * un) * ps / 3.0;
-    double I4xx = (pitx * stx - pixx * sxx - pixy * sxy - t2 * pixn * sxn) + (1.0 + ux2) * ps / 3.0;
-    double I4xy = (pitx * sty + pity * stx) / 2.0 - (pixx * sxy + pixy * sxx) / 2.0 - (pixy * syy + piyy * sxy) / 2.0 - t2 * (pixn * syn + piyn * sxn) / 2.0 + (ux * uy) * ps / 3.0;
-    double I4xn = (pitx * stn + pitn * stx) / 2.0 - (pixx * sxn + pixn * sxx) / 2.0 - (pixy * syn + piyn * sxy) / 2.0 - t2 * (pixn * snn + pinn * sxn) / 2.0 + (ux * un) * ps / 3.0;
-    double I4yy = (pity * sty - pixy * sxy - piyy * syy - t2 * piyn * syn) + (1.0 + uy2) * ps / 3.0;
-    double I4yn = (pity * stn + pitn * sty) / 2.0 - (pixy * sxn + pixn * sxy) / 2.0 - (piyy * syn + piyn * syy) / 2.0 - t2 * (piyn * snn + pinn * syn) / 2.0 + (uy * un) * ps / 3.0;
-    double I4nn = (pitn * stn - pixn * sxn - piyn * syn - t2 * pinn * snn) + (1.0 / t2 + un2) * ps / 3.0;
+    double I4tt = (pitt * stt - pitx * stx - pity * sty - t2 * pitn * stn) - div_rcp((1.0 - ut2) * ps, 3.0, kThird);
+    double I4tx = (pitt * stx + pitx * stt) / 2.0 - (pitx * sxx + pixx * stx) / 2.0 - (pity * sxy + pixy * sty) / 2.0 - t2 * (pitn * sxn + pixn * stn) / 2.0 + div_rcp((ut * ux) * ps, 3.0, kThird);
+    double I4ty = (pitt * sty + pity * stt) / 2.0 - (pitx * sxy + pixy * stx) / 2.0 - (pity * syy + piyy * sty) / 2.0 - t2 * (pitn * syn + piyn * stn) / 2.0 + div_rcp((ut * uy) * ps, 3.0, kThird);
+    double I4tn = (pitt * stn + pitn * stt) / 2.0 - (pitx * sxn + pixn * stx) / 2.0 - (pity * syn + piyn * sty) / 2.0 - t2 * (pitn * snn + pinn * stn) / 2.0 + div_rcp((ut * un) * ps, 3.0, kThird);
+    double I4xx = (pitx * stx - pixx * sxx - pixy * sxy - t2 * pixn * sxn) + div_rcp((1.0 + ux2) * ps, 3.0, kThird);
+    double I4xy = (pitx * sty + pity * stx) / 2.0 - (pixx * sxy + pixy * sxx) / 2.0 - (pixy * syy + piyy * sxy) / 2.0 - t2 * (pixn * syn + piyn * sxn) / 2.0 + div_rcp((ux * uy) * ps, 3.0, kThird);
+    double I4xn = (pitx * stn + pitn * stx) / 2.0 - (pixx * sxn + pixn * sxx) / 2.0 - (pixy * syn + piyn * sxy) / 2.0 - t2 * (pixn * snn + pinn * sxn) / 2.0 + div_rcp((ux * un) * ps, 3.0, kThird);
+    double I4yy = (pity * sty - pixy * sxy - piyy * syy - t2 * piyn * syn) + div_rcp((1.0 + uy2) * ps, 3.0, kThird);
+    double I4yn = (pity * stn + pitn * sty) / 2.0 - (pixy * sxn + pixn * sxy) / 2.0 - (piyy * syn + piyn * syy) / 2.0 - t2 * (piyn * snn + pinn * syn) / 2.0 + div_rcp((uy * un) * ps, 3.0, kThird);
+    double I4nn = (pitn * stn - pixn * sxn - piyn * syn - t2 * pinn * snn) + div_rcp((1.0 / t2 + un2) * ps, 3.0, kThird);
     double Itt = I1tt + delta_pipi * I2tt - I3tt + tau_pipi * I4tt - lambda_piPi * Pi * stt;
     double Itx = I1tx + delta_pipi * I2tx - I3tx + tau_pipi * I4tx - lambda_piPi * Pi * stx;
     double Ity = I1ty + delta_pipi * I2ty - I3ty + tau_pipi * I4ty - lambda_piPi * Pi * sty;
@@ -297,19 +319,19 @@ __device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, double *rhs, double t
     double dpiyy = 2.0 * beta_pi * syy - piyy * taupiInv - Iyy;
     double dpiyn = 2.0 * beta_pi * syn - piyn * taupiInv - Iyn - (ut * piyn + un * pity) / t;
     double dpinn = 2.0 * beta_pi * snn - pinn * taupiInv - Inn - 2 * (ut * pinn + un * pitn) / t;
-    rhs[0] = dpitt / ut + pitt * dkvk;
-    rhs[1] = dpitx / ut + pitx * dkvk;
-    rhs[2] = dpity / ut + pity * dkvk;
-    rhs[3] = dpitn / ut + pitn * dkvk;
-    rhs[4] = dpixx / ut + pixx * dkvk;
-    rhs[5] = dpixy / ut + pixy * dkvk;
-    rhs[6] = dpixn / ut + pixn * dkvk;
-    rhs[7] = dpiyy / ut + piyy * dkvk;
-    rhs[8] = dpiyn / ut + piyn * dkvk;
-    rhs[9] = dpinn / ut + pinn * dkvk;
+    rhs[0] = div_rcp(dpitt, ut, yut) + pitt * dkvk;
+    rhs[1] = div_rcp(dpitx, ut, yut) + pitx * dkvk;
+    rhs[2] = div_rcp(dpity, ut, yut) + pity * dkvk;
+    rhs[3] = div_rcp(dpitn, ut, yut) + pitn * dkvk;
+    rhs[4] = div_rcp(dpixx, ut, yut) + pixx * dkvk;
+    rhs[5] = div_rcp(dpixy, ut, yut) + pixy * dkvk;
+    rhs[6] = div_rcp(dpixn, ut, yut) + pixn * dkvk;
+    rhs[7] = div_rcp(dpiyy, ut, yut) + piyy * dkvk;
+    rhs[8] = div_rcp(dpiyn, ut, yut) + piyn * dkvk;
+    rhs[9] = div_rcp(dpinn, ut, yut) + pinn * dkvk;
     if (BULK) {
         double dPi = -beta_Pi * theta - Pi * tauPiInv - delta_PiPi * Pi * theta + lambda_Pipi * ps;
-        rhs[10] = dPi / ut + Pi * dkvk;
+        rhs[10] = div_rcp(dPi, ut, yut) + Pi * dkvk;
     }
 }
 

@@ -99,6 +99,7 @@ _sig("vh_event_device_field", C.c_int, [_evp, C.c_int, C.POINTER(C.c_void_p)])
 _sig("vh_event_energy_of_T", C.c_int, [_evp, C.c_double, C.POINTER(C.c_double)])
 _sig("vh_event_powf_misses", C.c_int, [_evp, C.POINTER(C.c_ulonglong)])
 _sig("vh_cornelius_surfaces", C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.POINTER(C.c_int)])
+_sig("vh_device_math_check", C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p])
 _sig("vh_eos_synthetic_table", C.c_int, [C.c_int] + [C.c_double] * 6 + [_dp])
 _sig("vh_eos_eval", C.c_double, [_cfgp, C.c_void_p, C.c_int, C.c_int, C.c_double])
 _sig("vh_ic_gubser", C.c_int, [_cfgp, C.c_double, C.c_double, _dp, _dp, _dp, C.c_void_p])
@@ -300,6 +301,14 @@ def cornelius_surfaces(dim: int, cubes: np.ndarray, value0: float, dx) -> tuple[
     check(lib.vh_cornelius_surfaces(dim, _ptr(cubes), len(cubes), value0, _ptr(dxa), _ptr(out), cap, _ptr(counts),
                                     C.byref(n)), "vh_cornelius_surfaces")
     return out[:n.value], counts
+
+
+def device_math(which: int, a: np.ndarray, b: np.ndarray | None = None) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    bb = None if b is None else np.ascontiguousarray(b, dtype=np.float64)
+    out = np.zeros_like(a)
+    check(lib.vh_device_math_check(which, _ptr(a), _ptr(bb), len(a), _ptr(out)), "vh_device_math_check")
+    return out
 
 
 def interior(cfg: VhConfig, a: np.ndarray) -> np.ndarray:

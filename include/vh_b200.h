@@ -193,6 +193,13 @@ int vh_cornelius_surfaces_noalloc(int dim, const double *d_cubes, int n_cubes, d
                                   double *d_elements, int cap_elements, int *d_counts, int *d_n_elements,
                                   void *stream);
 
+/* Self-check of the device arithmetic that must equal the host libm bit for
+ * bit: which = 0 out[i] = tanh(a[i]) (the regulation factor,
+ * FullyDiscreteKurganovTadmorScheme.cpp:775), 1 = a[i]/b[i] through the
+ * shared-reciprocal division, 2 = a[i]/b[i] IEEE, 3 = powf((float)a[i], 0.25f)
+ * (EquationOfState.cpp:196).  Host arrays of n doubles. */
+int vh_device_math_check(int which, const double *a, const double *b, int n, double *out);
+
 /* Inputs seen outside the calibrated powf range since creation (diagnostic;
  * 0 means every temperature matched the host libm exactly). */
 int vh_event_powf_misses(vh_event *ev, unsigned long long *misses);
