@@ -20,6 +20,7 @@
  * --fmad=false so no multiply-add is fused behind the reference's back.
  */
 #include <cuda_runtime.h>
+#include <cstdlib>
 #include "vh_kernels.h"
 
 namespace vh {
@@ -288,6 +289,97 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_stage_kernel(cons
     if (k == A.nz + 1) { put_cell<NQ>(A, s + sxy, acc, P); put_cell<NQ>(A, s + 2 * sxy, acc, P); }
 }
 
+/* ---------------------------------------------------------------------
+ * Phase-split form of the same stage: five short kernels instead of one long
+ * one, in the reference's own phase order (FullyDiscreteKurganovTadmorScheme.cpp:
+ * eulerStepKernelSource, X, Y, Z, then inference/regulation/ghosts).  The
+ * partial sums live in qout between phases; FP64 stores are exact, so the
+ * result is bit-identical to the fused kernel.  Each phase's code is a
+ * fraction of the fused kernel's, which fits the instruction cache: the fused
+ * kernel spends most of its stall time waiting for instruction fetch.
+ * --------------------------------------------------------------------- */
+__device__ __forceinline__ bool stage_cell(const StageArgs &A, int &i, int &j, int &k, long long &s)
+{
+    i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    k = blockIdx.z + 2;
+    if (i >= A.nx + 2 || j >= A.ny + 2) return false;
+    s = i + (long long)A.ncx * j + (long long)A.ncx * A.ncy * k;
+    return true;
+}
+
+template <int NQ, int EOS>
+__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_source_kernel(const __grid_constant__ StageArgs A)
+{
+    int i, j, k;
+    long long s;
+    if (!stage_cell(A, i, j, k, s)) return;
+    double acc[NQ];
+    source_update<NQ, EOS>(A, s, acc);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] = acc[n];
+}
+
+template <int NQ, int EOS, int DIR>
+__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_kernel(const __grid_constant__ StageArgs A)
+{
+    int i, j, k;
+    long long s;
+    if (!stage_cell(A, i, j, k, s)) return;
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    const long long st = (DIR == 1) ? 1 : (DIR == 2) ? (long long)A.ncx : (long long)A.ncx * A.ncy;
+    const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
+    const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
+    double r[NQ];
+#pragma unroll 1
+    for (int f = 0; f < 2; ++f) face_flux<NQ, EOS>(A, f == 0 ? s : s - st, st, DIR, f == 0, ePrev, r, bad);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) r[n] = div_rcp(r[n], d, yd);
+    double S[4];
+    dir_sources<NQ>(A, s, st, d, DIR, S);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) { r[n] += S[n]; r[n] *= A.dt; }
+#pragma unroll
+    for (int n = 4; n < NQ; ++n) r[n] *= A.dt;
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] += r[n];
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+}
+
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
+__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_final_kernel(const __grid_constant__ StageArgs A)
+{
+    int i, j, k;
+    long long s;
+    if (!stage_cell(A, i, j, k, s)) return;
+    const long long sxy = (long long)A.ncx * A.ncy;
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    double acc[NQ];
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) acc[n] = A.qout[n * A.L + s];
+    if (!HAS_Z) {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) acc[n] += 0.0;
+    }
+    if (STAGE2) {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) { acc[n] += __ldg(A.qbase + n * A.L + s); acc[n] /= 2; }
+    }
+    Prim P = infer<EOS>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
+                        (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
+    regulate<NQ>(A, acc, P, bad);
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+    put_cell<NQ>(A, s, acc, P);
+    if (i == 2) { put_cell<NQ>(A, s - 1, acc, P); put_cell<NQ>(A, s - 2, acc, P); }
+    if (i == A.nx + 1) { put_cell<NQ>(A, s + 1, acc, P); put_cell<NQ>(A, s + 2, acc, P); }
+    if (j == 2) { put_cell<NQ>(A, s - A.ncx, acc, P); put_cell<NQ>(A, s - 2 * A.ncx, acc, P); }
+    if (j == A.ny + 1) { put_cell<NQ>(A, s + A.ncx, acc, P); put_cell<NQ>(A, s + 2 * A.ncx, acc, P); }
+    if (k == 2) { put_cell<NQ>(A, s - sxy, acc, P); put_cell<NQ>(A, s - 2 * sxy, acc, P); }
+    if (k == A.nz + 1) { put_cell<NQ>(A, s + sxy, acc, P); put_cell<NQ>(A, s + 2 * sxy, acc, P); }
+}
+
 /* DynamicalVariables.cpp:169-218 (T^{tau mu} from e, p+Pi, u, pi) and the
  * ghost faces; the previous-step velocity starts equal to u. */
 __global__ void init_kernel(const __grid_constant__ InitArgs A)
@@ -353,16 +445,41 @@ void launch_init(const InitArgs &a, cudaStream_t s)
     init_kernel<<<grid, block, 0, s>>>(a);
 }
 
+/* Fused for small lattices (launch- and latency-bound: one wave of threads,
+ * each carrying a whole stage), phase-split from 2^18 interior cells up
+ * (measured on B200: 131x131x61 split 5.43 ms/step vs fused 6.82; 101x101x1
+ * fused 0.120 ms vs split 0.163).  VH_STAGE_MODE=fused|split overrides. */
+static bool use_split(const StageArgs &a)
+{
+    static int forced = [] {
+        const char *e = getenv("VH_STAGE_MODE");
+        return !e ? -1 : (e[0] == 'f' ? 0 : 1);
+    }();
+    if (forced >= 0) return forced == 1;
+    return (long long)a.nx * a.ny * a.nz >= (1LL << 18);
+}
+
 template <int NQ, int EOS>
 static void launch_stage_t(const StageArgs &a, cudaStream_t s)
 {
     dim3 block(32, 4, 1);
     dim3 grid((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
     const bool z = a.nz > 1, st2 = a.qbase != nullptr;
-    if (z && st2) kt_stage_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
-    else if (z) kt_stage_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
-    else if (st2) kt_stage_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);
-    else kt_stage_kernel<NQ, EOS, false, false><<<grid, block, 0, s>>>(a);
+    if (!use_split(a)) {
+        if (z && st2) kt_stage_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
+        else if (z) kt_stage_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
+        else if (st2) kt_stage_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);
+        else kt_stage_kernel<NQ, EOS, false, false><<<grid, block, 0, s>>>(a);
+        return;
+    }
+    kt_source_kernel<NQ, EOS><<<grid, block, 0, s>>>(a);
+    kt_flux_kernel<NQ, EOS, 1><<<grid, block, 0, s>>>(a);
+    kt_flux_kernel<NQ, EOS, 2><<<grid, block, 0, s>>>(a);
+    if (z) kt_flux_kernel<NQ, EOS, 3><<<grid, block, 0, s>>>(a);
+    if (z && st2) kt_final_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
+    else if (z) kt_final_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
+    else if (st2) kt_final_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);
+    else kt_final_kernel<NQ, EOS, false, false><<<grid, block, 0, s>>>(a);
 }
 
 void launch_stage(const StageArgs &a, int nq, int eos_kind, cudaStream_t s)
