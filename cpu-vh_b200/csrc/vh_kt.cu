@@ -40,7 +40,7 @@ __device__ __forceinline__ void extrapolate(const double *__restrict__ qn, long 
  * cells b and b+st along axis dir (1 x, 2 y, 3 eta).  fwd: r = -H, else r += H.
  * dir and fwd are runtime values so that the six faces of a cell share one copy
  * of this code (the fully unrolled form overflowed the instruction cache). */
-template <int NQ, int EOS>
+template <int NQ, int EOS, bool INL = false>
 __device__ __forceinline__ void face_flux(const StageArgs &A, long long b, long long st, int dir, bool fwd,
                                           double ePrev, double *__restrict__ r, bool &bad)
 {
@@ -52,8 +52,8 @@ __device__ __forceinline__ void face_flux(const StageArgs &A, long long b, long 
     for (int c = 0; c < 8; ++c) extrapolate(q + c * L, b, st, th, qRs[c], qLs[c]);
     double PiR = 0, PiL = 0;
     if (NQ == 15) extrapolate(q + 14 * L, b, st, th, PiR, PiL);
-    Prim R = infer<EOS>(A.eos, A.t, qRs[0] - qRs[4], qRs[1] - qRs[5], qRs[2] - qRs[6], qRs[3] - qRs[7], PiR, ePrev, bad);
-    Prim Lf = infer<EOS>(A.eos, A.t, qLs[0] - qLs[4], qLs[1] - qLs[5], qLs[2] - qLs[6], qLs[3] - qLs[7], PiL, ePrev, bad);
+    Prim R = infer<EOS, INL>(A.eos, A.t, qRs[0] - qRs[4], qRs[1] - qRs[5], qRs[2] - qRs[6], qRs[3] - qRs[7], PiR, ePrev, bad);
+    Prim Lf = infer<EOS, INL>(A.eos, A.t, qLs[0] - qLs[4], qLs[1] - qLs[5], qLs[2] - qLs[6], qLs[3] - qLs[7], PiL, ePrev, bad);
     const double vR = (dir == 1) ? R.ux : (dir == 2) ? R.uy : R.un;
     const double vL = (dir == 1) ? Lf.ux : (dir == 2) ? Lf.uy : Lf.un;
     const double rhoLeft = fabs(vL / Lf.ut);
@@ -333,7 +333,7 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_kernel(const
     const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
     double r[NQ];
 #pragma unroll 1
-    for (int f = 0; f < 2; ++f) face_flux<NQ, EOS>(A, f == 0 ? s : s - st, st, DIR, f == 0, ePrev, r, bad);
+    for (int f = 0; f < 2; ++f) face_flux<NQ, EOS, true>(A, f == 0 ? s : s - st, st, DIR, f == 0, ePrev, r, bad);
 #pragma unroll
     for (int n = 0; n < NQ; ++n) r[n] = div_rcp(r[n], d, yd);
     double S[4];
@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_final_kernel(cons
 #pragma unroll
         for (int n = 0; n < NQ; ++n) { acc[n] += __ldg(A.qbase + n * A.L + s); acc[n] /= 2; }
     }
-    Prim P = infer<EOS>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
+    Prim P = infer<EOS, true>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
                         (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
     regulate<NQ>(A, acc, P, bad);
     if (bad) raise_error(A.err, kErrNan, s, A.step);

@@ -118,7 +118,7 @@ __device__ __forceinline__ double approx_deriv(double th, double x, double y, do
  * ePrev, bisection if Newton does not converge.  Kept out of line: it is
  * called thirteen times per cell and stage, and inlining the loop that often
  * overflows the instruction cache. */
-static __device__ __noinline__ double e_newton_table(const DevEos &E, double ePrev, double M0, double M, double Pi, bool &bad)
+__device__ __forceinline__ double e_newton_table_body(const DevEos &E, double ePrev, double M0, double M, double Pi, bool &bad)
 {
     double e0 = ePrev;
     for (int j = 0; j < 10000; ++j) {                              /* MAX_ITERS_NR */
@@ -156,15 +156,23 @@ static __device__ __noinline__ double e_newton_table(const DevEos &E, double ePr
     return ePrev;
 }
 
+/* The root solve as a call (one copy of the loop for a long kernel whose
+ * instruction footprint matters) or inlined (short phase kernels). */
+static __device__ __noinline__ double e_newton_table(const DevEos &E, double ePrev, double M0, double M, double Pi, bool &bad)
+{
+    return e_newton_table_body(E, ePrev, M0, M, Pi, bad);
+}
+
 /* EnergyMomentumTensor.cpp:22-115: energy density from M0, M, Pi; the
  * conformal closed form (:113) truncates through float. */
-template <int EOS>
+template <int EOS, bool INL = false>
 __device__ __forceinline__ double e_from_conserved(const DevEos &E, double ePrev, double M0, double M, double Pi, bool &bad)
 {
     if (EOS == 0) {
         float h = sqrtf(fabsf(__double2float_rn(4 * M0 * M0 - 3 * M)));
         return (double)fabsf(__double2float_rn((double)h - M0));
     }
+    if (INL) return e_newton_table_body(E, ePrev, M0, M, Pi, bad);
     return e_newton_table(E, ePrev, M0, M, Pi, bad);
 }
 
@@ -172,14 +180,14 @@ struct Prim { double e, p, ut, ux, uy, un; };
 
 /* EnergyMomentumTensor.cpp:117-233, from the five combinations it uses
  * (M0 = ttt - pitt, M1..M3 = tt^i - pit^i, Pi). */
-template <int EOS>
+template <int EOS, bool INL = false>
 __device__ __forceinline__ Prim infer(const DevEos &E, double t, double M0, double M1, double M2, double M3,
                                       double Pi, double ePrev, bool &bad)
 {
     Prim r;
     double M = M1 * M1 + M2 * M2 + t * t * M3 * M3;
     if (ePrev <= 0.1) r.e = M0 - M / M0;
-    else r.e = e_from_conserved<EOS>(E, ePrev, M0, M, Pi, bad);
+    else r.e = e_from_conserved<EOS, INL>(E, ePrev, M0, M, Pi, bad);
     if (isnan(r.e)) bad = true;
     r.p = eos_p<EOS>(E, r.e);
     if (r.e < 1.e-7) { r.e = 1.e-7; r.p = 1.e-7; }
