@@ -14,9 +14,14 @@ event generators (none are public for this path).
   e2e    the same metric through the C ABI with pinned host buffers: upload of
          the initial condition, K steps, download of the energy density, timed
          on the host clock
-  roofline  dominant kernel = the fused stage kernel; algorithmic bytes per
-         launch = 428 B/cell (mean of the 368 B and 488 B the two stages must
-         move), peak = measured HBM copy bandwidth
+  roofline  dominant kernel = the one with the largest share of the timed
+         device time (on large lattices the x/y/eta flux kernel, else the
+         fused stage kernel); its launches are timed with CUDA events that the
+         library records between the stage kernels on the event's stream
+         during the timed steps.  Algorithmic bytes per launch = per-cell
+         compulsory words of that phase x interior cells (PHASE_WORDS);
+         peak = measured HBM copy bandwidth; traffic = DRAM bytes per launch
+         from an ncu capture of the same workload (NCU_TRAFFIC)
   cpu_baseline  the reference's own sources (oracle/_ref, OpenMP over all host
          cores) on a bounded sample of the same workload
 
@@ -38,7 +43,29 @@ sys.path.insert(0, os.path.join(ROOT, "cpu-vh_b200"))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 BYTES_PER_CELL_STEP = 856          # (5*Nq + 32) * 8 with Nq = 15
-BYTES_PER_CELL_LAUNCH = 428        # stage 1: 46 words, stage 2: 61 words; mean
+
+
+def phase_words(nq):
+    """Compulsory FP64 words per interior cell of one launch of each phase."""
+    return {
+        # q, u, up, e, p read; q* written
+        "source": 2 * nq + 10,
+        # q stencil (each value once), e, u^tau, u^dir, q* read; q* written
+        "flux": 3 * nq + 3,
+        # q* and e read (+ q^n in stage 2), q, e, p, u written: mean of stages
+        "final": 2.5 * nq + 7,
+        # the whole stage in one kernel: (46 + 61) / 2 words at Nq = 15
+        "fused": 2.5 * nq + 16,
+    }
+
+
+# DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
+# ncu capture kept in profiles/kt_stage_kernels_glauber_131x131x61.md
+NCU_TRAFFIC = {("glauber_3p1d", "flux"): 387.02e6, ("glauber_3p1d", "source"): 336.17e6}
+
+
+KERNEL_NAMES = {"source": "kt_source_kernel", "flux": "kt_flux_kernel (x, y, eta)",
+                "final": "kt_final_kernel", "fused": "kt_stage_kernel"}
 
 
 def parse():
@@ -224,6 +251,10 @@ def main():
 
     cfg, rows, st, variant, desc = workload(args.workload)
     N = cfg.nx * cfg.ny * cfg.nz
+    px, py, pz = cfg.padded()
+    state_mb = (3 * cfg.nq() + 16) * px * py * pz * 8 / 1e6   # q x3, e/p x2, u x3 planes
+    l2_note = (f"state {state_mb:.0f} MB > 126 MB L2, no flush" if state_mb > 126 else
+               f"state {state_mb:.0f} MB fits in the 126 MB L2 (not flushed; latency-bound small lattice)")
     ev = vh.Event(cfg, rows)
     ev.set_initial(st)
     stream = torch.cuda.ExternalStream(ev.stream())
@@ -247,9 +278,25 @@ def main():
     ms = max_over_ranks(e0.elapsed_time(e1))
     ms_step = ms / args.steps
     value = N * args.steps * world / (ms / 1e3)
-    launch_s = ms / 1e3 / (2 * args.steps)
+    # the same K steps again with CUDA events recorded between the stage
+    # kernels on the event's stream: per-kernel launch durations
+    ev.phase_timing(True)
+    ev.step(args.steps)
+    phases = ev.phase_times()
+    ev.phase_timing(False)
+    # dominant kernel: group the three flux directions (one kernel template)
+    kern = {}
+    for name, (t, n) in phases.items():
+        k = "flux" if name.startswith("flux") else name
+        kt, kn = kern.get(k, (0.0, 0))
+        kern[k] = (kt + t, kn + n)
+    dom = max(kern, key=lambda k: kern[k][0])
+    dom_ms, dom_n = kern[dom]
+    launch_s = dom_ms / 1e3 / dom_n
     peak, peak_kind = measured_peaks()
-    achieved = BYTES_PER_CELL_LAUNCH * N / launch_s / 1e9
+    alg_bytes = phase_words(ev.nq)[dom] * 8 * N
+    achieved = alg_bytes / launch_s / 1e9
+    traffic = NCU_TRAFFIC.get((args.workload, dom))
 
     e2e = None
     if not args.no_e2e:
@@ -292,12 +339,16 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
                 "config": {"workload": desc, "cells": N, "parallelism": f"replicas x{world}",
-                           "l2": "state ~580 MB > 126 MB L2, no flush"},
+                           "l2": l2_note},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": None,
-                             "note": f"peak {peak_kind}; algorithmic {BYTES_PER_CELL_LAUNCH} B/cell per launch; "
-                                     "the FP64 step is bound by the FP64 pipe, not HBM"},
-                "clocks": clk, "gpu_launches": 2 * args.steps}
+                             "frac": achieved / peak, "traffic": traffic,
+                             "kernel": KERNEL_NAMES[dom], "launches": dom_n,
+                             "launch_us": launch_s * 1e6, "algorithmic_bytes": alg_bytes,
+                             "share": dom_ms / sum(t for t, _ in kern.values()),
+                             "note": f"peak: {peak_kind} HBM copy bandwidth; the strict-parity FP64 "
+                                     "step is bound by FP64 issue latency, not HBM"},
+                "phases_ms_per_step": {k: t / args.steps for k, (t, _) in phases.items()},
+                "clocks": clk, "gpu_launches": ev.launches_per_step() * args.steps}
         if e2e:
             line["e2e"] = e2e
         if base:

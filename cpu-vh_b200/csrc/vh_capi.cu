@@ -114,6 +114,10 @@ struct vh_event {
     double *fo_elems = nullptr;
     int fo_cap = 0;
     int fo_count = 0;
+    /* per-phase timing (vh_event_phase_timing) */
+    bool timing = false;
+    std::vector<vh::StageMarks> marks;    /* one per stage launched since enabling */
+    size_t marks_used = 0;
 };
 
 static vh::DevEos dev_eos(const vh_event *ev)
@@ -160,6 +164,8 @@ int vh_event_destroy(vh_event *ev)
     cudaFree(ev->fo_slabs);
     cudaFree(ev->fo_scratch);
     cudaFree(ev->fo_elems);
+    for (auto &m : ev->marks)
+        for (cudaEvent_t e : m.ev) cudaEventDestroy(e);
     if (ev->stream) cudaStreamDestroy(ev->stream);
     delete ev;
     return VH_OK;
@@ -263,6 +269,18 @@ int vh_event_set_initial_device(vh_event *ev, const double *d_e, const double *d
     return do_init(ev, d_e, d_p, d_u, d_pi, d_Pi);
 }
 
+static vh::StageMarks *next_marks(vh_event *ev)
+{
+    if (!ev->timing) return nullptr;
+    if (ev->marks_used == ev->marks.size()) {
+        vh::StageMarks m{};
+        for (cudaEvent_t &e : m.ev)
+            if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        ev->marks.push_back(m);
+    }
+    return &ev->marks[ev->marks_used++];
+}
+
 int vh_event_step(vh_event *ev, int nsteps)
 {
     if (!ev || nsteps < 0) return fail(VH_ERR_ARG, "bad argument");
@@ -287,14 +305,14 @@ int vh_event_step(vh_event *ev, int nsteps)
         A.eout = ev->ep[1 - ev->ec]; A.pout = ev->ep[1 - ev->ec] + ev->L;
         A.uin = ev->u[ev->uc]; A.upin = ev->u[ev->up]; A.uout = ev->u[ev->us];
         A.t = t; A.t2pow = pow(t, 2); A.t_inf = t1; A.inv_t = 1.0 / t;
-        vh::launch_stage(A, ev->nq, c.eos_kind, ev->stream);
+        vh::launch_stage(A, ev->nq, c.eos_kind, ev->stream, next_marks(ev));
         /* stage 2: qS -> Q, convex with q; u(new) goes to the old up buffer */
         A.qin = ev->q[ev->qs]; A.qout = ev->q[ev->qn]; A.qbase = ev->q[ev->qc];
         A.ein = ev->ep[1 - ev->ec]; A.pin = ev->ep[1 - ev->ec] + ev->L;
         A.eout = ev->ep[ev->ec]; A.pout = ev->ep[ev->ec] + ev->L;
         A.uin = ev->u[ev->us]; A.upin = ev->u[ev->uc]; A.uout = ev->u[ev->up];
         A.t = t1; A.t2pow = pow(t1, 2); A.t_inf = t1; A.inv_t = 1.0 / t1;
-        vh::launch_stage(A, ev->nq, c.eos_kind, ev->stream);
+        vh::launch_stage(A, ev->nq, c.eos_kind, ev->stream, next_marks(ev));
         std::swap(ev->qc, ev->qn);
         std::swap(ev->uc, ev->up);
         ev->n += 1;
@@ -357,6 +375,39 @@ int vh_event_device_field(vh_event *ev, int field, double **d_ptr)
     const double *src = field_ptr(ev, field);
     if (!src) return fail(VH_ERR_ARG, "unknown field id");
     *d_ptr = const_cast<double *>(src);
+    return VH_OK;
+}
+
+int vh_event_phase_timing(vh_event *ev, int enable)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    ev->timing = enable != 0;
+    ev->marks_used = 0;
+    return VH_OK;
+}
+
+int vh_event_phase_times(vh_event *ev, double *ms, long long *launches)
+{
+    if (!ev || !ms || !launches) return fail(VH_ERR_ARG, "null argument");
+    CUDA_TRY(cudaStreamSynchronize(ev->stream));
+    for (int p = 0; p < VH_NPHASES; ++p) { ms[p] = 0; launches[p] = 0; }
+    for (size_t i = 0; i < ev->marks_used; ++i) {
+        const vh::StageMarks &m = ev->marks[i];
+        for (int n = 0; n < m.n; ++n) {
+            float t = 0;
+            CUDA_TRY(cudaEventElapsedTime(&t, m.ev[n], m.ev[n + 1]));
+            ms[m.phase[n]] += t;
+            launches[m.phase[n]] += 1;
+        }
+    }
+    ev->marks_used = 0;
+    return VH_OK;
+}
+
+int vh_event_kernel_launches(vh_event *ev, int *per_step)
+{
+    if (!ev || !per_step) return fail(VH_ERR_ARG, "null argument");
+    *per_step = 2 * vh::stage_launches(ev->cfg.nx, ev->cfg.ny, ev->cfg.nz);
     return VH_OK;
 }
 

@@ -47,7 +47,16 @@ struct InitArgs {
 
 void launch_init(const InitArgs &a, cudaStream_t s);
 void launch_math_check(int which, const double *a, const double *b, int n, double *out, const PowfTab &pq, cudaStream_t s);
-void launch_stage(const StageArgs &a, int nq, int eos_kind, cudaStream_t s);
+/* Optional per-phase timing marks of one stage: ev[0] is recorded before the
+ * first kernel, ev[n+1] after kernel n, whose phase id is phase[n]
+ * (0 source, 1-3 x/y/eta flux, 4 finalize, 5 fused stage). */
+struct StageMarks {
+    cudaEvent_t ev[6];
+    int phase[5];
+    int n;
+};
+void launch_stage(const StageArgs &a, int nq, int eos_kind, cudaStream_t s, StageMarks *m = nullptr);
+int stage_launches(int nx, int ny, int nz);   /* kernel launches per RK stage */
 
 /* ---- freezeout ---- */
 struct FoArgs {

@@ -460,34 +460,53 @@ static bool use_split(const StageArgs &a)
 }
 
 template <int NQ, int EOS>
-static void launch_stage_t(const StageArgs &a, cudaStream_t s)
+static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
 {
     dim3 block(32, 4, 1);
     dim3 grid((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
     const bool z = a.nz > 1, st2 = a.qbase != nullptr;
+    if (m) { m->n = 0; cudaEventRecord(m->ev[0], s); }
+    auto mark = [&](int phase) {
+        if (!m) return;
+        m->phase[m->n] = phase;
+        cudaEventRecord(m->ev[++m->n], s);
+    };
     if (!use_split(a)) {
         if (z && st2) kt_stage_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
         else if (z) kt_stage_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
         else if (st2) kt_stage_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);
         else kt_stage_kernel<NQ, EOS, false, false><<<grid, block, 0, s>>>(a);
+        mark(5);
         return;
     }
     kt_source_kernel<NQ, EOS><<<grid, block, 0, s>>>(a);
+    mark(0);
     kt_flux_kernel<NQ, EOS, 1><<<grid, block, 0, s>>>(a);
+    mark(1);
     kt_flux_kernel<NQ, EOS, 2><<<grid, block, 0, s>>>(a);
-    if (z) kt_flux_kernel<NQ, EOS, 3><<<grid, block, 0, s>>>(a);
+    mark(2);
+    if (z) { kt_flux_kernel<NQ, EOS, 3><<<grid, block, 0, s>>>(a); mark(3); }
     if (z && st2) kt_final_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
     else if (z) kt_final_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
     else if (st2) kt_final_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);
     else kt_final_kernel<NQ, EOS, false, false><<<grid, block, 0, s>>>(a);
+    mark(4);
 }
 
-void launch_stage(const StageArgs &a, int nq, int eos_kind, cudaStream_t s)
+int stage_launches(int nx, int ny, int nz)
+{
+    StageArgs a{};
+    a.nx = nx; a.ny = ny; a.nz = nz;
+    if (!use_split(a)) return 1;
+    return nz > 1 ? 5 : 4;
+}
+
+void launch_stage(const StageArgs &a, int nq, int eos_kind, cudaStream_t s, StageMarks *m)
 {
     if (nq == 15) {
-        if (eos_kind == 1) launch_stage_t<15, 1>(a, s); else launch_stage_t<15, 0>(a, s);
+        if (eos_kind == 1) launch_stage_t<15, 1>(a, s, m); else launch_stage_t<15, 0>(a, s, m);
     } else {
-        if (eos_kind == 1) launch_stage_t<14, 1>(a, s); else launch_stage_t<14, 0>(a, s);
+        if (eos_kind == 1) launch_stage_t<14, 1>(a, s, m); else launch_stage_t<14, 0>(a, s, m);
     }
 }
 

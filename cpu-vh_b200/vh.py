@@ -38,6 +38,7 @@ VH_ZETA_REFERENCE, VH_ZETA_GAUSSIAN = 0, 1
 VH_PREC_FP64, VH_PREC_MIXED = 0, 1
 VH_F_UT, VH_F_UPT, VH_F_E, VH_F_P = 100, 110, 200, 201
 VH_FO_COLUMNS = 20
+PHASES = ("source", "flux_x", "flux_y", "flux_eta", "final", "fused")
 HBARC = 0.197326938
 
 FO_COLUMN_NAMES = ["tau", "x", "y", "eta", "ds0", "ds1", "ds2", "ds3", "ux", "uy", "un",
@@ -95,6 +96,9 @@ _sig("vh_event_get_field", C.c_int, [_evp, C.c_int, _dp])
 _sig("vh_event_freezeout", C.c_int, [_evp, C.POINTER(C.c_int), C.POINTER(C.c_int)])
 _sig("vh_event_fetch_surface", C.c_int, [_evp, C.c_void_p, C.c_int, C.POINTER(C.c_int)])
 _sig("vh_event_stream", C.c_int, [_evp, C.POINTER(C.c_void_p)])
+_sig("vh_event_kernel_launches", C.c_int, [_evp, C.POINTER(C.c_int)])
+_sig("vh_event_phase_timing", C.c_int, [_evp, C.c_int])
+_sig("vh_event_phase_times", C.c_int, [_evp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)])
 _sig("vh_event_device_field", C.c_int, [_evp, C.c_int, C.POINTER(C.c_void_p)])
 _sig("vh_event_energy_of_T", C.c_int, [_evp, C.c_double, C.POINTER(C.c_double)])
 _sig("vh_event_powf_misses", C.c_int, [_evp, C.POINTER(C.c_ulonglong)])
@@ -273,6 +277,21 @@ class Event:
         if n.value:
             check(lib.vh_event_fetch_surface(self.h, _ptr(out), n.value, C.byref(n)), "vh_event_fetch_surface")
         return out
+
+    def launches_per_step(self) -> int:
+        n = C.c_int()
+        check(lib.vh_event_kernel_launches(self.h, C.byref(n)), "vh_event_kernel_launches")
+        return n.value
+
+    def phase_timing(self, enable: bool = True) -> None:
+        check(lib.vh_event_phase_timing(self.h, 1 if enable else 0), "vh_event_phase_timing")
+
+    def phase_times(self) -> dict:
+        """{phase name: (total ms, launches)} since phase_timing(True) or the last call."""
+        ms = (C.c_double * 6)()
+        n = (C.c_longlong * 6)()
+        check(lib.vh_event_phase_times(self.h, ms, n), "vh_event_phase_times")
+        return {name: (ms[i], n[i]) for i, name in enumerate(PHASES) if n[i]}
 
     def stream(self) -> int:
         s = C.c_void_p()

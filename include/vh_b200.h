@@ -151,6 +151,27 @@ int vh_event_freezeout(vh_event *ev, int *n_elements, int *n_above);
  * doubles per element.  Returns VH_ERR_CAPACITY if cap_elements is too small. */
 int vh_event_fetch_surface(vh_event *ev, double *host_out, int cap_elements, int *n_elements);
 
+/* Kernel launches one vh_event_step(ev, 1) issues (2 RK stages; a stage is
+ * one fused kernel on small lattices, or the source, x, y, [eta] flux and
+ * finalize phase kernels on large ones). */
+int vh_event_kernel_launches(vh_event *ev, int *per_step);
+
+/* Per-phase device timing of the RK stages (no counterpart in the reference,
+ * which times the whole loop, HydroPlugin.cpp:284-297).  While enabled,
+ * vh_event_step records CUDA events between the stage kernels on the event's
+ * stream.  vh_event_phase_times waits for the stream, writes per phase the
+ * summed milliseconds and launch count since enabling (or since the previous
+ * read), and clears the record. */
+#define VH_PHASE_SOURCE 0   /* eulerStepKernelSource */
+#define VH_PHASE_FLUX_X 1   /* eulerStepKernelX */
+#define VH_PHASE_FLUX_Y 2   /* eulerStepKernelY */
+#define VH_PHASE_FLUX_ETA 3 /* eulerStepKernelZ */
+#define VH_PHASE_FINAL 4    /* convex combination, inference, regulation, ghosts */
+#define VH_PHASE_FUSED 5    /* all of one stage in one kernel (small lattices) */
+#define VH_NPHASES 6
+int vh_event_phase_timing(vh_event *ev, int enable);
+int vh_event_phase_times(vh_event *ev, double ms[VH_NPHASES], long long launches[VH_NPHASES]);
+
 /* The CUDA stream (cudaStream_t) the event's work is queued on. */
 int vh_event_stream(vh_event *ev, void **stream);
 
