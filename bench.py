@@ -74,7 +74,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="glauber_3p1d", choices=["glauber_3p1d", "gubser_2p1d"])
+    ap.add_argument("--workload", default="glauber_3p1d",
+                    choices=["glauber_3p1d", "gubser_2p1d", "batch_hotspots_2p1d"])
+    ap.add_argument("--events", type=int, default=256, help="batch_hotspots_2p1d: events in the batch")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     return ap.parse_args()
@@ -92,6 +94,27 @@ def workload(name):
     return cfg, rows, vh.glauber_ic(cfg, rows), "table", (
         "glauber_3p1d: 131x131x61, dx=dy=0.15 fm, deta=0.2, tau0=0.6, dtau=0.015, Au+Au optical Glauber b=7 fm, "
         "peak 30 GeV/fm^3, 2000-row synthetic crossover EoS, eta/s=0.08, Gaussian zeta/s (bulk on), FP64")
+
+
+BATCH_SIZES = (81, 101, 121, 141, 161, 181, 201)
+EVENT_STEPS = 300      # RK2 steps of one event for events/s (the Gubser event's step count)
+
+
+def batch_workload(n_events):
+    """Lumpy 2+1D events, n x n with n drawn uniformly from BATCH_SIZES
+    (seed 2024), hotspot initial conditions seeded with the event index."""
+    import numpy as np
+    import vh
+    rng = np.random.default_rng(2024)
+    sizes = [int(x) for x in rng.choice(BATCH_SIZES, size=n_events)]
+    rows = vh.synthetic_eos_table()
+    cfgs = [vh.hotspot_config(n) for n in sizes]
+    ics = [vh.hotspot_ic(c, rows, seed=i) for i, c in enumerate(cfgs)]
+    desc = (f"batch_hotspots_2p1d: {n_events} events, n x n x 1 with n uniform in {{81..201 step 20}} (seed 2024), "
+            "dx=0.1 fm, tau0=0.6, dtau=0.01, Poisson(200) hotspots of width 0.4 fm, Gamma(1.6) amplitudes, "
+            "mean peak 20 GeV/fm^3, centres in the b=0 Woods-Saxon overlap, 2000-row synthetic EoS, eta/s=0.08, "
+            "Gaussian zeta/s (bulk on), FP64")
+    return cfgs, rows, ics, desc
 
 
 def measured_peaks():
@@ -187,25 +210,39 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    cfg, rows, st, variant, desc = workload(args.workload)
     import oracle as O
-    N = cfg.nx * cfg.ny * cfg.nz
-    threads = os.cpu_count() or 1
-    if O.ref_available(variant):
-        ref, kind = O.RefEvent(variant, cfg, rows, threads=threads), "reference"
+    if args.workload == "batch_hotspots_2p1d":
+        cfgs, rows, ics, desc = batch_workload(args.events)
+        items, variant = list(zip(cfgs, ics))[:8], "table"
+        sample = "the first 8 events of the batch, one after another"
     else:
-        ref, kind, threads = O.OracleEvent(cfg, rows), "port", 1
-    ref.set_initial(st)
+        cfg, rows, st, variant, desc = workload(args.workload)
+        items, sample = [(cfg, st)], "the event"
+    threads = os.cpu_count() or 1
+    refs = []
+    for cfg, st in items:
+        if O.ref_available(variant):
+            ref, kind = O.RefEvent(variant, cfg, rows, threads=threads), "reference"
+        else:
+            ref, kind, threads = O.OracleEvent(cfg, rows), "port", 1
+        ref.set_initial(st)
+        refs.append(ref)
+    N = sum(c.nx * c.ny * c.nz for c, _ in items)
+
+    def step_all(k):
+        for r in refs:
+            r.step(k)
+
     # bounded sample: at most ~150 s of timed CPU work
     t0 = time.perf_counter()
-    ref.step(1)
+    step_all(1)
     est = time.perf_counter() - t0
     warm = max(0, min(args.warmup, int(30.0 / max(est, 1e-3))) - 1)
     if warm:
-        ref.step(warm)
+        step_all(warm)
     k = max(1, min(args.steps, int(150.0 / max(est, 1e-3))))
     t0 = time.perf_counter()
-    ref.step(k)
+    step_all(k)
     secs = time.perf_counter() - t0
     v = N * k / secs
     line = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
@@ -214,10 +251,151 @@ def run_reference(args):
             "data": "synthetic", "impl": "reference",
             "config": {"workload": desc, "cells": N, "timed_steps": k},
             "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": kind,
-                             "sample": f"{k} RK2 steps timed of {args.steps} requested (bounded to ~150 s), "
-                                       f"{threads} OpenMP threads"},
+                             "sample": f"{k} RK2 steps of {sample}, timed of {args.steps} requested "
+                                       f"(bounded to ~150 s), {threads} OpenMP threads"},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_batch(args, torch, dist, world, rank, barrier, max_over_ranks):
+    """All events of the batched workload advanced by one vh_batch: one launch
+    per RK phase for every event, CUDA-graph replay, autotuned launch shapes."""
+    import numpy as np
+    import vh
+    cfgs, rows, ics, desc = batch_workload(args.events)
+    Ns = [c.nx * c.ny * c.nz for c in cfgs]
+    Ntot = sum(Ns)
+    evs = []
+    for c, st in zip(cfgs, ics):
+        e = vh.Event(c, rows)
+        e.set_initial(st)
+        evs.append(e)
+    b = vh.Batch(evs)
+    tune = b.autotune()
+    stream = torch.cuda.ExternalStream(b.stream())
+    b.step(args.warmup)
+    for e in evs:
+        e.sync()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    clocks.start()
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    b.step(args.steps)
+    e1.record(stream)
+    e1.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    for e in evs:
+        vh.check(e.status()[0], "batched steps")
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    ms_step = ms / args.steps
+    value = Ntot * args.steps * world / (ms / 1e3)
+    b.phase_timing(True)
+    b.step(args.steps)
+    phases = b.phase_times()
+    b.phase_timing(False)
+    kern = {}
+    for name, (t, n) in phases.items():
+        k = "flux" if name.startswith("flux") else name
+        kt, kn = kern.get(k, (0.0, 0))
+        kern[k] = (kt + t, kn + n)
+    dom = max(kern, key=lambda k: kern[k][0])
+    dom_ms, dom_n = kern[dom]
+    launch_s = dom_ms / 1e3 / dom_n
+    peak, peak_kind = measured_peaks()
+    alg_bytes = phase_words(cfgs[0].nq())[dom] * 8 * Ntot
+    achieved = alg_bytes / launch_s / 1e9
+
+    # the plain single-event path on the same events, one event at a time
+    solo_steps = max(1, min(args.steps, 10))
+    for e, st in zip(evs, ics):
+        e.set_initial(st)
+    t_solo = 0.0
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for e in evs:
+        es = torch.cuda.ExternalStream(e.stream())
+        e.step(1)
+        s0.record(es)
+        e.step(solo_steps)
+        s1.record(es)
+        s1.synchronize()
+        t_solo += s0.elapsed_time(s1)
+    solo_value = Ntot * solo_steps / (t_solo / 1e3)
+
+    e2e = None
+    if not args.no_e2e:
+        pins = []
+        for st in ics:
+            N = st.e.shape[0]
+            pin = torch.empty((17, N), dtype=torch.float64, pin_memory=True)
+            h = pin.numpy()
+            h[0], h[1], h[2:6], h[6:16], h[16] = st.e, st.p, st.u, 0.0, 0.0 if st.Pi is None else st.Pi
+            pins.append((pin, vh.InitialState(h[0], h[1], h[2:6], None, h[16])))
+        outs = [torch.empty(int(np.prod(c.padded())), dtype=torch.float64, pin_memory=True).numpy() for c in cfgs]
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for e, (_, init) in zip(evs, pins):
+            e.set_initial(init)
+        b.step(args.steps)
+        for e, o in zip(evs, outs):
+            vh.check(vh.lib.vh_event_get_field(e.h, vh.VH_F_E, o), "vh_event_get_field")
+        t1 = time.perf_counter()
+        barrier()
+        secs = max_over_ranks(t1 - t0)
+        h2d = sum((6 * N + (N if c.bulk else 0)) * 8 for c, N in zip(cfgs, Ns))
+        d2h = sum(o.nbytes for o in outs)
+        e2e = {"value": Ntot * args.steps * world / secs, "unit": "cell-updates/s",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "timer": "host wall clock, pinned buffers, IC upload of every event + K batched steps + e download"}
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_baseline:
+        # the reference on a bounded sample: the first 4 events, 2 steps each
+        tot_cells, tot_s = 0, 0.0
+        for c, st in list(zip(cfgs, ics))[:4]:
+            r = cpu_baseline(c, rows, st, "table", steps=2)
+            tot_cells += c.nx * c.ny * c.nz * 2
+            tot_s += r["seconds"]
+        base = dict(r)
+        base["value"] = tot_cells / tot_s
+        base["sample"] = ("2 RK2 steps of each of the first 4 events of the batch after 1 warm-up step, "
+                          f"{r['cores']} OpenMP threads (reference sources, one event at a time)")
+
+    if rank == 0:
+        line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
+                "config": {"workload": desc, "events": len(cfgs), "cells": Ntot, "parallelism": f"replicas x{world}",
+                           "l2": "batch state > 126 MB L2, no flush", "tuning": tune.describe()},
+                "events_per_s": value / Ntot / EVENT_STEPS * len(cfgs),
+                "events_per_s_note": f"events of {EVENT_STEPS} RK2 steps, from the batched step time",
+                "plain_single_event": {"value": solo_value, "unit": "cell-updates/s",
+                                       "events_per_s": solo_value / Ntot / EVENT_STEPS * len(cfgs),
+                                       "how": f"vh_event_step, one event at a time, {solo_steps} steps each, "
+                                              "CUDA events per event"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None,
+                             "kernel": "kt_batch_kernel " + dom, "launches": dom_n,
+                             "launch_us": launch_s * 1e6, "algorithmic_bytes": alg_bytes,
+                             "share": dom_ms / sum(t for t, _ in kern.values()),
+                             "note": f"peak: {peak_kind} HBM copy bandwidth; FP64-issue bound"},
+                "phases_ms_per_step": {k: t / args.steps for k, (t, _) in phases.items()},
+                "clocks": clk, "gpu_launches": b.launches_per_step() * args.steps}
+        if e2e:
+            line["e2e"] = e2e
+        if base:
+            line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        print(json.dumps(line), flush=True)
+    b.close()
+    for e in evs:
+        e.close()
     return 0
 
 
@@ -249,6 +427,11 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.workload == "batch_hotspots_2p1d":
+        rc = run_batch(args, torch, dist, world, rank, barrier, max_over_ranks)
+        if world > 1:
+            dist.destroy_process_group()
+        return rc
     cfg, rows, st, variant, desc = workload(args.workload)
     N = cfg.nx * cfg.ny * cfg.nz
     px, py, pz = cfg.padded()

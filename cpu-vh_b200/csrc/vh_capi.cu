@@ -1,15 +1,9 @@
 /*
  * vh_capi.cu -- the C ABI event implementation (include/vh_b200.h).
  *
- * An event owns one device allocation holding every plane of its state:
- *   q[3]  : NQ planes each -- current q, next Q, stage qS
- *           (the reference's q, Q, qS, DynamicalVariables.cpp:21)
- *   ep[2] : (e, p) twice -- read by one stage, written by the other
- *   u[3]  : 4 planes each -- u, up, uS (DynamicalVariables.cpp:23)
- * Planes are padded to a multiple of 32 doubles so every plane starts on a
- * 256-byte boundary.  One RK2 step is two launches of the fused stage kernel;
- * buffer roles rotate by index on the host, exactly as the reference swaps
- * pointers (setCurrentConservedVariables, swapFluidVelocity).
+ * The event object and its state layout are described in vh_event.h.  One
+ * RK2 step is two RK stages (vh_kt.cu), each either one fused kernel or the
+ * phase-split kernels; buffer roles rotate by index on the host.
  */
 #include <cuda_runtime.h>
 #include <cmath>
@@ -23,6 +17,7 @@
 #include "vh_b200.h"
 #include "vh_internal.h"
 #include "vh_kernels.h"
+#include "vh_event.h"
 
 static thread_local std::string g_err;
 
@@ -42,23 +37,16 @@ int vh::set_error(int code, const std::string &msg) { return fail(code, msg); }
 
 namespace {
 
-/* host-exact powf table, uploaded once per device */
-struct DevPowf {
-    unsigned *keys = nullptr;
-    float *vals = nullptr;
-    unsigned *bucket = nullptr;
-    unsigned hb0 = 0, hb1 = 0;
-};
 std::mutex g_powf_mu;
-std::map<int, DevPowf> g_powf;
+std::map<int, vh::DevPowf> g_powf;
 
-int device_powf(int dev, DevPowf *out)
+int device_powf(int dev, vh::DevPowf *out)
 {
     std::lock_guard<std::mutex> lk(g_powf_mu);
     auto it = g_powf.find(dev);
     if (it != g_powf.end()) { *out = it->second; return VH_OK; }
     const vh::PowfQuarterTable &T = vh::powf_quarter_table();
-    DevPowf d;
+    vh::DevPowf d;
     unsigned lob, hib;
     std::memcpy(&lob, &T.lo, 4);
     std::memcpy(&hib, &T.hi, 4);
@@ -80,64 +68,21 @@ int device_powf(int dev, DevPowf *out)
 
 } // namespace
 
-struct vh_event {
-    vh_config cfg;
-    int nq = 14;
-    int ncx = 0, ncy = 0, ncz = 0;
-    long long L = 0;          /* plane stride (padded) */
-    long long N = 0;          /* interior cells */
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    double *slab = nullptr;
-    double *q[3] = {nullptr, nullptr, nullptr};
-    double *ep[2] = {nullptr, nullptr};   /* e plane; p plane follows at +L */
-    double *u[3] = {nullptr, nullptr, nullptr};
-    int qc = 0, qn = 1, qs = 2;          /* current q, next Q, stage qS */
-    int ec = 0;                           /* e/p buffer holding the current state */
-    int uc = 0, up = 1, us = 2;           /* u, up, uS */
-    double *tables = nullptr;             /* p_tb then T_tb */
-    int *err = nullptr;                   /* [0] code, [1] step */
-    long long *err_cell = nullptr;
-    unsigned long long *powf_miss = nullptr;
-    double *ic = nullptr;                 /* interior staging: e, p, u(4), pi(10), Pi */
-    vh::HostEos heos;
-    DevPowf powf;
-    double e_reg = 0, e_fo = 0;
-    int n = 0;
-    double t = 0;
-    bool initialised = false;
-    /* freezeout */
-    double *fo_slabs = nullptr;           /* 2 x 11 x N */
-    int fo_prev = 0;                      /* which half is the previous slab */
-    int *fo_scratch = nullptr;
-    size_t fo_scratch_ints = 0;
-    double *fo_elems = nullptr;
-    int fo_cap = 0;
-    int fo_count = 0;
-    /* per-phase timing (vh_event_phase_timing) */
-    bool timing = false;
-    std::vector<vh::StageMarks> marks;    /* one per stage launched since enabling */
-    size_t marks_used = 0;
-};
 
-static vh::DevEos dev_eos(const vh_event *ev)
+
+vh::StageArgs vh::stage_args_base(const vh_event *ev)
 {
-    vh::DevEos E;
-    E.kind = ev->cfg.eos_kind;
-    E.a = ev->cfg.eos_factor;
-    E.p_tb = ev->tables;
-    E.T_tb = ev->tables ? ev->tables + ev->heos.e_length : nullptr;
-    E.e_length = ev->heos.e_length;
-    E.e_min = ev->heos.e_min;
-    E.e_spacing = ev->heos.e_spacing;
-    E.inv_spacing = 1.0 / ev->heos.e_spacing;
-    E.pq.keys = ev->powf.keys;
-    E.pq.vals = ev->powf.vals;
-    E.pq.bucket = ev->powf.bucket;
-    E.pq.hb0 = ev->powf.hb0;
-    E.pq.hb1 = ev->powf.hb1;
-    E.pq.miss = ev->powf_miss;
-    return E;
+    const vh_config &c = ev->cfg;
+    vh::StageArgs A{};
+    A.L = ev->L;
+    A.nx = c.nx; A.ny = c.ny; A.nz = c.nz; A.ncx = ev->ncx; A.ncy = ev->ncy;
+    A.dt = c.dt; A.dx = c.dx; A.dy = c.dy; A.dz = c.dz; A.theta = c.theta; A.etabar = c.etabar;
+    A.inv_dx = 1.0 / c.dx; A.inv_dy = 1.0 / c.dy; A.inv_dz = 1.0 / c.dz;
+    A.e_reg = ev->e_reg;
+    A.eos = dev_eos(ev);
+    A.zeta.law = c.zeta_law; A.zeta.norm = c.zeta_norm; A.zeta.T0 = c.zeta_T0_GeV; A.zeta.w = c.zeta_width_GeV;
+    A.err.code = ev->err; A.err.step = ev->err + 1; A.err.cell = ev->err_cell;
+    return A;
 }
 
 extern "C" {
@@ -286,15 +231,7 @@ int vh_event_step(vh_event *ev, int nsteps)
     if (!ev || nsteps < 0) return fail(VH_ERR_ARG, "bad argument");
     if (!ev->initialised) return fail(VH_ERR_STATE, "vh_event_step before vh_event_set_initial");
     const vh_config &c = ev->cfg;
-    vh::StageArgs A;
-    A.L = ev->L;
-    A.nx = c.nx; A.ny = c.ny; A.nz = c.nz; A.ncx = ev->ncx; A.ncy = ev->ncy;
-    A.dt = c.dt; A.dx = c.dx; A.dy = c.dy; A.dz = c.dz; A.theta = c.theta; A.etabar = c.etabar;
-    A.inv_dx = 1.0 / c.dx; A.inv_dy = 1.0 / c.dy; A.inv_dz = 1.0 / c.dz;
-    A.e_reg = ev->e_reg;
-    A.eos = dev_eos(ev);
-    A.zeta.law = c.zeta_law; A.zeta.norm = c.zeta_norm; A.zeta.T0 = c.zeta_T0_GeV; A.zeta.w = c.zeta_width_GeV;
-    A.err.code = ev->err; A.err.step = ev->err + 1; A.err.cell = ev->err_cell;
+    vh::StageArgs A = vh::stage_args_base(ev);
     for (int it = 0; it < nsteps; ++it) {
         const double t = ev->t;
         const double t1 = t + c.dt;           /* `t += dt` of rungeKutta2 */
@@ -511,7 +448,7 @@ int vh_device_math_check(int which, const double *a, const double *b, int n, dou
     if (!vh_device_available()) return fail(VH_ERR_NODEVICE, "no CUDA device");
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
-    DevPowf pw;
+    vh::DevPowf pw;
     vh::PowfTab pq{};
     if (which == 3) {
         int rc = device_powf(dev, &pw);

@@ -1,0 +1,343 @@
+/*
+ * vh_stage.cuh -- per-cell bodies of the KT RK2 stage, shared by the
+ * single-event kernels (vh_kt.cu) and the batched kernels (vh_batch.cu).
+ *
+ * Every body takes the stage's arguments by reference and the cell it owns;
+ * the arithmetic is the reference's, operation for operation, in FP64 with
+ * float truncations where the reference has them.  Because both launch forms
+ * run these same functions, a cell's result does not depend on which form
+ * (fused or phase-split, single event or batch) computed it.
+ */
+#ifndef VH_STAGE_CUH
+#define VH_STAGE_CUH
+
+#include "vh_kernels.h"
+
+namespace vh {
+
+/* Half-site states at the face between cells b and b+st (HalfSiteExtrapolation.cpp:12-26):
+ * for the forward face of cell s, b = s; for its backward face, b = s - st. */
+__device__ __forceinline__ void extrapolate(const double *__restrict__ qn, long long b, long long st, double th,
+                                            double &qR, double &qL)
+{
+    double A = __ldg(qn + b - st), B = __ldg(qn + b), C = __ldg(qn + b + st), D = __ldg(qn + b + 2 * st);
+    qR = C - approx_deriv(th, B, C, D) / 2;
+    qL = B + approx_deriv(th, A, B, C) / 2;
+}
+
+/* SemiDiscreteKurganovTadmorScheme.cpp:14-62 with LocalPropagationSpeed.cpp:14-22,
+ * SpectralRadius.cpp:14-24 and FluxFunctions.cpp:15-25, for the face between
+ * cells b and b+st along axis dir (1 x, 2 y, 3 eta).  fwd: r = -H, else r += H.
+ * dir and fwd are runtime values so that the six faces of a cell share one copy
+ * of this code (the fully unrolled form overflowed the instruction cache). */
+template <int NQ, int EOS, bool INL = false>
+__device__ __forceinline__ void face_flux(const StageArgs &A, long long b, long long st, int dir, bool fwd,
+                                          double ePrev, double *__restrict__ r, bool &bad)
+{
+    const double th = A.theta;
+    const long long L = A.L;
+    const double *__restrict__ q = A.qin;
+    double qRs[8], qLs[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) extrapolate(q + c * L, b, st, th, qRs[c], qLs[c]);
+    double PiR = 0, PiL = 0;
+    if (NQ == 15) extrapolate(q + 14 * L, b, st, th, PiR, PiL);
+    Prim R = infer<EOS, INL>(A.eos, A.t, qRs[0] - qRs[4], qRs[1] - qRs[5], qRs[2] - qRs[6], qRs[3] - qRs[7], PiR, ePrev, bad);
+    Prim Lf = infer<EOS, INL>(A.eos, A.t, qLs[0] - qLs[4], qLs[1] - qLs[5], qLs[2] - qLs[6], qLs[3] - qLs[7], PiL, ePrev, bad);
+    const double vR = (dir == 1) ? R.ux : (dir == 2) ? R.uy : R.un;
+    const double vL = (dir == 1) ? Lf.ux : (dir == 2) ? Lf.uy : Lf.un;
+    const double rhoLeft = fabs(vL / Lf.ut);
+    const double rhoRight = fabs(vR / R.ut);
+    const double a = fmax(rhoLeft, rhoRight);
+    const double yR = 1.0 / R.ut, yL = 1.0 / Lf.ut;   /* one reciprocal per state, exact quotients via div_rcp */
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) {
+        double qR, qL;
+        if (n < 8) { qR = qRs[n]; qL = qLs[n]; }
+        else if (n == 14) { qR = PiR; qL = PiL; }
+        else extrapolate(q + n * L, b, st, th, qR, qL);
+        double FqR = div_rcp(vR * qR, R.ut, yR);
+        double FqL = div_rcp(vL * qL, Lf.ut, yL);
+        double res = FqR + FqL - a * (qR - qL);
+        res /= 2;
+        r[n] = fwd ? -res : r[n] + res;
+    }
+}
+
+/* SourceTerms.cpp:316-419: sources from d(pi^{tau mu})/dx^i of the T^{tau mu} rows. */
+template <int NQ>
+__device__ __forceinline__ void dir_sources(const StageArgs &A, long long s, long long st, double d, int dir, double *S)
+{
+    const long long L = A.L;
+    const double *__restrict__ q = A.qin;
+    const double fac = 1 / d / 2;
+    const double ut = __ldg(A.uin + s);
+    const double v = __ldg(A.uin + dir * L + s);
+    const double vv = v / ut;
+#define DER(n) ((__ldg(q + (n) * L + s + st) - __ldg(q + (n) * L + s - st)) * fac)
+    const double dpitt = DER(4), dpitx = DER(5), dpity = DER(6), dpitn = DER(7);
+    if (dir == 1) {
+        double dpixx = DER(8), dpixy = DER(9), dpixn = DER(10);
+        if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpitx - vv * dPi; S[1] = dpitx * vv - dpixx - dPi; }
+        else { S[0] = dpitt * vv - dpitx; S[1] = dpitx * vv - dpixx; }
+        S[2] = dpity * vv - dpixy;
+        S[3] = dpitn * vv - dpixn;
+    } else if (dir == 2) {
+        double dpixy = DER(9), dpiyy = DER(11), dpiyn = DER(12);
+        if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpity - vv * dPi; S[2] = dpity * vv - dpiyy - dPi; }
+        else { S[0] = dpitt * vv - dpity; S[2] = dpity * vv - dpiyy; }
+        S[1] = dpitx * vv - dpixy;
+        S[3] = dpitn * vv - dpiyn;
+    } else {
+        double dpixn = DER(10), dpiyn = DER(12), dpinn = DER(13);
+        if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpitn - vv * dPi; S[3] = dpitn * vv - dpinn - dPi / A.t2pow; }
+        else { S[0] = dpitt * vv - dpitn; S[3] = dpitn * vv - dpinn; }
+        S[1] = dpitx * vv - dpixn;
+        S[2] = dpity * vv - dpiyn;
+    }
+#undef DER
+}
+
+/* eulerStepKernelX/Y/Z (FullyDiscreteKurganovTadmorScheme.cpp:300-634), the
+ * axes in the reference's order x, y, eta. */
+template <int NQ, int EOS, bool HAS_Z>
+__device__ __forceinline__ void flux_update(const StageArgs &A, long long s, double ePrev, double *__restrict__ acc, bool &bad)
+{
+#pragma unroll 1
+    for (int dir = 1; dir <= (HAS_Z ? 3 : 2); ++dir) {
+        const long long st = (dir == 1) ? 1 : (dir == 2) ? (long long)A.ncx : (long long)A.ncx * A.ncy;
+        const double d = (dir == 1) ? A.dx : (dir == 2) ? A.dy : A.dz;
+        const double yd = (dir == 1) ? A.inv_dx : (dir == 2) ? A.inv_dy : A.inv_dz;
+        double r[NQ];
+#pragma unroll 1
+        for (int f = 0; f < 2; ++f) face_flux<NQ, EOS>(A, f == 0 ? s : s - st, st, dir, f == 0, ePrev, r, bad);
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) r[n] = div_rcp(r[n], d, yd);
+        double S[4];
+        dir_sources<NQ>(A, s, st, d, dir, S);
+#pragma unroll
+        for (int n = 0; n < 4; ++n) { r[n] += S[n]; r[n] *= A.dt; }
+#pragma unroll
+        for (int n = 4; n < NQ; ++n) r[n] *= A.dt;
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) acc[n] += r[n];
+    }
+}
+
+/* SourceTerms.cpp:421-612 (USE_APPROX_DERIVATIVE; the dynamical-source arrays
+ * are zero, DynamicalVariables.cpp:47-52), then Q + dt S
+ * (FullyDiscreteKurganovTadmorScheme.cpp:264-273). */
+template <int NQ, int EOS>
+__device__ __forceinline__ void source_update(const StageArgs &A, long long s, double *__restrict__ acc)
+{
+    const long long L = A.L;
+    const double th = A.theta;
+    const long long sx = 1, sy = A.ncx, sz = (long long)A.ncx * A.ncy;
+    double Qv[NQ];
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) Qv[n] = __ldg(A.qin + n * L + s);
+    const double Pi = (NQ == 15) ? Qv[14] : 0;
+    const double *__restrict__ utv = A.uin, *__restrict__ uxv = A.uin + L, *__restrict__ uyv = A.uin + 2 * L,
+                 *__restrict__ unv = A.uin + 3 * L, *__restrict__ pv = A.pin;
+    const double e = __ldg(A.ein + s), p = __ldg(pv + s);
+    const double ut = __ldg(utv + s), ux = __ldg(uxv + s), uy = __ldg(uyv + s), un = __ldg(unv + s);
+    const double dxut = div_rcp(approx_deriv(th, __ldg(utv + s - sx), ut, __ldg(utv + s + sx)), A.dx, A.inv_dx);
+    const double dxux = div_rcp(approx_deriv(th, __ldg(uxv + s - sx), ux, __ldg(uxv + s + sx)), A.dx, A.inv_dx);
+    const double dxuy = div_rcp(approx_deriv(th, __ldg(uyv + s - sx), uy, __ldg(uyv + s + sx)), A.dx, A.inv_dx);
+    const double dxun = div_rcp(approx_deriv(th, __ldg(unv + s - sx), un, __ldg(unv + s + sx)), A.dx, A.inv_dx);
+    const double dyut = div_rcp(approx_deriv(th, __ldg(utv + s - sy), ut, __ldg(utv + s + sy)), A.dy, A.inv_dy);
+    const double dyux = div_rcp(approx_deriv(th, __ldg(uxv + s - sy), ux, __ldg(uxv + s + sy)), A.dy, A.inv_dy);
+    const double dyuy = div_rcp(approx_deriv(th, __ldg(uyv + s - sy), uy, __ldg(uyv + s + sy)), A.dy, A.inv_dy);
+    const double dyun = div_rcp(approx_deriv(th, __ldg(unv + s - sy), un, __ldg(unv + s + sy)), A.dy, A.inv_dy);
+    const double dnut = div_rcp(approx_deriv(th, __ldg(utv + s - sz), ut, __ldg(utv + s + sz)), A.dz, A.inv_dz);
+    const double dnux = div_rcp(approx_deriv(th, __ldg(uxv + s - sz), ux, __ldg(uxv + s + sz)), A.dz, A.inv_dz);
+    const double dnuy = div_rcp(approx_deriv(th, __ldg(uyv + s - sz), uy, __ldg(uyv + s + sz)), A.dz, A.inv_dz);
+    const double dnun = div_rcp(approx_deriv(th, __ldg(unv + s - sz), un, __ldg(unv + s + sz)), A.dz, A.inv_dz);
+    const double dxp = div_rcp(approx_deriv(th, __ldg(pv + s - sx), p, __ldg(pv + s + sx)), A.dx, A.inv_dx);
+    const double dyp = div_rcp(approx_deriv(th, __ldg(pv + s - sy), p, __ldg(pv + s + sy)), A.dy, A.inv_dy);
+    const double dnp = div_rcp(approx_deriv(th, __ldg(pv + s - sz), p, __ldg(pv + s + sz)), A.dz, A.inv_dz);
+    const double t = A.t;
+    /* Tnn(e, p + Pi, un, pinn, t), EnergyMomentumTensor.cpp:328-330 */
+    const double pP = p + Pi;
+    const double yt = A.inv_t;
+    const double tnn = (e + pP) * un * un + div_rcp(div_rcp(pP, t, yt), t, yt) + Qv[13];
+    const double yut = 1.0 / ut;
+    const double vx = div_rcp(ux, ut, yut), vy = div_rcp(uy, ut, yut), vn = div_rcp(un, ut, yut);
+    const double dxvx = div_rcp(dxux - vx * dxut, ut, yut);
+    const double dyvy = div_rcp(dyuy - vy * dyut, ut, yut);
+    const double dnvn = div_rcp(dnun - vn * dnut, ut, yut);
+    const double dkvk = dxvx + dyvy + dnvn;
+    double S[NQ];
+    S[0] = 0.0 - (div_rcp(Qv[0], t, yt) + t * tnn) + dkvk * (Qv[4] - p - Pi) - vx * dxp - vy * dyp - vn * dnp;
+    S[1] = 0.0 - div_rcp(Qv[1], t, yt) - dxp + dkvk * Qv[5];
+    S[2] = 0.0 - div_rcp(Qv[2], t, yt) - dyp + dkvk * Qv[6];
+    S[3] = 0.0 - div_rcp(3 * Qv[3], t, yt) - dnp / A.t2pow + dkvk * Qv[7];
+    pimunu_rhs<EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, e, p, ut, ux, uy, un,
+                              __ldg(A.upin + s), __ldg(A.upin + L + s), __ldg(A.upin + 2 * L + s), __ldg(A.upin + 3 * L + s),
+                              Qv + 4, Pi, dxut, dyut, dnut, dxux, dyux, dnux, dxuy, dyuy, dnuy, dxun, dyun, dnun, dkvk,
+                              A.etabar, A.dt);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) acc[n] = Qv[n] + A.dt * S[n];
+}
+
+/* regulateDissipativeCurrents, REG_SCHEME_1 (FullyDiscreteKurganovTadmorScheme.cpp:690-859).
+ * When e > e_reg both factors are exactly 1 and the reference's multiplies are
+ * identities, so the block is skipped. */
+template <int NQ>
+__device__ __forceinline__ void regulate(const StageArgs &A, double *__restrict__ acc, const Prim &P, bool &bad)
+{
+    if (P.e > A.e_reg) return;
+    const double t = A.t_inf, t2 = t * t;
+    const double pitt = acc[4], pitx = acc[5], pity = acc[6], pitn = acc[7], pixx = acc[8];
+    const double pixy = acc[9], pixn = acc[10], piyy = acc[11], piyn = acc[12], pinn = acc[13];
+    const double Pi = (NQ == 15) ? acc[14] : 0;
+    const double ut = P.ut, ux = P.ux, uy = P.uy, un = P.un;
+    const double xi0 = 0.1, rhomax = 1.0;
+    double pipi = pitt * pitt - 2 * pitx * pitx - 2 * pity * pity + pixx * pixx + 2 * pixy * pixy + piyy * piyy - 2 * pitn * pitn * t2 + 2 * pixn * pixn * t2 + 2 * piyn * piyn * t2 + pinn * pinn * t2 * t2;
+    double spipi = sqrt(fabs(pipi));
+    double pimumu = pitt - pixx - piyy - pinn * t * t;
+    double piu0 = -(pitn * t2 * un) + pitt * ut - pitx * ux - pity * uy;
+    double piu1 = -(pixn * t2 * un) + pitx * ut - pixx * ux - pixy * uy;
+    double piu2 = -(piyn * t2 * un) + pity * ut - pixy * ux - piyy * uy;
+    double piu3 = -(pinn * t2 * un) + pitn * ut - pixn * ux - piyn * uy;
+    double a1 = spipi / rhomax / (double)sqrtf(__double2float_rn(P.e * P.e + 3 * P.p * P.p));
+    double a2 = pimumu / xi0 / rhomax / spipi;
+    double a3 = piu0 / xi0 / rhomax / spipi;
+    double a4 = piu1 / xi0 / rhomax / spipi;
+    double a5 = piu2 / xi0 / rhomax / spipi;
+    double a6 = piu3 / xi0 / rhomax / spipi;
+    double a12 = fmax(a1, a2), a34 = fmax(a3, a4), a56 = fmax(a5, a6), a3456 = fmax(a34, a56);
+    double rho = fmax(a12, a3456);
+    double facShear = vh_tanh(rho) / rho;
+    if (fabs(rho) < 1.e-7) facShear = 1.0;
+#pragma unroll
+    for (int n = 4; n < 14; ++n) acc[n] *= facShear;
+    if (isnan(facShear)) bad = true;
+    if (NQ == 15) {
+        double rhoBulk = fabs(Pi) / P.p;
+        double facBulk = vh_tanh(rhoBulk) / rhoBulk;
+        if (fabs(rhoBulk) < 1.e-7) facBulk = 1.0;
+        acc[14] *= facBulk;
+        if (isnan(facBulk)) bad = true;
+    }
+}
+
+template <int NQ>
+__device__ __forceinline__ void put_cell(const StageArgs &A, long long d, const double *__restrict__ acc, const Prim &P)
+{
+    const long long L = A.L;
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) A.qout[n * L + d] = acc[n];
+    A.eout[d] = P.e;
+    A.pout[d] = P.p;
+    A.uout[d] = P.ut;
+    A.uout[L + d] = P.ux;
+    A.uout[2 * L + d] = P.uy;
+    A.uout[3 * L + d] = P.un;
+}
+
+/* the cell and its zero-gradient ghost copies (DynamicalVariables.cpp:220-378) */
+template <int NQ>
+__device__ __forceinline__ void put_with_ghosts(const StageArgs &A, int i, int j, int k, long long s,
+                                                const double *__restrict__ acc, const Prim &P)
+{
+    const long long sxy = (long long)A.ncx * A.ncy;
+    put_cell<NQ>(A, s, acc, P);
+    if (i == 2) { put_cell<NQ>(A, s - 1, acc, P); put_cell<NQ>(A, s - 2, acc, P); }
+    if (i == A.nx + 1) { put_cell<NQ>(A, s + 1, acc, P); put_cell<NQ>(A, s + 2, acc, P); }
+    if (j == 2) { put_cell<NQ>(A, s - A.ncx, acc, P); put_cell<NQ>(A, s - 2 * A.ncx, acc, P); }
+    if (j == A.ny + 1) { put_cell<NQ>(A, s + A.ncx, acc, P); put_cell<NQ>(A, s + 2 * A.ncx, acc, P); }
+    if (k == 2) { put_cell<NQ>(A, s - sxy, acc, P); put_cell<NQ>(A, s - 2 * sxy, acc, P); }
+    if (k == A.nz + 1) { put_cell<NQ>(A, s + sxy, acc, P); put_cell<NQ>(A, s + 2 * sxy, acc, P); }
+}
+
+/* One whole stage for cell (i, j, k) at padded index s. */
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
+__device__ __forceinline__ void stage_body(const StageArgs &A, int i, int j, int k, long long s)
+{
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    double acc[NQ];
+    source_update<NQ, EOS>(A, s, acc);
+    flux_update<NQ, EOS, HAS_Z>(A, s, ePrev, acc, bad);
+    if (!HAS_Z) {
+        /* nz = 1: the eta ghosts equal the cell, every eta slope is 0 and the
+         * reference's eta pass adds exactly +0.0 (which turns a -0 into +0). */
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) acc[n] += 0.0;
+    }
+    if (STAGE2) {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) { acc[n] += __ldg(A.qbase + n * A.L + s); acc[n] /= 2; }
+    }
+    /* setInferredVariablesKernel (EnergyMomentumTensor.cpp:235-287) with ePrev = e[s] */
+    Prim P = infer<EOS>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
+                        (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
+    regulate<NQ>(A, acc, P, bad);
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+    put_with_ghosts<NQ>(A, i, j, k, s, acc, P);
+}
+
+/* Phase bodies of the split stage, in the reference's phase order
+ * (eulerStepKernelSource, X, Y, Z, then inference/regulation/ghosts).  The
+ * partial sums live in qout between phases; FP64 stores are exact, so the
+ * split stage is bit-identical to stage_body. */
+template <int NQ, int EOS>
+__device__ __forceinline__ void source_body(const StageArgs &A, long long s)
+{
+    double acc[NQ];
+    source_update<NQ, EOS>(A, s, acc);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] = acc[n];
+}
+
+template <int NQ, int EOS, int DIR>
+__device__ __forceinline__ void flux_body(const StageArgs &A, long long s)
+{
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    const long long st = (DIR == 1) ? 1 : (DIR == 2) ? (long long)A.ncx : (long long)A.ncx * A.ncy;
+    const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
+    const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
+    double r[NQ];
+#pragma unroll 1
+    for (int f = 0; f < 2; ++f) face_flux<NQ, EOS, true>(A, f == 0 ? s : s - st, st, DIR, f == 0, ePrev, r, bad);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) r[n] = div_rcp(r[n], d, yd);
+    double S[4];
+    dir_sources<NQ>(A, s, st, d, DIR, S);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) { r[n] += S[n]; r[n] *= A.dt; }
+#pragma unroll
+    for (int n = 4; n < NQ; ++n) r[n] *= A.dt;
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] += r[n];
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+}
+
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
+__device__ __forceinline__ void final_body(const StageArgs &A, int i, int j, int k, long long s)
+{
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    double acc[NQ];
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) acc[n] = A.qout[n * A.L + s];
+    if (!HAS_Z) {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) acc[n] += 0.0;
+    }
+    if (STAGE2) {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) { acc[n] += __ldg(A.qbase + n * A.L + s); acc[n] /= 2; }
+    }
+    Prim P = infer<EOS, true>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
+                              (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
+    regulate<NQ>(A, acc, P, bad);
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+    put_with_ghosts<NQ>(A, i, j, k, s, acc, P);
+}
+
+} // namespace vh
+
+#endif

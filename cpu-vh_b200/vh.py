@@ -99,6 +99,16 @@ _sig("vh_event_stream", C.c_int, [_evp, C.POINTER(C.c_void_p)])
 _sig("vh_event_kernel_launches", C.c_int, [_evp, C.POINTER(C.c_int)])
 _sig("vh_event_phase_timing", C.c_int, [_evp, C.c_int])
 _sig("vh_event_phase_times", C.c_int, [_evp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)])
+_btp = C.c_void_p
+_sig("vh_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(_btp)])
+_sig("vh_batch_destroy", C.c_int, [_btp])
+_sig("vh_batch_size", C.c_int, [_btp, C.POINTER(C.c_int)])
+_sig("vh_batch_step", C.c_int, [_btp, C.c_int])
+_sig("vh_batch_set_active", C.c_int, [_btp, C.c_int, C.c_int])
+_sig("vh_batch_kernel_launches", C.c_int, [_btp, C.POINTER(C.c_int)])
+_sig("vh_batch_phase_timing", C.c_int, [_btp, C.c_int])
+_sig("vh_batch_phase_times", C.c_int, [_btp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)])
+_sig("vh_batch_stream", C.c_int, [_btp, C.POINTER(C.c_void_p)])
 _sig("vh_event_device_field", C.c_int, [_evp, C.c_int, C.POINTER(C.c_void_p)])
 _sig("vh_event_energy_of_T", C.c_int, [_evp, C.c_double, C.POINTER(C.c_double)])
 _sig("vh_event_powf_misses", C.c_int, [_evp, C.POINTER(C.c_ulonglong)])
@@ -141,6 +151,16 @@ def synthetic_eos_table(nrows: int = 2000, T_lo: float = 0.05, e_max: float = 60
     rows = np.zeros((nrows, 4))
     check(lib.vh_eos_synthetic_table(nrows, T_lo, e_max, a, dip, Tc, w, rows), "vh_eos_synthetic_table")
     return rows
+
+
+def hotspot_config(n=101) -> VhConfig:
+    """2+1D lumpy event of the batched workload: n x n cells, dx = 0.1 fm,
+    tau0 = 0.6 fm/c, dtau = 0.01 fm/c, table EoS, eta/s = 0.08, Gaussian
+    zeta/s (bulk evolved), as the 3+1D Glauber event."""
+    c = glauber_config(n, n, 1)
+    c.dx = c.dy = c.dz = 0.1
+    c.t0, c.dt = 0.6, 0.01
+    return c
 
 
 def gubser_config(nx=101, ny=101) -> VhConfig:
@@ -307,6 +327,90 @@ class Event:
         e = C.c_double()
         check(lib.vh_event_energy_of_T(self.h, T, C.byref(e)), "vh_event_energy_of_T")
         return e.value
+
+
+class BatchTuning(C.Structure):
+    """vh_batch_tuning: launch configuration of a batch (per phase, indexed as PHASES)."""
+    _fields_ = [("fused", C.c_int), ("tile_x", C.c_int * 6), ("tile_y", C.c_int * 6),
+                ("persistent", C.c_int * 6), ("stage_ms", C.c_double)]
+
+    def describe(self) -> dict:
+        phases = ["fused"] if self.fused else ["source", "flux_x", "flux_y", "flux_eta", "final"]
+        return {"fused": bool(self.fused), "stage_ms": self.stage_ms,
+                "phases": {p: f"{self.tile_x[PHASES.index(p)]}x{self.tile_y[PHASES.index(p)]}"
+                              f"{' persistent' if self.persistent[PHASES.index(p)] else ''}" for p in phases}}
+
+
+_sig("vh_batch_autotune", C.c_int, [_btp, C.POINTER(BatchTuning)])
+_sig("vh_batch_get_tuning", C.c_int, [_btp, C.POINTER(BatchTuning)])
+_sig("vh_batch_set_tuning", C.c_int, [_btp, C.POINTER(BatchTuning)])
+
+
+class Batch:
+    """Events advanced together (vh_batch_*): one launch per RK phase for all
+    members; the members stay ordinary Events (fields, freezeout, status)."""
+
+    def __init__(self, events):
+        self.events = list(events)
+        arr = (C.c_void_p * len(self.events))(*[e.h.value if isinstance(e.h, C.c_void_p) else e.h
+                                                for e in self.events])
+        h = C.c_void_p()
+        check(lib.vh_batch_create(arr, len(self.events), C.byref(h)), "vh_batch_create")
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib.vh_batch_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def step(self, n: int = 1):
+        check(lib.vh_batch_step(self.h, n), "vh_batch_step")
+
+    def set_active(self, i: int, active: bool):
+        check(lib.vh_batch_set_active(self.h, i, 1 if active else 0), "vh_batch_set_active")
+
+    def autotune(self) -> BatchTuning:
+        t = BatchTuning()
+        check(lib.vh_batch_autotune(self.h, C.byref(t)), "vh_batch_autotune")
+        return t
+
+    def tuning(self) -> BatchTuning:
+        t = BatchTuning()
+        check(lib.vh_batch_get_tuning(self.h, C.byref(t)), "vh_batch_get_tuning")
+        return t
+
+    def set_tuning(self, t: BatchTuning):
+        check(lib.vh_batch_set_tuning(self.h, C.byref(t)), "vh_batch_set_tuning")
+
+    def launches_per_step(self) -> int:
+        n = C.c_int()
+        check(lib.vh_batch_kernel_launches(self.h, C.byref(n)), "vh_batch_kernel_launches")
+        return n.value
+
+    def phase_timing(self, enable: bool = True) -> None:
+        check(lib.vh_batch_phase_timing(self.h, 1 if enable else 0), "vh_batch_phase_timing")
+
+    def phase_times(self) -> dict:
+        ms = (C.c_double * 6)()
+        n = (C.c_longlong * 6)()
+        check(lib.vh_batch_phase_times(self.h, ms, n), "vh_batch_phase_times")
+        return {name: (ms[i], n[i]) for i, name in enumerate(PHASES) if n[i]}
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        check(lib.vh_batch_stream(self.h, C.byref(s)), "vh_batch_stream")
+        return s.value or 0
+
+
+def make_tuning(fused: bool, tx: int, persistent: bool) -> BatchTuning:
+    t = BatchTuning()
+    t.fused = 1 if fused else 0
+    for i in range(6):
+        t.tile_x[i], t.tile_y[i], t.persistent[i] = tx, 128 // tx, 1 if persistent else 0
+    return t
 
 
 def cornelius_surfaces(dim: int, cubes: np.ndarray, value0: float, dx) -> tuple[np.ndarray, np.ndarray]:

@@ -175,6 +175,50 @@ int vh_event_phase_times(vh_event *ev, double ms[VH_NPHASES], long long launches
 /* The CUDA stream (cudaStream_t) the event's work is queued on. */
 int vh_event_stream(vh_event *ev, void **stream);
 
+/* ------------------------------------------------------------------ batches
+ * Many resident events advanced together (no counterpart in the reference,
+ * which evolves one event per process, HydroPlugin.cpp:226-307).  A batch
+ * refers to existing events (it owns none of their memory): one launch per
+ * RK phase covers every member, a CUDA graph of one whole RK2 step is
+ * replayed, and the tile shape, grid form and fused/split choice come from
+ * timing the batch's own members.  Each member's results are bit-identical
+ * to vh_event_step on it alone.  Members must share the EoS kind, bulk on/off
+ * and the device, must have an initial state, and must outlive the batch.
+ * Between batch steps every single-event call (freezeout, fields, status,
+ * even vh_event_step) may be used on a member; its stream is ordered after
+ * the batch's work and the batch after its stream.
+ */
+typedef struct vh_batch vh_batch;
+
+typedef struct vh_batch_tuning {
+    int fused;                   /* 1: one kernel per RK stage; 0: the phase kernels      */
+    int tile_x[VH_NPHASES];      /* tile (= 128-thread block) shape per phase, indexed by  */
+    int tile_y[VH_NPHASES];      /* VH_PHASE_*: 32x4, 64x2, 16x8, 128x1 or 8x16             */
+    int persistent[VH_NPHASES];  /* 1: grid of resident blocks striding over the tiles;    */
+                                 /* 0: one block per tile                                   */
+    double stage_ms;             /* measured RK stage-1 time of this choice (autotuner)    */
+} vh_batch_tuning;
+
+int vh_batch_create(vh_event *const *events, int n_events, vh_batch **out);
+int vh_batch_destroy(vh_batch *b);
+int vh_batch_size(vh_batch *b, int *n_events);
+/* nsteps RK2 steps of every active member (autotunes on the first call). */
+int vh_batch_step(vh_batch *b, int nsteps);
+/* An inactive member is skipped (its tiles do no work) until re-activated. */
+int vh_batch_set_active(vh_batch *b, int member, int active);
+/* Run the tuner now (members' state is untouched) and report its choice. */
+int vh_batch_autotune(vh_batch *b, vh_batch_tuning *out);
+int vh_batch_get_tuning(vh_batch *b, vh_batch_tuning *out);
+/* Fix the launch configuration (tile shapes must be one of the five). */
+int vh_batch_set_tuning(vh_batch *b, const vh_batch_tuning *t);
+/* Kernel launches per batch step (the step-argument kernel + both stages). */
+int vh_batch_kernel_launches(vh_batch *b, int *per_step);
+/* Per-phase device timing, as for events; while enabled the steps are
+ * launched one by one instead of through the CUDA graph. */
+int vh_batch_phase_timing(vh_batch *b, int enable);
+int vh_batch_phase_times(vh_batch *b, double ms[VH_NPHASES], long long launches[VH_NPHASES]);
+int vh_batch_stream(vh_batch *b, void **stream);
+
 /* Device pointer of a padded field (for zero-copy inspection / timing). */
 int vh_event_device_field(vh_event *ev, int field, double **d_ptr);
 

@@ -12,9 +12,11 @@ this module, and only as the checker or the timed CPU baseline.
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes as C
 import os
 import subprocess
+import sys
 
 import numpy as np
 
@@ -22,6 +24,25 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "liboracle_vh.so")
 REF_DIR = os.path.join(HERE, "_ref")
 _dp = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+
+
+_libc = C.CDLL(None)
+_libc.fflush.argtypes = [C.c_void_p]
+
+
+@contextlib.contextmanager
+def _stdout_to_stderr():
+    """C-level stdout (fd 1) goes to stderr inside the block."""
+    sys.stdout.flush()
+    _libc.fflush(None)
+    saved = os.dup(1)
+    os.dup2(2, 1)
+    try:
+        yield
+    finally:
+        _libc.fflush(None)
+        os.dup2(saved, 1)
+        os.close(saved)
 
 
 def build_oracle(force: bool = False) -> str:
@@ -124,7 +145,9 @@ class RefEvent:
     """The reference's own code (oracle/_ref), single-threaded unless asked.
 
     The reference keeps its state in process globals, so only one RefEvent per
-    variant library may be live at a time."""
+    variant library may be live at a time.  Its diagnostics (printf to
+    stdout) are sent to stderr while it runs, so that a caller's stdout stays
+    its own."""
 
     def __init__(self, variant, cfg, eos_rows=None, threads=1):
         path = os.path.join(REF_DIR, f"libvhref_{variant}.so")
@@ -157,13 +180,16 @@ class RefEvent:
         Pi = np.zeros(N) if st.Pi is None else np.ascontiguousarray(st.Pi, dtype=np.float64)
         self.L.vhref_set_ic_arrays(np.ascontiguousarray(st.e), np.ascontiguousarray(st.p),
                                    np.ascontiguousarray(st.u, dtype=np.float64).reshape(-1), pi, Pi)
-        self.L.vhref_init()
+        with _stdout_to_stderr():
+            self.L.vhref_init()
 
     def step(self, n=1):
-        self.L.vhref_step(n)
+        with _stdout_to_stderr():
+            self.L.vhref_step(n)
 
     def time_steps(self, n):
-        return self.L.vhref_time_steps(n)
+        with _stdout_to_stderr():
+            return self.L.vhref_time_steps(n)
 
     def field(self, fid):
         ncx, ncy, ncz = self.cfg.nx + 4, self.cfg.ny + 4, self.cfg.nz + 4
@@ -172,4 +198,5 @@ class RefEvent:
         return out
 
     def freezeout(self, path):
-        return self.L.vhref_freezeout(path.encode())
+        with _stdout_to_stderr():
+            return self.L.vhref_freezeout(path.encode())

@@ -65,7 +65,7 @@ static struct HydroParameters g_hydro;
 static struct InitialConditionParameters g_ic;
 static int g_n = 0;          /* completed RK2 steps */
 static double g_t = 0.0;     /* current proper time */
-static int g_allocated = 0;
+static int g_allocated = 0;   /* padded cells the reference's arrays hold */
 
 /* initial-condition arrays over the interior (column-major i + nx*(j + ny*k)) */
 static std::vector<double> ic_e, ic_p, ic_u[4], ic_pi[10], ic_Pi;
@@ -343,7 +343,13 @@ void vhref_init(void)
 {
     int nx = g_lat.numLatticePointsX, ny = g_lat.numLatticePointsY, nz = g_lat.numLatticePointsRapidity;
     int len = g_lat.numComputationalLatticePointsX * g_lat.numComputationalLatticePointsY * g_lat.numComputationalLatticePointsRapidity;
-    if (!g_allocated) { allocateHostMemory(len); g_allocated = 1; }
+    if (len > g_allocated) {
+        /* the reference sizes its global arrays once per run; a larger event
+         * in the same process needs them again at the new size */
+        if (g_allocated) freeHostMemory();
+        allocateHostMemory(len);
+        g_allocated = len;
+    }
     inject_ic();
     g_n = 0;
     g_t = g_hydro.initialProperTimePoint;

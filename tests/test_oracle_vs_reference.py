@@ -38,16 +38,27 @@ def small_glauber():
     return cfg, rows, vh.glauber_ic(cfg, rows)
 
 
+def small_hotspots():
+    """a lumpy 2+1D event whose edge cells hit the e floor and the u^tau > 1e3
+    velocity reset (EnergyMomentumTensor.cpp:205-232)"""
+    cfg = vh.hotspot_config(41)
+    rows = vh.synthetic_eos_table()
+    return cfg, rows, vh.hotspot_ic(cfg, rows, seed=3)
+
+
 def small_gubser():
     cfg = vh.gubser_config(31, 27)
     return cfg, None, vh.gubser_ic(cfg)
 
 
-@pytest.mark.parametrize("case,variant", [("gubser", "conf"), ("glauber", "table")])
+CASES = {"gubser": small_gubser, "glauber": small_glauber, "hotspots": small_hotspots}
+
+
+@pytest.mark.parametrize("case,variant", [("gubser", "conf"), ("glauber", "table"), ("hotspots", "table")])
 def test_kt_steps_bitexact_vs_reference(case, variant):
     if not O.ref_available(variant):
         pytest.skip("reference build not present")
-    cfg, rows, st = small_gubser() if case == "gubser" else small_glauber()
+    cfg, rows, st = CASES[case]()
     ref = O.RefEvent(variant, cfg, rows, threads=1)
     orc = O.OracleEvent(cfg, rows)
     ref.set_initial(st)
