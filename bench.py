@@ -258,7 +258,7 @@ def run_reference(args):
     return 0
 
 
-def run_batch(args, torch, dist, world, rank, barrier, max_over_ranks):
+def run_batch(args, torch, world, rank, barrier, max_over_ranks):
     """All events of the batched workload advanced by one vh_batch: one launch
     per RK phase for every event, CUDA-graph replay, autotuned launch shapes."""
     import numpy as np
@@ -405,32 +405,16 @@ def main():
         return run_reference(args)
     import numpy as np
     import torch
-    import torch.distributed as dist
     import vh
+    from replicas import Replicas
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    R = Replicas("nccl")
+    world, rank, local = R.world, R.rank, R.local
+    barrier, max_over_ranks = R.barrier, R.max
 
     if args.workload == "batch_hotspots_2p1d":
-        rc = run_batch(args, torch, dist, world, rank, barrier, max_over_ranks)
-        if world > 1:
-            dist.destroy_process_group()
+        rc = run_batch(args, torch, world, rank, barrier, max_over_ranks)
+        R.close()
         return rc
     cfg, rows, st, variant, desc = workload(args.workload)
     N = cfg.nx * cfg.ny * cfg.nz
@@ -538,8 +522,7 @@ def main():
             line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
         print(json.dumps(line), flush=True)
     ev.close()
-    if world > 1:
-        dist.destroy_process_group()
+    R.close()
     return 0
 
 
