@@ -32,7 +32,7 @@
 #include <string>
 #include <vector>
 
-#include "vh_stage.cuh"
+#include "vh_batch_kernels.cuh"
 #include "vh_event.h"
 
 namespace vh {
@@ -90,77 +90,9 @@ __global__ void batch_prep_kernel(const __grid_constant__ BatchPrep P)
     if (P.advance) P.nstep[e] = n + 1;
 }
 
-struct BatchLaunch {
-    const StageArgs *args; /* this stage's arguments, one per member */
-    const int4 *tiles;     /* (member, i0, j0, k) in interior coordinates */
-    int ntiles;
-};
-
-static_assert(sizeof(StageArgs) % 8 == 0, "StageArgs is staged to shared memory in 8-byte words");
-
-/* phase 0 source, 1-3 x/y/eta flux, 4 finalize, 5 fused stage; ZM (phases 4
- * and 5): 0 every member 2+1D, 1 every member 3+1D, 2 mixed (per member) */
-template <int NQ, int EOS, int PHASE, bool STAGE2, int ZM>
-__global__ void __launch_bounds__(128, 4) kt_batch_kernel(const __grid_constant__ BatchLaunch B)
+BatchKernel batch_kernel(int nq, int eos_kind, int phase, bool st2, int zm, bool mixed)
 {
-    __shared__ __align__(16) StageArgs sA;
-    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-    const int nthr = blockDim.x * blockDim.y;
-    int cur = -1;
-    for (int t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
-        const int4 tile = __ldg(B.tiles + t);
-        if (tile.x != cur) {           /* uniform over the block */
-            __syncthreads();
-            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(B.args + tile.x);
-            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sA);
-            for (int w = tid; w < (int)(sizeof(StageArgs) / 8); w += nthr) dst[w] = src[w];
-            __syncthreads();
-            cur = tile.x;
-        }
-        const int i = tile.y + threadIdx.x + 2, j = tile.z + threadIdx.y + 2, k = tile.w + 2;
-        if (i >= sA.nx + 2 || j >= sA.ny + 2) continue;
-        const long long s = i + (long long)sA.ncx * j + (long long)sA.ncx * sA.ncy * k;
-        if constexpr (PHASE == 0) {
-            source_body<NQ, EOS>(sA, s);
-        } else if constexpr (PHASE >= 1 && PHASE <= 3) {
-            flux_body<NQ, EOS, PHASE>(sA, s);
-        } else if constexpr (PHASE == 4) {
-            if (ZM == 1 || (ZM == 2 && sA.nz > 1)) final_body<NQ, EOS, true, STAGE2>(sA, i, j, k, s);
-            else final_body<NQ, EOS, false, STAGE2>(sA, i, j, k, s);
-        } else {
-            if (ZM == 1 || (ZM == 2 && sA.nz > 1)) stage_body<NQ, EOS, true, STAGE2>(sA, i, j, k, s);
-            else stage_body<NQ, EOS, false, STAGE2>(sA, i, j, k, s);
-        }
-    }
-}
-
-using BatchKernel = void (*)(BatchLaunch);
-
-template <int NQ, int EOS, int PHASE>
-static BatchKernel batch_kernel_z(bool st2, int zm)
-{
-    if (zm == 0) return st2 ? kt_batch_kernel<NQ, EOS, PHASE, true, 0> : kt_batch_kernel<NQ, EOS, PHASE, false, 0>;
-    if (zm == 1) return st2 ? kt_batch_kernel<NQ, EOS, PHASE, true, 1> : kt_batch_kernel<NQ, EOS, PHASE, false, 1>;
-    return st2 ? kt_batch_kernel<NQ, EOS, PHASE, true, 2> : kt_batch_kernel<NQ, EOS, PHASE, false, 2>;
-}
-
-template <int NQ, int EOS>
-static BatchKernel batch_kernel_t(int phase, bool st2, int zm)
-{
-    switch (phase) {
-    case 0: return kt_batch_kernel<NQ, EOS, 0, false, 0>;
-    case 1: return kt_batch_kernel<NQ, EOS, 1, false, 0>;
-    case 2: return kt_batch_kernel<NQ, EOS, 2, false, 0>;
-    case 3: return kt_batch_kernel<NQ, EOS, 3, false, 0>;
-    case 4: return batch_kernel_z<NQ, EOS, 4>(st2, zm);
-    default: return batch_kernel_z<NQ, EOS, 5>(st2, zm);
-    }
-}
-
-static BatchKernel batch_kernel(int nq, int eos_kind, int phase, bool st2, int zm)
-{
-    if (nq == 15) return eos_kind == 1 ? batch_kernel_t<15, 1>(phase, st2, zm) : batch_kernel_t<15, 0>(phase, st2, zm);
-    return eos_kind == 1 ? batch_kernel_t<14, 1>(phase, st2, zm) : batch_kernel_t<14, 0>(phase, st2, zm);
+    return mixed ? batch_kernel_mixed(nq, eos_kind, phase, st2, zm) : batch_kernel_of<false>(nq, eos_kind, phase, st2, zm);
 }
 
 /* resident 128-thread blocks per SM of a batch kernel (persistent grid size) */
@@ -206,6 +138,7 @@ struct vh_batch {
     cudaEvent_t sync = nullptr;
     std::vector<vh_event *> mem;
     int nq = 14, eos_kind = 0;
+    bool mixed = false;              /* members evolve in mixed precision */
     bool any_z = false;
     int zmode = 0;                   /* 0 all 2+1D, 1 all 3+1D, 2 mixed */
     std::vector<vh::BatchMember> h_mem;
@@ -335,7 +268,7 @@ void launch_phase(vh_batch *b, int stage, int phase, int tx, int persistent)
     B.tiles = phase == 3 ? T.z : T.all;
     B.ntiles = phase == 3 ? T.n_z : T.n_all;
     if (B.ntiles == 0) return;
-    vh::BatchKernel k = vh::batch_kernel(b->nq, b->eos_kind, phase, stage == 1, b->zmode);
+    vh::BatchKernel k = vh::batch_kernel(b->nq, b->eos_kind, phase, stage == 1, b->zmode, b->mixed);
     int grid = B.ntiles;
     if (persistent) grid = std::min(grid, vh::resident_blocks(k) * b->sms);
     dim3 block(tx, 128 / tx, 1);
@@ -474,7 +407,7 @@ int preload(vh_batch *b)
     BTRY(cudaFuncGetAttributes(&attr, vh::batch_prep_kernel));
     for (int stage = 0; stage < 2; ++stage)
         for (int ph = 0; ph < VH_NPHASES; ++ph) {
-            vh::BatchKernel k = vh::batch_kernel(b->nq, b->eos_kind, ph, stage == 1, b->zmode);
+            vh::BatchKernel k = vh::batch_kernel(b->nq, b->eos_kind, ph, stage == 1, b->zmode, b->mixed);
             BTRY(cudaFuncGetAttributes(&attr, k));
             vh::resident_blocks(k);
         }
@@ -524,11 +457,12 @@ int vh_batch_create(vh_event *const *events, int n_events, vh_batch **out)
         if (!ev) { vh_batch_destroy(b); return bfail(VH_ERR_ARG, "null member"); }
         for (int j = 0; j < i; ++j)
             if (events[j] == ev) { vh_batch_destroy(b); return bfail(VH_ERR_ARG, "event listed twice"); }
-        if (i > 0 && (ev->nq != b->nq || ev->cfg.eos_kind != b->eos_kind || ev->device != b->device)) {
+        const bool mixed = ev->cfg.precision == VH_PREC_MIXED;
+        if (i > 0 && (ev->nq != b->nq || ev->cfg.eos_kind != b->eos_kind || ev->device != b->device || mixed != b->mixed)) {
             vh_batch_destroy(b);
-            return bfail(VH_ERR_ARG, "batch members must share the EoS kind, bulk on/off and the device");
+            return bfail(VH_ERR_ARG, "batch members must share the EoS kind, bulk on/off, the precision and the device");
         }
-        if (i == 0) { b->nq = ev->nq; b->eos_kind = ev->cfg.eos_kind; b->device = ev->device; }
+        if (i == 0) { b->nq = ev->nq; b->eos_kind = ev->cfg.eos_kind; b->device = ev->device; b->mixed = mixed; }
         b->mem.push_back(ev);
         b->any_z |= ev->cfg.nz > 1;
     }

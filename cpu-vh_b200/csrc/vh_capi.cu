@@ -125,7 +125,7 @@ int vh_event_create(const vh_config *cfg, const double *eos_rows, int eos_nrows,
         return fail(VH_ERR_ARG, "spacings and t0 must be positive");
     if (cfg->eos_kind == VH_EOS_TABLE && (!eos_rows || eos_nrows < 2 || eos_nrows > 100000))
         return fail(VH_ERR_ARG, "tabulated EoS needs 2..100000 rows");
-    if (cfg->precision != VH_PREC_FP64) return fail(VH_ERR_ARG, "only VH_PREC_FP64 is available on this build path");
+    if (cfg->precision != VH_PREC_FP64 && cfg->precision != VH_PREC_MIXED) return fail(VH_ERR_ARG, "unknown precision mode");
     if (!vh_device_available()) return fail(VH_ERR_NODEVICE, "no CUDA device");
     vh_event *ev = new vh_event();
     ev->cfg = *cfg;
@@ -232,6 +232,11 @@ int vh_event_step(vh_event *ev, int nsteps)
     if (!ev->initialised) return fail(VH_ERR_STATE, "vh_event_step before vh_event_set_initial");
     const vh_config &c = ev->cfg;
     vh::StageArgs A = vh::stage_args_base(ev);
+    const bool mixed = c.precision == VH_PREC_MIXED;
+    auto launch = [&](const vh::StageArgs &a, vh::StageMarks *m) {
+        if (mixed) vh::launch_stage_mixed(a, ev->nq, c.eos_kind, ev->stream, m);
+        else vh::launch_stage(a, ev->nq, c.eos_kind, ev->stream, m);
+    };
     for (int it = 0; it < nsteps; ++it) {
         const double t = ev->t;
         const double t1 = t + c.dt;           /* `t += dt` of rungeKutta2 */
@@ -242,14 +247,14 @@ int vh_event_step(vh_event *ev, int nsteps)
         A.eout = ev->ep[1 - ev->ec]; A.pout = ev->ep[1 - ev->ec] + ev->L;
         A.uin = ev->u[ev->uc]; A.upin = ev->u[ev->up]; A.uout = ev->u[ev->us];
         A.t = t; A.t2pow = pow(t, 2); A.t_inf = t1; A.inv_t = 1.0 / t;
-        vh::launch_stage(A, ev->nq, c.eos_kind, ev->stream, next_marks(ev));
+        launch(A, next_marks(ev));
         /* stage 2: qS -> Q, convex with q; u(new) goes to the old up buffer */
         A.qin = ev->q[ev->qs]; A.qout = ev->q[ev->qn]; A.qbase = ev->q[ev->qc];
         A.ein = ev->ep[1 - ev->ec]; A.pin = ev->ep[1 - ev->ec] + ev->L;
         A.eout = ev->ep[ev->ec]; A.pout = ev->ep[ev->ec] + ev->L;
         A.uin = ev->u[ev->us]; A.upin = ev->u[ev->uc]; A.uout = ev->u[ev->up];
         A.t = t1; A.t2pow = pow(t1, 2); A.t_inf = t1; A.inv_t = 1.0 / t1;
-        vh::launch_stage(A, ev->nq, c.eos_kind, ev->stream, next_marks(ev));
+        launch(A, next_marks(ev));
         std::swap(ev->qc, ev->qn);
         std::swap(ev->uc, ev->up);
         ev->n += 1;

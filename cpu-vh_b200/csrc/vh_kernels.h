@@ -57,6 +57,19 @@ struct StageMarks {
 };
 void launch_stage(const StageArgs &a, int nq, int eos_kind, cudaStream_t s, StageMarks *m = nullptr);
 int stage_launches(int nx, int ny, int nz);   /* kernel launches per RK stage */
+/* the same stage in mixed precision (vh_mixed.cu) */
+void launch_stage_mixed(const StageArgs &a, int nq, int eos_kind, cudaStream_t s, StageMarks *m = nullptr);
+
+/* ---- batched phase kernels (vh_batch_kernels.cuh) ---- */
+struct BatchLaunch {
+    const StageArgs *args; /* this stage's arguments, one per member */
+    const int4 *tiles;     /* (member, i0, j0, k) in interior coordinates */
+    int ntiles;
+};
+using BatchKernel = void (*)(BatchLaunch);
+/* phase: VH_PHASE_*; zm: 0 all members 2+1D, 1 all 3+1D, 2 mixed */
+BatchKernel batch_kernel(int nq, int eos_kind, int phase, bool st2, int zm, bool mixed);
+BatchKernel batch_kernel_mixed(int nq, int eos_kind, int phase, bool st2, int zm);
 
 /* ---- freezeout ---- */
 struct FoArgs {

@@ -22,64 +22,9 @@
  */
 #include <cuda_runtime.h>
 #include <cstdlib>
-#include "vh_stage.cuh"
+#include "vh_stage_kernels.cuh"
 
 namespace vh {
-
-#ifndef VH_STAGE_MIN_BLOCKS
-#define VH_STAGE_MIN_BLOCKS 4   /* 128 registers: 16 warps/SM; measured faster than 2-3 blocks at 168-255 */
-#endif
-
-/* interior cell (i, j, k) of this thread, at padded index s */
-__device__ __forceinline__ bool stage_cell(const StageArgs &A, int &i, int &j, int &k, long long &s)
-{
-    i = blockIdx.x * blockDim.x + threadIdx.x + 2;
-    j = blockIdx.y * blockDim.y + threadIdx.y + 2;
-    k = blockIdx.z + 2;
-    if (i >= A.nx + 2 || j >= A.ny + 2) return false;
-    s = i + (long long)A.ncx * j + (long long)A.ncx * A.ncy * k;
-    return true;
-}
-
-template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
-__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_stage_kernel(const __grid_constant__ StageArgs A)
-{
-    int i, j, k;
-    long long s;
-    if (!stage_cell(A, i, j, k, s)) return;
-    stage_body<NQ, EOS, HAS_Z, STAGE2>(A, i, j, k, s);
-}
-
-/* Phase-split form of the same stage: five short kernels instead of one long
- * one.  Each phase's code is a fraction of the fused kernel's and fits the
- * instruction cache: the fused kernel spends most of its stall time waiting
- * for instruction fetch on large lattices. */
-template <int NQ, int EOS>
-__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_source_kernel(const __grid_constant__ StageArgs A)
-{
-    int i, j, k;
-    long long s;
-    if (!stage_cell(A, i, j, k, s)) return;
-    source_body<NQ, EOS>(A, s);
-}
-
-template <int NQ, int EOS, int DIR>
-__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_kernel(const __grid_constant__ StageArgs A)
-{
-    int i, j, k;
-    long long s;
-    if (!stage_cell(A, i, j, k, s)) return;
-    flux_body<NQ, EOS, DIR>(A, s);
-}
-
-template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
-__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_final_kernel(const __grid_constant__ StageArgs A)
-{
-    int i, j, k;
-    long long s;
-    if (!stage_cell(A, i, j, k, s)) return;
-    final_body<NQ, EOS, HAS_Z, STAGE2>(A, i, j, k, s);
-}
 
 /* DynamicalVariables.cpp:169-218 (T^{tau mu} from e, p+Pi, u, pi) and the
  * ghost faces; the previous-step velocity starts equal to u. */
@@ -146,54 +91,6 @@ void launch_init(const InitArgs &a, cudaStream_t s)
     init_kernel<<<grid, block, 0, s>>>(a);
 }
 
-/* Fused for small lattices (launch- and latency-bound: one wave of threads,
- * each carrying a whole stage), phase-split from 2^18 interior cells up
- * (measured on B200: 131x131x61 split 5.43 ms/step vs fused 6.82; 101x101x1
- * fused 0.120 ms vs split 0.163).  VH_STAGE_MODE=fused|split overrides. */
-static bool use_split(const StageArgs &a)
-{
-    static int forced = [] {
-        const char *e = getenv("VH_STAGE_MODE");
-        return !e ? -1 : (e[0] == 'f' ? 0 : 1);
-    }();
-    if (forced >= 0) return forced == 1;
-    return (long long)a.nx * a.ny * a.nz >= (1LL << 18);
-}
-
-template <int NQ, int EOS>
-static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
-{
-    dim3 block(32, 4, 1);
-    dim3 grid((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
-    const bool z = a.nz > 1, st2 = a.qbase != nullptr;
-    if (m) { m->n = 0; cudaEventRecord(m->ev[0], s); }
-    auto mark = [&](int phase) {
-        if (!m) return;
-        m->phase[m->n] = phase;
-        cudaEventRecord(m->ev[++m->n], s);
-    };
-    if (!use_split(a)) {
-        if (z && st2) kt_stage_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
-        else if (z) kt_stage_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
-        else if (st2) kt_stage_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);
-        else kt_stage_kernel<NQ, EOS, false, false><<<grid, block, 0, s>>>(a);
-        mark(5);
-        return;
-    }
-    kt_source_kernel<NQ, EOS><<<grid, block, 0, s>>>(a);
-    mark(0);
-    kt_flux_kernel<NQ, EOS, 1><<<grid, block, 0, s>>>(a);
-    mark(1);
-    kt_flux_kernel<NQ, EOS, 2><<<grid, block, 0, s>>>(a);
-    mark(2);
-    if (z) { kt_flux_kernel<NQ, EOS, 3><<<grid, block, 0, s>>>(a); mark(3); }
-    if (z && st2) kt_final_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
-    else if (z) kt_final_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
-    else if (st2) kt_final_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);
-    else kt_final_kernel<NQ, EOS, false, false><<<grid, block, 0, s>>>(a);
-    mark(4);
-}
-
 int stage_launches(int nx, int ny, int nz)
 {
     StageArgs a{};
@@ -205,9 +102,9 @@ int stage_launches(int nx, int ny, int nz)
 void launch_stage(const StageArgs &a, int nq, int eos_kind, cudaStream_t s, StageMarks *m)
 {
     if (nq == 15) {
-        if (eos_kind == 1) launch_stage_t<15, 1>(a, s, m); else launch_stage_t<15, 0>(a, s, m);
+        if (eos_kind == 1) launch_stage_t<15, 1, false>(a, s, m); else launch_stage_t<15, 0, false>(a, s, m);
     } else {
-        if (eos_kind == 1) launch_stage_t<14, 1>(a, s, m); else launch_stage_t<14, 0>(a, s, m);
+        if (eos_kind == 1) launch_stage_t<14, 1, false>(a, s, m); else launch_stage_t<14, 0, false>(a, s, m);
     }
 }
 

@@ -218,128 +218,133 @@ __device__ __forceinline__ double zeta_over_s(const Zeta &Z, double T)
     return -13.77 * x * x + 27.55 * x - 13.45;
 }
 
+/* a / b with y = RN(1/b): exact (div_rcp) in FP64, a * y in FP32 */
+__device__ __forceinline__ double dvr(double a, double b, double y) { return div_rcp(a, b, y); }
+__device__ __forceinline__ float dvr(float a, float, float y) { return a * y; }
+
 /* SourceTerms.cpp:55-313, the right-hand side of the pi^{mu nu} (and Pi)
  * relaxation equations divided by u^tau. */
-template <int EOS, bool BULK>
-__device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, double *rhs, double t, double e, double p,
-    double ut, double ux, double uy, double un, double utp, double uxp, double uyp, double unp,
-    const double *pv, double Pi,
-    double dxut, double dyut, double dnut, double dxux, double dyux, double dnux,
-    double dxuy, double dyuy, double dnuy, double dxun, double dyun, double dnun, double dkvk,
-    double d_etabar, double d_dt)
+template <typename R, int EOS, bool BULK>
+__device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, R *rhs, R t, double e_d, double p_d,
+    double ut_d, double ux_d, double uy_d, double un_d, double utp, double uxp, double uyp, double unp,
+    const R *pv, R Pi,
+    R dxut, R dyut, R dnut, R dxux, R dyux, R dnux,
+    R dxuy, R dyuy, R dnuy, R dxun, R dyun, R dnun, R dkvk,
+    R d_etabar, R d_dt)
 {
-    const double delta_pipi = 1.33333, tau_pipi = 1.42857, delta_PiPi = 0.666667, lambda_piPi = 1.2;
-    const double pitt = pv[0], pitx = pv[1], pity = pv[2], pitn = pv[3], pixx = pv[4];
-    const double pixy = pv[5], pixn = pv[6], piyy = pv[7], piyn = pv[8], pinn = pv[9];
-    double T = eos_T<EOS>(E, e);
-    double taupiInv = T / 5 / d_etabar;
-    double beta_pi = (e + p) / 5;
-    double cs2 = eos_cs2<EOS>(E, e);
-    double a = 1.0 / 3.0 - cs2;
-    double a2 = a * a;
-    double beta_Pi = 15 * a2 * (e + p);
-    double lambda_Pipi = 8 * a / 5;
-    double tauPiInv = 0.0;
-    if (BULK) tauPiInv = 15 * a2 * T / zeta_over_s(Z, T);
-    double ut2 = ut * ut, un2 = un * un, t2 = t * t, t3 = t * t2;
-    const double kThird = 1.0 / 3.0, yut = 1.0 / ut, ydt = 1.0 / d_dt;
-    double dtut = div_rcp((ut - utp), d_dt, ydt), dtux = div_rcp((ux - uxp), d_dt, ydt), dtuy = div_rcp((uy - uyp), d_dt, ydt), dtun = div_rcp((un - unp), d_dt, ydt);
-    double Dut = ut * dtut + ux * dxut + uy * dyut + un * dnut + t * un * un;
-    double DuxUpper = ut * dtux + ux * dxux + uy * dyux + un * dnux;
-    double Dux = -DuxUpper;
-    double DuyUpper = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
-    double Duy = -DuyUpper;
-    double DunUpper = ut * dtun + ux * dxun + uy * dyun + un * dnun + 2 * ut * un / t;
-    double Dun = -t2 * DunUpper;
-    double dut = Dut - t * un * un;
-    double dux = ut * dtux + ux * dxux + uy * dyux + un * dnux;
-    double duy = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
-    double dun = ut * dtun + ux * dxun + uy * dyun + un * dnun;
-    double theta = ut / t + dtut + dxux + dyuy + dnun;
-    double stt = -t * ut * un2 + (dtut - ut * dut) + div_rcp((ut2 - 1) * theta, 3.0, kThird);
-    double stx = -(t * un2 * ux) / 2.0 + (dtux - dxut) / 2.0 - (ux * dut + ut * dux) / 2.0 + div_rcp(ut * ux * theta, 3.0, kThird);
-    double sty = -(t * un2 * uy) / 2.0 + (dtuy - dyut) / 2.0 - (uy * dut + ut * duy) / 2.0 + div_rcp(ut * uy * theta, 3.0, kThird);
-    double stn = -un * (2.0 * ut2 + t2 * un2) / (2.0 * t) + (dtun - dnut / t2) / 2.0 - (un * dut + ut * dun) / 2.0 + div_rcp(ut * un * theta, 3.0, kThird);
-    double sxx = -(dxux + ux * dux) + div_rcp((1.0 + ux * ux) * theta, 3.0, kThird);
-    double sxy = -(dxuy + dyux) / 2.0 - (uy * dux + ux * duy) / 2.0 + div_rcp(ux * uy * theta, 3.0, kThird);
-    double sxn = -ut * ux * un / t - (dxun + dnux / t2) / 2.0 - (un * dux + ux * dun) / 2.0 + div_rcp(ux * un * theta, 3.0, kThird);
-    double syy = -(dyuy + uy * duy) + div_rcp((1.0 + uy * uy) * theta, 3.0, kThird);
-    double syn = -ut * uy * un / t - (dyun + dnuy / t2) / 2.0 - (un * duy + uy * dun) / 2.0 + div_rcp(uy * un * theta, 3.0, kThird);
-    double snn = -ut * (1.0 + 2.0 * t2 * un2) / t3 - dnun / t2 - un * dun + div_rcp((1.0 / t2 + un2) * theta, 3.0, kThird);
-    double wtx = (-dtux - dxut + ut * dux - ux * dut - t * un2 * ux) / 2.0;
-    double wty = (-dtuy - dyut + ut * duy - uy * dut - t * un2 * uy) / 2.0;
-    double wtn = (-t2 * dtun - 2.0 * t * un - dnut - ut * Dun - t2 * un * dut - t3 * un * un2) / 2.0;
-    double wxy = (dxuy - dyux + ux * duy - uy * dux) / 2.0;
-    double wxn = (t2 * dxun - dnux - ux * Dun - t2 * un * dux) / 2.0;
-    double wyn = (t2 * dyun - dnuy - uy * Dun - t2 * un * duy) / 2.0;
-    double wxt = wtx, wyt = wty, wnt = wtn / t2, wyx = -wxy, wnx = -wxn / t2, wny = -wyn / t2;
-    double I1tt = 2.0 * ut * (pitt * Dut + pitx * Dux + pity * Duy + pitn * Dun);
-    double I1tx = (pitt * ux + pitx * ut) * Dut + (pitx * ux + pixx * ut) * Dux + (pity * ux + pixy * ut) * Duy + (pitn * ux + pixn * ut) * Dun;
-    double I1ty = (pitt * uy + pity * ut) * Dut + (pitx * uy + pixy * ut) * Dux + (pity * uy + piyy * ut) * Duy + (pitn * uy + piyn * ut) * Dun;
-    double I1tn = (pitt * un + pitn * ut) * Dut + (pitx * un + pixn * ut) * Dux + (pity * un + piyn * ut) * Duy + (pitn * un + pinn * ut) * Dun;
-    double I1xx = 2.0 * ux * (pitx * Dut + pixx * Dux + pixy * Duy + pixn * Dun);
-    double I1xy = (pitx * uy + pity * ux) * Dut + (pixx * uy + pixy * ux) * Dux + (pixy * uy + piyy * ux) * Duy + (pixn * uy + piyn * ux) * Dun;
-    double I1xn = (pitx * un + pitn * ux) * Dut + (pixx * un + pixn * ux) * Dux + (pixy * un + piyn * ux) * Duy + (pixn * un + pinn * ux) * Dun;
-    double I1yy = 2.0 * uy * (pity * Dut + pixy * Dux + piyy * Duy + piyn * Dun);
-    double I1yn = (pity * un + pitn * uy) * Dut + (pixy * un + pixn * uy) * Dux + (piyy * un + piyn * uy) * Duy + (piyn * un + pinn * uy) * Dun;
-    double I1nn = 2.0 * un * (pitn * Dut + pixn * Dux + piyn * Duy + pinn * Dun);
-    double I2tt = theta * pitt, I2tx = theta * pitx, I2ty = theta * pity, I2tn = theta * pitn, I2xx = theta * pixx;
-    double I2xy = theta * pixy, I2xn = theta * pixn, I2yy = theta * piyy, I2yn = theta * piyn, I2nn = theta * pinn;
-    double I3tt = 2.0 * (pitx * wtx + pity * wty + pitn * wtn);
-    double I3tx = pitt * wxt + pity * wxy + pitn * wxn + pixx * wtx + pixy * wty + pixn * wtn;
-    double I3ty = pitt * wyt + pitx * wyx + pitn * wyn + pixy * wtx + piyy * wty + piyn * wtn;
-    double I3tn = pitt * wnt + pitx * wnx + pity * wny + pixn * wtx + piyn * wty + pinn * wtn;
-    double I3xx = 2.0 * (pitx * wxt + pixy * wxy + pixn * wxn);
-    double I3xy = pitx * wyt + pity * wxt + pixx * wyx + piyy * wxy + pixn * wyn + piyn * wxn;
-    double I3xn = pitx * wnt + pitn * wxt + pixx * wnx + pixy * wny + piyn * wxy + pinn * wxn;
-    double I3yy = 2.0 * (pity * wyt + pixy * wyx + piyn * wyn);
-    double I3yn = pity * wnt + pitn * wyt + pixy * wnx + pixn * wyx + piyy * wny + pinn * wyn;
-    double I3nn = 2.0 * (pitn * wnt + pixn * wnx + piyn * wny);
-    double ux2 = ux * ux, uy2 = uy * uy;
-    double ps = pitt * stt - 2.0 * pitx * stx - 2.0 * pity * sty + pixx * sxx + 2.0 * pixy * sxy + piyy * syy - 2.0 * pitn * stn * t2 + 2.0 * pixn * sxn * t2 + 2.0 * piyn * syn * t2 + pinn * snn * t2 * t2;
-    double I4tt = (pitt * stt - pitx * stx - pity * sty - t2 * pitn * stn) - div_rcp((1.0 - ut2) * ps, 3.0, kThird);
-    double I4tx = (pitt * stx + pitx * stt) / 2.0 - (pitx * sxx + pixx * stx) / 2.0 - (pity * sxy + pixy * sty) / 2.0 - t2 * (pitn * sxn + pixn * stn) / 2.0 + div_rcp((ut * ux) * ps, 3.0, kThird);
-    double I4ty = (pitt * sty + pity * stt) / 2.0 - (pitx * sxy + pixy * stx) / 2.0 - (pity * syy + piyy * sty) / 2.0 - t2 * (pitn * syn + piyn * stn) / 2.0 + div_rcp((ut * uy) * ps, 3.0, kThird);
-    double I4tn = (pitt * stn + pitn * stt) / 2.0 - (pitx * sxn + pixn * stx) / 2.0 - (pity * syn + piyn * sty) / 2.0 - t2 * (pitn * snn + pinn * stn) / 2.0 + div_rcp((ut * un) * ps, 3.0, kThird);
-    double I4xx = (pitx * stx - pixx * sxx - pixy * sxy - t2 * pixn * sxn) + div_rcp((1.0 + ux2) * ps, 3.0, kThird);
-    double I4xy = (pitx * sty + pity * stx) / 2.0 - (pixx * sxy + pixy * sxx) / 2.0 - (pixy * syy + piyy * sxy) / 2.0 - t2 * (pixn * syn + piyn * sxn) / 2.0 + div_rcp((ux * uy) * ps, 3.0, kThird);
-    double I4xn = (pitx * stn + pitn * stx) / 2.0 - (pixx * sxn + pixn * sxx) / 2.0 - (pixy * syn + piyn * sxy) / 2.0 - t2 * (pixn * snn + pinn * sxn) / 2.0 + div_rcp((ux * un) * ps, 3.0, kThird);
-    double I4yy = (pity * sty - pixy * sxy - piyy * syy - t2 * piyn * syn) + div_rcp((1.0 + uy2) * ps, 3.0, kThird);
-    double I4yn = (pity * stn + pitn * sty) / 2.0 - (pixy * sxn + pixn * sxy) / 2.0 - (piyy * syn + piyn * syy) / 2.0 - t2 * (piyn * snn + pinn * syn) / 2.0 + div_rcp((uy * un) * ps, 3.0, kThird);
-    double I4nn = (pitn * stn - pixn * sxn - piyn * syn - t2 * pinn * snn) + div_rcp((1.0 / t2 + un2) * ps, 3.0, kThird);
-    double Itt = I1tt + delta_pipi * I2tt - I3tt + tau_pipi * I4tt - lambda_piPi * Pi * stt;
-    double Itx = I1tx + delta_pipi * I2tx - I3tx + tau_pipi * I4tx - lambda_piPi * Pi * stx;
-    double Ity = I1ty + delta_pipi * I2ty - I3ty + tau_pipi * I4ty - lambda_piPi * Pi * sty;
-    double Itn = I1tn + delta_pipi * I2tn - I3tn + tau_pipi * I4tn - lambda_piPi * Pi * stn;
-    double Ixx = I1xx + delta_pipi * I2xx - I3xx + tau_pipi * I4xx - lambda_piPi * Pi * sxx;
-    double Ixy = I1xy + delta_pipi * I2xy - I3xy + tau_pipi * I4xy - lambda_piPi * Pi * sxy;
-    double Ixn = I1xn + delta_pipi * I2xn - I3xn + tau_pipi * I4xn - lambda_piPi * Pi * sxn;
-    double Iyy = I1yy + delta_pipi * I2yy - I3yy + tau_pipi * I4yy - lambda_piPi * Pi * syy;
-    double Iyn = I1yn + delta_pipi * I2yn - I3yn + tau_pipi * I4yn - lambda_piPi * Pi * syn;
-    double Inn = I1nn + delta_pipi * I2nn - I3nn + tau_pipi * I4nn - lambda_piPi * Pi * snn;
-    double dpitt = 2.0 * beta_pi * stt - pitt * taupiInv - Itt - 2.0 * un * t * pitn;
-    double dpitx = 2.0 * beta_pi * stx - pitx * taupiInv - Itx - un * t * pixn;
-    double dpity = 2.0 * beta_pi * sty - pity * taupiInv - Ity - un * t * piyn;
-    double dpitn = 2.0 * beta_pi * stn - pitn * taupiInv - Itn - un * t * pinn - (ut * pitn + un * pitt) / t;
-    double dpixx = 2.0 * beta_pi * sxx - pixx * taupiInv - Ixx;
-    double dpixy = 2.0 * beta_pi * sxy - pixy * taupiInv - Ixy;
-    double dpixn = 2.0 * beta_pi * sxn - pixn * taupiInv - Ixn - (ut * pixn + un * pitx) / t;
-    double dpiyy = 2.0 * beta_pi * syy - piyy * taupiInv - Iyy;
-    double dpiyn = 2.0 * beta_pi * syn - piyn * taupiInv - Iyn - (ut * piyn + un * pity) / t;
-    double dpinn = 2.0 * beta_pi * snn - pinn * taupiInv - Inn - 2 * (ut * pinn + un * pitn) / t;
-    rhs[0] = div_rcp(dpitt, ut, yut) + pitt * dkvk;
-    rhs[1] = div_rcp(dpitx, ut, yut) + pitx * dkvk;
-    rhs[2] = div_rcp(dpity, ut, yut) + pity * dkvk;
-    rhs[3] = div_rcp(dpitn, ut, yut) + pitn * dkvk;
-    rhs[4] = div_rcp(dpixx, ut, yut) + pixx * dkvk;
-    rhs[5] = div_rcp(dpixy, ut, yut) + pixy * dkvk;
-    rhs[6] = div_rcp(dpixn, ut, yut) + pixn * dkvk;
-    rhs[7] = div_rcp(dpiyy, ut, yut) + piyy * dkvk;
-    rhs[8] = div_rcp(dpiyn, ut, yut) + piyn * dkvk;
-    rhs[9] = div_rcp(dpinn, ut, yut) + pinn * dkvk;
+    const R ut = R(ut_d), ux = R(ux_d), uy = R(uy_d), un = R(un_d), e = R(e_d), p = R(p_d);
+    const R delta_pipi = R(1.33333), tau_pipi = R(1.42857), delta_PiPi = R(0.666667), lambda_piPi = R(1.2);
+    const R pitt = pv[0], pitx = pv[1], pity = pv[2], pitn = pv[3], pixx = pv[4];
+    const R pixy = pv[5], pixn = pv[6], piyy = pv[7], piyn = pv[8], pinn = pv[9];
+    R T = R(eos_T<EOS>(E, e_d));
+    R taupiInv = T / 5 / d_etabar;
+    R beta_pi = (e + p) / 5;
+    R cs2 = R(eos_cs2<EOS>(E, e_d));
+    R a = R(1.0) / R(3.0) - cs2;
+    R a2 = a * a;
+    R beta_Pi = 15 * a2 * (e + p);
+    R lambda_Pipi = 8 * a / 5;
+    R tauPiInv = R(0.0);
+    if (BULK) tauPiInv = 15 * a2 * T / R(zeta_over_s(Z, double(T)));
+    R ut2 = ut * ut, un2 = un * un, t2 = t * t, t3 = t * t2;
+    const R kThird = R(1.0) / R(3.0), yut = R(1.0) / ut, ydt = R(1.0) / d_dt;
+    R dtut = dvr(R(ut_d - utp), d_dt, ydt), dtux = dvr(R(ux_d - uxp), d_dt, ydt), dtuy = dvr(R(uy_d - uyp), d_dt, ydt), dtun = dvr(R(un_d - unp), d_dt, ydt);
+    R Dut = ut * dtut + ux * dxut + uy * dyut + un * dnut + t * un * un;
+    R DuxUpper = ut * dtux + ux * dxux + uy * dyux + un * dnux;
+    R Dux = -DuxUpper;
+    R DuyUpper = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
+    R Duy = -DuyUpper;
+    R DunUpper = ut * dtun + ux * dxun + uy * dyun + un * dnun + 2 * ut * un / t;
+    R Dun = -t2 * DunUpper;
+    R dut = Dut - t * un * un;
+    R dux = ut * dtux + ux * dxux + uy * dyux + un * dnux;
+    R duy = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
+    R dun = ut * dtun + ux * dxun + uy * dyun + un * dnun;
+    R theta = ut / t + dtut + dxux + dyuy + dnun;
+    R stt = -t * ut * un2 + (dtut - ut * dut) + dvr((ut2 - 1) * theta, R(3.0), kThird);
+    R stx = -(t * un2 * ux) / R(2.0) + (dtux - dxut) / R(2.0) - (ux * dut + ut * dux) / R(2.0) + dvr(ut * ux * theta, R(3.0), kThird);
+    R sty = -(t * un2 * uy) / R(2.0) + (dtuy - dyut) / R(2.0) - (uy * dut + ut * duy) / R(2.0) + dvr(ut * uy * theta, R(3.0), kThird);
+    R stn = -un * (R(2.0) * ut2 + t2 * un2) / (R(2.0) * t) + (dtun - dnut / t2) / R(2.0) - (un * dut + ut * dun) / R(2.0) + dvr(ut * un * theta, R(3.0), kThird);
+    R sxx = -(dxux + ux * dux) + dvr((R(1.0) + ux * ux) * theta, R(3.0), kThird);
+    R sxy = -(dxuy + dyux) / R(2.0) - (uy * dux + ux * duy) / R(2.0) + dvr(ux * uy * theta, R(3.0), kThird);
+    R sxn = -ut * ux * un / t - (dxun + dnux / t2) / R(2.0) - (un * dux + ux * dun) / R(2.0) + dvr(ux * un * theta, R(3.0), kThird);
+    R syy = -(dyuy + uy * duy) + dvr((R(1.0) + uy * uy) * theta, R(3.0), kThird);
+    R syn = -ut * uy * un / t - (dyun + dnuy / t2) / R(2.0) - (un * duy + uy * dun) / R(2.0) + dvr(uy * un * theta, R(3.0), kThird);
+    R snn = -ut * (R(1.0) + R(2.0) * t2 * un2) / t3 - dnun / t2 - un * dun + dvr((R(1.0) / t2 + un2) * theta, R(3.0), kThird);
+    R wtx = (-dtux - dxut + ut * dux - ux * dut - t * un2 * ux) / R(2.0);
+    R wty = (-dtuy - dyut + ut * duy - uy * dut - t * un2 * uy) / R(2.0);
+    R wtn = (-t2 * dtun - R(2.0) * t * un - dnut - ut * Dun - t2 * un * dut - t3 * un * un2) / R(2.0);
+    R wxy = (dxuy - dyux + ux * duy - uy * dux) / R(2.0);
+    R wxn = (t2 * dxun - dnux - ux * Dun - t2 * un * dux) / R(2.0);
+    R wyn = (t2 * dyun - dnuy - uy * Dun - t2 * un * duy) / R(2.0);
+    R wxt = wtx, wyt = wty, wnt = wtn / t2, wyx = -wxy, wnx = -wxn / t2, wny = -wyn / t2;
+    R I1tt = R(2.0) * ut * (pitt * Dut + pitx * Dux + pity * Duy + pitn * Dun);
+    R I1tx = (pitt * ux + pitx * ut) * Dut + (pitx * ux + pixx * ut) * Dux + (pity * ux + pixy * ut) * Duy + (pitn * ux + pixn * ut) * Dun;
+    R I1ty = (pitt * uy + pity * ut) * Dut + (pitx * uy + pixy * ut) * Dux + (pity * uy + piyy * ut) * Duy + (pitn * uy + piyn * ut) * Dun;
+    R I1tn = (pitt * un + pitn * ut) * Dut + (pitx * un + pixn * ut) * Dux + (pity * un + piyn * ut) * Duy + (pitn * un + pinn * ut) * Dun;
+    R I1xx = R(2.0) * ux * (pitx * Dut + pixx * Dux + pixy * Duy + pixn * Dun);
+    R I1xy = (pitx * uy + pity * ux) * Dut + (pixx * uy + pixy * ux) * Dux + (pixy * uy + piyy * ux) * Duy + (pixn * uy + piyn * ux) * Dun;
+    R I1xn = (pitx * un + pitn * ux) * Dut + (pixx * un + pixn * ux) * Dux + (pixy * un + piyn * ux) * Duy + (pixn * un + pinn * ux) * Dun;
+    R I1yy = R(2.0) * uy * (pity * Dut + pixy * Dux + piyy * Duy + piyn * Dun);
+    R I1yn = (pity * un + pitn * uy) * Dut + (pixy * un + pixn * uy) * Dux + (piyy * un + piyn * uy) * Duy + (piyn * un + pinn * uy) * Dun;
+    R I1nn = R(2.0) * un * (pitn * Dut + pixn * Dux + piyn * Duy + pinn * Dun);
+    R I2tt = theta * pitt, I2tx = theta * pitx, I2ty = theta * pity, I2tn = theta * pitn, I2xx = theta * pixx;
+    R I2xy = theta * pixy, I2xn = theta * pixn, I2yy = theta * piyy, I2yn = theta * piyn, I2nn = theta * pinn;
+    R I3tt = R(2.0) * (pitx * wtx + pity * wty + pitn * wtn);
+    R I3tx = pitt * wxt + pity * wxy + pitn * wxn + pixx * wtx + pixy * wty + pixn * wtn;
+    R I3ty = pitt * wyt + pitx * wyx + pitn * wyn + pixy * wtx + piyy * wty + piyn * wtn;
+    R I3tn = pitt * wnt + pitx * wnx + pity * wny + pixn * wtx + piyn * wty + pinn * wtn;
+    R I3xx = R(2.0) * (pitx * wxt + pixy * wxy + pixn * wxn);
+    R I3xy = pitx * wyt + pity * wxt + pixx * wyx + piyy * wxy + pixn * wyn + piyn * wxn;
+    R I3xn = pitx * wnt + pitn * wxt + pixx * wnx + pixy * wny + piyn * wxy + pinn * wxn;
+    R I3yy = R(2.0) * (pity * wyt + pixy * wyx + piyn * wyn);
+    R I3yn = pity * wnt + pitn * wyt + pixy * wnx + pixn * wyx + piyy * wny + pinn * wyn;
+    R I3nn = R(2.0) * (pitn * wnt + pixn * wnx + piyn * wny);
+    R ux2 = ux * ux, uy2 = uy * uy;
+    R ps = pitt * stt - R(2.0) * pitx * stx - R(2.0) * pity * sty + pixx * sxx + R(2.0) * pixy * sxy + piyy * syy - R(2.0) * pitn * stn * t2 + R(2.0) * pixn * sxn * t2 + R(2.0) * piyn * syn * t2 + pinn * snn * t2 * t2;
+    R I4tt = (pitt * stt - pitx * stx - pity * sty - t2 * pitn * stn) - dvr((R(1.0) - ut2) * ps, R(3.0), kThird);
+    R I4tx = (pitt * stx + pitx * stt) / R(2.0) - (pitx * sxx + pixx * stx) / R(2.0) - (pity * sxy + pixy * sty) / R(2.0) - t2 * (pitn * sxn + pixn * stn) / R(2.0) + dvr((ut * ux) * ps, R(3.0), kThird);
+    R I4ty = (pitt * sty + pity * stt) / R(2.0) - (pitx * sxy + pixy * stx) / R(2.0) - (pity * syy + piyy * sty) / R(2.0) - t2 * (pitn * syn + piyn * stn) / R(2.0) + dvr((ut * uy) * ps, R(3.0), kThird);
+    R I4tn = (pitt * stn + pitn * stt) / R(2.0) - (pitx * sxn + pixn * stx) / R(2.0) - (pity * syn + piyn * sty) / R(2.0) - t2 * (pitn * snn + pinn * stn) / R(2.0) + dvr((ut * un) * ps, R(3.0), kThird);
+    R I4xx = (pitx * stx - pixx * sxx - pixy * sxy - t2 * pixn * sxn) + dvr((R(1.0) + ux2) * ps, R(3.0), kThird);
+    R I4xy = (pitx * sty + pity * stx) / R(2.0) - (pixx * sxy + pixy * sxx) / R(2.0) - (pixy * syy + piyy * sxy) / R(2.0) - t2 * (pixn * syn + piyn * sxn) / R(2.0) + dvr((ux * uy) * ps, R(3.0), kThird);
+    R I4xn = (pitx * stn + pitn * stx) / R(2.0) - (pixx * sxn + pixn * sxx) / R(2.0) - (pixy * syn + piyn * sxy) / R(2.0) - t2 * (pixn * snn + pinn * sxn) / R(2.0) + dvr((ux * un) * ps, R(3.0), kThird);
+    R I4yy = (pity * sty - pixy * sxy - piyy * syy - t2 * piyn * syn) + dvr((R(1.0) + uy2) * ps, R(3.0), kThird);
+    R I4yn = (pity * stn + pitn * sty) / R(2.0) - (pixy * sxn + pixn * sxy) / R(2.0) - (piyy * syn + piyn * syy) / R(2.0) - t2 * (piyn * snn + pinn * syn) / R(2.0) + dvr((uy * un) * ps, R(3.0), kThird);
+    R I4nn = (pitn * stn - pixn * sxn - piyn * syn - t2 * pinn * snn) + dvr((R(1.0) / t2 + un2) * ps, R(3.0), kThird);
+    R Itt = I1tt + delta_pipi * I2tt - I3tt + tau_pipi * I4tt - lambda_piPi * Pi * stt;
+    R Itx = I1tx + delta_pipi * I2tx - I3tx + tau_pipi * I4tx - lambda_piPi * Pi * stx;
+    R Ity = I1ty + delta_pipi * I2ty - I3ty + tau_pipi * I4ty - lambda_piPi * Pi * sty;
+    R Itn = I1tn + delta_pipi * I2tn - I3tn + tau_pipi * I4tn - lambda_piPi * Pi * stn;
+    R Ixx = I1xx + delta_pipi * I2xx - I3xx + tau_pipi * I4xx - lambda_piPi * Pi * sxx;
+    R Ixy = I1xy + delta_pipi * I2xy - I3xy + tau_pipi * I4xy - lambda_piPi * Pi * sxy;
+    R Ixn = I1xn + delta_pipi * I2xn - I3xn + tau_pipi * I4xn - lambda_piPi * Pi * sxn;
+    R Iyy = I1yy + delta_pipi * I2yy - I3yy + tau_pipi * I4yy - lambda_piPi * Pi * syy;
+    R Iyn = I1yn + delta_pipi * I2yn - I3yn + tau_pipi * I4yn - lambda_piPi * Pi * syn;
+    R Inn = I1nn + delta_pipi * I2nn - I3nn + tau_pipi * I4nn - lambda_piPi * Pi * snn;
+    R dpitt = R(2.0) * beta_pi * stt - pitt * taupiInv - Itt - R(2.0) * un * t * pitn;
+    R dpitx = R(2.0) * beta_pi * stx - pitx * taupiInv - Itx - un * t * pixn;
+    R dpity = R(2.0) * beta_pi * sty - pity * taupiInv - Ity - un * t * piyn;
+    R dpitn = R(2.0) * beta_pi * stn - pitn * taupiInv - Itn - un * t * pinn - (ut * pitn + un * pitt) / t;
+    R dpixx = R(2.0) * beta_pi * sxx - pixx * taupiInv - Ixx;
+    R dpixy = R(2.0) * beta_pi * sxy - pixy * taupiInv - Ixy;
+    R dpixn = R(2.0) * beta_pi * sxn - pixn * taupiInv - Ixn - (ut * pixn + un * pitx) / t;
+    R dpiyy = R(2.0) * beta_pi * syy - piyy * taupiInv - Iyy;
+    R dpiyn = R(2.0) * beta_pi * syn - piyn * taupiInv - Iyn - (ut * piyn + un * pity) / t;
+    R dpinn = R(2.0) * beta_pi * snn - pinn * taupiInv - Inn - 2 * (ut * pinn + un * pitn) / t;
+    rhs[0] = dvr(dpitt, ut, yut) + pitt * dkvk;
+    rhs[1] = dvr(dpitx, ut, yut) + pitx * dkvk;
+    rhs[2] = dvr(dpity, ut, yut) + pity * dkvk;
+    rhs[3] = dvr(dpitn, ut, yut) + pitn * dkvk;
+    rhs[4] = dvr(dpixx, ut, yut) + pixx * dkvk;
+    rhs[5] = dvr(dpixy, ut, yut) + pixy * dkvk;
+    rhs[6] = dvr(dpixn, ut, yut) + pixn * dkvk;
+    rhs[7] = dvr(dpiyy, ut, yut) + piyy * dkvk;
+    rhs[8] = dvr(dpiyn, ut, yut) + piyn * dkvk;
+    rhs[9] = dvr(dpinn, ut, yut) + pinn * dkvk;
     if (BULK) {
-        double dPi = -beta_Pi * theta - Pi * tauPiInv - delta_PiPi * Pi * theta + lambda_Pipi * ps;
-        rhs[10] = div_rcp(dPi, ut, yut) + Pi * dkvk;
+        R dPi = -beta_Pi * theta - Pi * tauPiInv - delta_PiPi * Pi * theta + lambda_Pipi * ps;
+        rhs[10] = dvr(dPi, ut, yut) + Pi * dkvk;
     }
 }
 

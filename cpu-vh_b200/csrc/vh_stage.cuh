@@ -172,7 +172,7 @@ __device__ __forceinline__ void source_update(const StageArgs &A, long long s, d
     S[1] = 0.0 - div_rcp(Qv[1], t, yt) - dxp + dkvk * Qv[5];
     S[2] = 0.0 - div_rcp(Qv[2], t, yt) - dyp + dkvk * Qv[6];
     S[3] = 0.0 - div_rcp(3 * Qv[3], t, yt) - dnp / A.t2pow + dkvk * Qv[7];
-    pimunu_rhs<EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, e, p, ut, ux, uy, un,
+    pimunu_rhs<double, EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, e, p, ut, ux, uy, un,
                               __ldg(A.upin + s), __ldg(A.upin + L + s), __ldg(A.upin + 2 * L + s), __ldg(A.upin + 3 * L + s),
                               Qv + 4, Pi, dxut, dyut, dnut, dxux, dyux, dnux, dxuy, dyuy, dnuy, dxun, dyun, dnun, dkvk,
                               A.etabar, A.dt);
@@ -336,6 +336,197 @@ __device__ __forceinline__ void final_body(const StageArgs &A, int i, int j, int
     regulate<NQ>(A, acc, P, bad);
     if (bad) raise_error(A.err, kErrNan, s, A.step);
     put_with_ghosts<NQ>(A, i, j, k, s, acc, P);
+}
+
+/* =====================================================================
+ * Mixed precision (vh_config.precision = VH_PREC_MIXED): the limiter, the
+ * flux arithmetic and the source terms in FP32; the conserved variables,
+ * their RK accumulation, the half-site states fed to the root solve, the
+ * root solve itself (infer) and the EoS stay FP64.  Differences of stored
+ * FP64 values are taken in FP64 before rounding to FP32, so no cancellation
+ * happens in FP32.  These bodies are instantiated only by the mixed
+ * translation unit (vh_mixed.cu, compiled with fast FP32 division).
+ * ===================================================================== */
+__device__ __forceinline__ float minmod_f(float x, float y)
+{
+    const float sx = (x < 0.f) ? -1.f : 1.f, sy = (y < 0.f) ? -1.f : 1.f;
+    return (sx + sy) * fminf(fabsf(x), fabsf(y)) * 0.5f;
+}
+
+/* FluxLimiter.cpp:14-32 on the FP64 differences y - x, z - x, z - y */
+__device__ __forceinline__ float slope_f(float th, double x, double y, double z)
+{
+    const float l = th * (float)(y - x), c = (float)(z - x) * 0.5f, r = th * (float)(z - y);
+    return minmod_f(l, minmod_f(c, r));
+}
+
+__device__ __forceinline__ void extrapolate_m(const double *__restrict__ qn, long long b, long long st, float th,
+                                              double &qR, double &qL)
+{
+    const double A = __ldg(qn + b - st), B = __ldg(qn + b), C = __ldg(qn + b + st), D = __ldg(qn + b + 2 * st);
+    qR = C - (double)(0.5f * slope_f(th, B, C, D));
+    qL = B + (double)(0.5f * slope_f(th, A, B, C));
+}
+
+/* face_flux with FP32 slopes and flux arithmetic; FP64 half-site states and root solve */
+template <int NQ, int EOS>
+__device__ __forceinline__ void face_flux_m(const StageArgs &A, long long b, long long st, int dir, bool fwd,
+                                            double ePrev, double *__restrict__ r, bool &bad)
+{
+    const float th = (float)A.theta;
+    const long long L = A.L;
+    const double *__restrict__ q = A.qin;
+    double qRs[8], qLs[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) extrapolate_m(q + c * L, b, st, th, qRs[c], qLs[c]);
+    double PiR = 0, PiL = 0;
+    if (NQ == 15) extrapolate_m(q + 14 * L, b, st, th, PiR, PiL);
+    Prim R = infer<EOS, true>(A.eos, A.t, qRs[0] - qRs[4], qRs[1] - qRs[5], qRs[2] - qRs[6], qRs[3] - qRs[7], PiR, ePrev, bad);
+    Prim Lf = infer<EOS, true>(A.eos, A.t, qLs[0] - qLs[4], qLs[1] - qLs[5], qLs[2] - qLs[6], qLs[3] - qLs[7], PiL, ePrev, bad);
+    const float vR = (float)((dir == 1) ? R.ux : (dir == 2) ? R.uy : R.un);
+    const float vL = (float)((dir == 1) ? Lf.ux : (dir == 2) ? Lf.uy : Lf.un);
+    const float sR = vR / (float)R.ut, sL = vL / (float)Lf.ut;
+    const float a = fmaxf(fabsf(sL), fabsf(sR));
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) {
+        double qR, qL;
+        if (n < 8) { qR = qRs[n]; qL = qLs[n]; }
+        else if (n == 14) { qR = PiR; qL = PiL; }
+        else extrapolate_m(q + n * L, b, st, th, qR, qL);
+        const float res = 0.5f * (sR * (float)qR + sL * (float)qL - a * (float)(qR - qL));
+        r[n] = fwd ? -(double)res : r[n] + (double)res;
+    }
+}
+
+/* source_update in FP32 (SourceTerms.cpp:421-612), accumulated onto the FP64 q */
+template <int NQ, int EOS>
+__device__ __forceinline__ void source_update_m(const StageArgs &A, long long s, double *__restrict__ acc)
+{
+    const long long L = A.L;
+    const float th = (float)A.theta;
+    const long long sx = 1, sy = A.ncx, sz = (long long)A.ncx * A.ncy;
+    double Qv[NQ];
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) Qv[n] = __ldg(A.qin + n * L + s);
+    const double *__restrict__ utv = A.uin, *__restrict__ uxv = A.uin + L, *__restrict__ uyv = A.uin + 2 * L,
+                 *__restrict__ unv = A.uin + 3 * L, *__restrict__ pv = A.pin;
+    const double e = __ldg(A.ein + s), p = __ldg(pv + s);
+    const double utd = __ldg(utv + s), uxd = __ldg(uxv + s), uyd = __ldg(uyv + s), und = __ldg(unv + s);
+    const float ydx = (float)A.inv_dx, ydy = (float)A.inv_dy, ydz = (float)A.inv_dz;
+#define SLOPE(v, c, st, y) (slope_f(th, __ldg((v) + s - (st)), (c), __ldg((v) + s + (st))) * (y))
+    const float dxut = SLOPE(utv, utd, sx, ydx), dxux = SLOPE(uxv, uxd, sx, ydx), dxuy = SLOPE(uyv, uyd, sx, ydx), dxun = SLOPE(unv, und, sx, ydx);
+    const float dyut = SLOPE(utv, utd, sy, ydy), dyux = SLOPE(uxv, uxd, sy, ydy), dyuy = SLOPE(uyv, uyd, sy, ydy), dyun = SLOPE(unv, und, sy, ydy);
+    const float dnut = SLOPE(utv, utd, sz, ydz), dnux = SLOPE(uxv, uxd, sz, ydz), dnuy = SLOPE(uyv, uyd, sz, ydz), dnun = SLOPE(unv, und, sz, ydz);
+    const float dxp = SLOPE(pv, p, sx, ydx), dyp = SLOPE(pv, p, sy, ydy), dnp = SLOPE(pv, p, sz, ydz);
+#undef SLOPE
+    const float t = (float)A.t, yt = (float)A.inv_t;
+    const float Pi = (NQ == 15) ? (float)Qv[14] : 0.f;
+    const float ut = (float)utd, ux = (float)uxd, uy = (float)uyd, un = (float)und;
+    const float pP = (float)p + Pi;
+    const float tnn = ((float)e + pP) * un * un + pP * yt * yt + (float)Qv[13];
+    const float yut = 1.f / ut;
+    const float vx = ux * yut, vy = uy * yut, vn = un * yut;
+    const float dkvk = (dxux - vx * dxut) * yut + (dyuy - vy * dyut) * yut + (dnun - vn * dnut) * yut;
+    float S[NQ];
+    S[0] = -((float)Qv[0] * yt + t * tnn) + dkvk * ((float)Qv[4] - (float)p - Pi) - vx * dxp - vy * dyp - vn * dnp;
+    S[1] = -(float)Qv[1] * yt - dxp + dkvk * (float)Qv[5];
+    S[2] = -(float)Qv[2] * yt - dyp + dkvk * (float)Qv[6];
+    S[3] = -3.f * (float)Qv[3] * yt - dnp / (float)A.t2pow + dkvk * (float)Qv[7];
+    float pvf[10];
+#pragma unroll
+    for (int n = 0; n < 10; ++n) pvf[n] = (float)Qv[4 + n];
+    pimunu_rhs<float, EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, e, p, utd, uxd, uyd, und,
+                                     __ldg(A.upin + s), __ldg(A.upin + L + s), __ldg(A.upin + 2 * L + s), __ldg(A.upin + 3 * L + s),
+                                     pvf, Pi, dxut, dyut, dnut, dxux, dyux, dnux, dxuy, dyuy, dnuy, dxun, dyun, dnun, dkvk,
+                                     (float)A.etabar, (float)A.dt);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) acc[n] = Qv[n] + A.dt * (double)S[n];
+}
+
+template <int NQ, int EOS>
+__device__ __forceinline__ void source_body_m(const StageArgs &A, long long s)
+{
+    double acc[NQ];
+    source_update_m<NQ, EOS>(A, s, acc);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] = acc[n];
+}
+
+template <int NQ, int EOS, int DIR>
+__device__ __forceinline__ void flux_body_m(const StageArgs &A, long long s)
+{
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    const long long st = (DIR == 1) ? 1 : (DIR == 2) ? (long long)A.ncx : (long long)A.ncx * A.ncy;
+    const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
+    const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
+    double r[NQ];
+#pragma unroll 1
+    for (int f = 0; f < 2; ++f) face_flux_m<NQ, EOS>(A, f == 0 ? s : s - st, st, DIR, f == 0, ePrev, r, bad);
+    double S[4];
+    dir_sources<NQ>(A, s, st, d, DIR, S);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) r[n] = (r[n] * yd + S[n]) * A.dt;
+#pragma unroll
+    for (int n = 4; n < NQ; ++n) r[n] *= yd * A.dt;
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] += r[n];
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+}
+
+/* the fused stage in mixed precision */
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
+__device__ __forceinline__ void stage_body_m(const StageArgs &A, int i, int j, int k, long long s)
+{
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    double acc[NQ];
+    source_update_m<NQ, EOS>(A, s, acc);
+#pragma unroll 1
+    for (int dir = 1; dir <= (HAS_Z ? 3 : 2); ++dir) {
+        const long long st = (dir == 1) ? 1 : (dir == 2) ? (long long)A.ncx : (long long)A.ncx * A.ncy;
+        const double d = (dir == 1) ? A.dx : (dir == 2) ? A.dy : A.dz;
+        const double yd = (dir == 1) ? A.inv_dx : (dir == 2) ? A.inv_dy : A.inv_dz;
+        double r[NQ];
+#pragma unroll 1
+        for (int f = 0; f < 2; ++f) face_flux_m<NQ, EOS>(A, f == 0 ? s : s - st, st, dir, f == 0, ePrev, r, bad);
+        double S[4];
+        dir_sources<NQ>(A, s, st, d, dir, S);
+#pragma unroll
+        for (int n = 0; n < 4; ++n) acc[n] += (r[n] * yd + S[n]) * A.dt;
+#pragma unroll
+        for (int n = 4; n < NQ; ++n) acc[n] += r[n] * yd * A.dt;
+    }
+    if (STAGE2) {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) acc[n] = (acc[n] + __ldg(A.qbase + n * A.L + s)) * 0.5;
+    }
+    Prim P = infer<EOS>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
+                        (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
+    regulate<NQ>(A, acc, P, bad);
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+    put_with_ghosts<NQ>(A, i, j, k, s, acc, P);
+}
+
+/* launch-form independent selection of the per-cell bodies: MIXED picks the
+ * mixed-precision source, flux and fused bodies; finalize is FP64 in both */
+template <int NQ, int EOS, bool MIXED>
+__device__ __forceinline__ void source_phase(const StageArgs &A, long long s)
+{
+    if constexpr (MIXED) source_body_m<NQ, EOS>(A, s);
+    else source_body<NQ, EOS>(A, s);
+}
+template <int NQ, int EOS, int DIR, bool MIXED>
+__device__ __forceinline__ void flux_phase(const StageArgs &A, long long s)
+{
+    if constexpr (MIXED) flux_body_m<NQ, EOS, DIR>(A, s);
+    else flux_body<NQ, EOS, DIR>(A, s);
+}
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2, bool MIXED>
+__device__ __forceinline__ void stage_phase(const StageArgs &A, int i, int j, int k, long long s)
+{
+    if constexpr (MIXED) stage_body_m<NQ, EOS, HAS_Z, STAGE2>(A, i, j, k, s);
+    else stage_body<NQ, EOS, HAS_Z, STAGE2>(A, i, j, k, s);
 }
 
 } // namespace vh

@@ -1,0 +1,120 @@
+/*
+ * vh_stage_kernels.cuh -- the single-event stage kernels and their launcher,
+ * templated on the precision mode.  vh_kt.cu instantiates the FP64 form
+ * (MIXED = false, bit-exact), vh_mixed.cu the mixed-precision form; the two
+ * translation units are compiled with different floating-point flags.
+ */
+#ifndef VH_STAGE_KERNELS_CUH
+#define VH_STAGE_KERNELS_CUH
+
+#include <cstdlib>
+#include "vh_stage.cuh"
+
+namespace vh {
+
+#ifndef VH_STAGE_MIN_BLOCKS
+#define VH_STAGE_MIN_BLOCKS 4   /* 128 registers: 16 warps/SM; measured faster than 2-3 blocks at 168-255 */
+#endif
+
+/* interior cell (i, j, k) of this thread, at padded index s */
+__device__ __forceinline__ bool stage_cell(const StageArgs &A, int &i, int &j, int &k, long long &s)
+{
+    i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    k = blockIdx.z + 2;
+    if (i >= A.nx + 2 || j >= A.ny + 2) return false;
+    s = i + (long long)A.ncx * j + (long long)A.ncx * A.ncy * k;
+    return true;
+}
+
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2, bool MIXED>
+__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_stage_kernel(const __grid_constant__ StageArgs A)
+{
+    int i, j, k;
+    long long s;
+    if (!stage_cell(A, i, j, k, s)) return;
+    stage_phase<NQ, EOS, HAS_Z, STAGE2, MIXED>(A, i, j, k, s);
+}
+
+/* Phase-split form of the same stage: five short kernels instead of one long
+ * one.  Each phase's code is a fraction of the fused kernel's and fits the
+ * instruction cache: the fused kernel spends most of its stall time waiting
+ * for instruction fetch on large lattices. */
+template <int NQ, int EOS, bool MIXED>
+__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_source_kernel(const __grid_constant__ StageArgs A)
+{
+    int i, j, k;
+    long long s;
+    if (!stage_cell(A, i, j, k, s)) return;
+    source_phase<NQ, EOS, MIXED>(A, s);
+}
+
+template <int NQ, int EOS, int DIR, bool MIXED>
+__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_kernel(const __grid_constant__ StageArgs A)
+{
+    int i, j, k;
+    long long s;
+    if (!stage_cell(A, i, j, k, s)) return;
+    flux_phase<NQ, EOS, DIR, MIXED>(A, s);
+}
+
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
+__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_final_kernel(const __grid_constant__ StageArgs A)
+{
+    int i, j, k;
+    long long s;
+    if (!stage_cell(A, i, j, k, s)) return;
+    final_body<NQ, EOS, HAS_Z, STAGE2>(A, i, j, k, s);
+}
+
+/* Fused for small lattices (launch- and latency-bound: one wave of threads,
+ * each carrying a whole stage), phase-split from 2^18 interior cells up
+ * (measured on B200: 131x131x61 split 5.43 ms/step vs fused 6.82; 101x101x1
+ * fused 0.120 ms vs split 0.163).  VH_STAGE_MODE=fused|split overrides. */
+static inline bool use_split(const StageArgs &a)
+{
+    static int forced = [] {
+        const char *e = getenv("VH_STAGE_MODE");
+        return !e ? -1 : (e[0] == 'f' ? 0 : 1);
+    }();
+    if (forced >= 0) return forced == 1;
+    return (long long)a.nx * a.ny * a.nz >= (1LL << 18);
+}
+
+template <int NQ, int EOS, bool MIXED>
+static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
+{
+    dim3 block(32, 4, 1);
+    dim3 grid((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
+    const bool z = a.nz > 1, st2 = a.qbase != nullptr;
+    if (m) { m->n = 0; cudaEventRecord(m->ev[0], s); }
+    auto mark = [&](int phase) {
+        if (!m) return;
+        m->phase[m->n] = phase;
+        cudaEventRecord(m->ev[++m->n], s);
+    };
+    if (!use_split(a)) {
+        if (z && st2) kt_stage_kernel<NQ, EOS, true, true, MIXED><<<grid, block, 0, s>>>(a);
+        else if (z) kt_stage_kernel<NQ, EOS, true, false, MIXED><<<grid, block, 0, s>>>(a);
+        else if (st2) kt_stage_kernel<NQ, EOS, false, true, MIXED><<<grid, block, 0, s>>>(a);
+        else kt_stage_kernel<NQ, EOS, false, false, MIXED><<<grid, block, 0, s>>>(a);
+        mark(5);
+        return;
+    }
+    kt_source_kernel<NQ, EOS, MIXED><<<grid, block, 0, s>>>(a);
+    mark(0);
+    kt_flux_kernel<NQ, EOS, 1, MIXED><<<grid, block, 0, s>>>(a);
+    mark(1);
+    kt_flux_kernel<NQ, EOS, 2, MIXED><<<grid, block, 0, s>>>(a);
+    mark(2);
+    if (z) { kt_flux_kernel<NQ, EOS, 3, MIXED><<<grid, block, 0, s>>>(a); mark(3); }
+    if (z && st2) kt_final_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
+    else if (z) kt_final_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
+    else if (st2) kt_final_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);
+    else kt_final_kernel<NQ, EOS, false, false><<<grid, block, 0, s>>>(a);
+    mark(4);
+}
+
+} // namespace vh
+
+#endif

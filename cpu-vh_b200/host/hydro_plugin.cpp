@@ -416,6 +416,7 @@ static void read_plugin_properties(const char *configDirectory)
         else if (k == "zeta_norm") P.phys.zeta_norm = atof(v.c_str());
         else if (k == "zeta_T0_GeV") P.phys.zeta_T0_GeV = atof(v.c_str());
         else if (k == "zeta_width_GeV") P.phys.zeta_width_GeV = atof(v.c_str());
+        else if (k == "precision") P.phys.precision = (v == "mixed") ? VH_PREC_MIXED : VH_PREC_FP64;
     }
 }
 

@@ -19,7 +19,7 @@
  * EOS_FACTOR, PI) default to its shipped values and can be changed at run
  * time with vh_plugin_set_config() or an optional <configDir>/b200.properties
  * file (named keys: theta, eos, eos_factor, eos_table, bulk, zeta_law,
- * zeta_norm, zeta_T0_GeV, zeta_width_GeV).
+ * zeta_norm, zeta_T0_GeV, zeta_width_GeV, precision = fp64 | mixed).
  */
 #ifndef CPU_VH_H
 #define CPU_VH_H

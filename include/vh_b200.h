@@ -50,8 +50,8 @@ extern "C" {
 
 /* arithmetic modes */
 #define VH_PREC_FP64       0   /* FP64 throughout, op-for-op with the reference (parity)  */
-#define VH_PREC_MIXED      1   /* FP32 limiter/flux/source arithmetic and FP32 storage of  */
-                               /* e, p, u; FP64 conserved accumulation and root solve      */
+#define VH_PREC_MIXED      1   /* FP32 limiter, flux and source arithmetic; FP64 conserved */
+                               /* variables, RK accumulation, root solve, EoS and storage  */
 
 /* field ids for vh_event_get_field / vh_event_set_field */
 #define VH_F_Q0            0   /* 0..14: ttt ttx tty ttn pitt pitx pity pitn pixx pixy pixn piyy piyn pinn Pi */

@@ -1,0 +1,139 @@
+"""Mixed precision (VH_PREC_MIXED): FP32 limiter, flux and source arithmetic
+with FP64 accumulation and root solve, against the FP64 path (bit-identical
+to the oracle and the reference).
+
+The reference's scheme is chaotic in the dilute edge region: its discrete
+switches (the e <= 0.1 inversion branch, EnergyMomentumTensor.cpp:188-191;
+the e < e_reg regulation threshold; the u^tau > 1e3 reset) turn any
+perturbation into O(1) local differences, so a relative change of 2^-50 in
+the initial energy density alone grows to ~8 % relative L-infinity in e after
+the Gubser event's 300 steps.  The mixed path is therefore checked (a) to
+1e-4 relative L-infinity (max |a - b| / max |b|) before that growth sets in,
+and (b) at the end of the event against the FP64 path's own sensitivity: its
+error must stay within a small factor of what a one-ulp-scale perturbation of
+the FP64 run produces."""
+import numpy as np
+import pytest
+
+import vh
+from oracle import OracleEvent
+
+pytestmark = pytest.mark.gpu
+
+
+def rel_linf(a, b):
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def _run(cfg, rows, st, steps, mixed):
+    c = cfg.copy(precision=vh.VH_PREC_MIXED if mixed else vh.VH_PREC_FP64)
+    ev = vh.Event(c, rows)
+    ev.set_initial(st)
+    ev.step(steps)
+    ev.sync()
+    return ev
+
+
+def _errors(cfg, ev, orc):
+    out = {}
+    for name, fid in [("e", vh.VH_F_E), ("ut", vh.VH_F_UT), ("ux", vh.VH_F_UT + 1), ("uy", vh.VH_F_UT + 2),
+                      ("pixx", 8), ("pixy", 9), ("piyy", 11), ("pinn", 13)]:
+        out[name] = rel_linf(vh.interior(cfg, ev.field(fid)), vh.interior(cfg, orc.field(fid)))
+    return out
+
+
+def test_gubser_mixed_vs_fp64():
+    cfg = vh.gubser_config()
+    st = vh.gubser_ic(cfg)
+    err = _errors(cfg, _run(cfg, None, st, 30, True), _run(cfg, None, st, 30, False))
+    assert max(err.values()) <= 1e-4, err
+
+
+def test_gubser_mixed_error_within_fp64_sensitivity():
+    """the full Gubser event (101 x 101, 300 steps)"""
+    cfg = vh.gubser_config()
+    st = vh.gubser_ic(cfg)
+    bumped = vh.gubser_ic(cfg)
+    bumped.e = bumped.e * (1 + 2.0 ** -50)
+    ref = _run(cfg, None, st, 300, False)
+    mixed = _errors(cfg, _run(cfg, None, st, 300, True), ref)
+    floor = _errors(cfg, _run(cfg, None, bumped, 300, False), ref)
+    assert floor["e"] > 1e-3, floor           # the chaotic growth this test is built around
+    for k in ("e", "ut", "ux", "uy"):
+        assert mixed[k] <= 3 * floor[k], (k, mixed, floor)
+
+
+def test_glauber_mixed_vs_oracle():
+    cfg = vh.glauber_config(27, 25, 9)
+    cfg.dx = cfg.dy = 0.5
+    cfg.dz = 0.4
+    cfg.dt = 0.05
+    rows = vh.synthetic_eos_table()
+    st = vh.glauber_ic(cfg, rows)
+    ev = _run(cfg, rows, st, 40, True)
+    orc = OracleEvent(cfg, rows)
+    orc.set_initial(st)
+    assert orc.step(40) == 0
+    err = _errors(cfg, ev, orc)
+    err["Pi"] = rel_linf(vh.interior(cfg, ev.field(14)), vh.interior(cfg, orc.field(14)))
+    assert err["e"] <= 1e-4, err
+    assert ev.status()[0] == 0
+
+
+def _surface_sums(ev, steps, fo_every):
+    ev.freezeout()
+    tot = np.zeros(4)
+    count = 0
+    for _ in range(steps // fo_every):
+        ev.step(fo_every)
+        n, _ = ev.freezeout()
+        if n:
+            s = ev.surface()
+            tot += s[:, 4:8].sum(axis=0)
+            count += n
+    return count, tot
+
+
+def test_freezeout_surface_mixed_vs_fp64():
+    cfg = vh.gubser_config()
+    st = vh.gubser_ic(cfg)
+    bumped = vh.gubser_ic(cfg)
+    bumped.e = bumped.e * (1 + 2.0 ** -50)
+    res = {}
+    for key, prec, ic in (("fp64", vh.VH_PREC_FP64, st), ("mixed", vh.VH_PREC_MIXED, st),
+                          ("fp64_bumped", vh.VH_PREC_FP64, bumped)):
+        ev = vh.Event(cfg.copy(precision=prec))
+        ev.set_initial(ic)
+        res[key] = _surface_sums(ev, 300, 10)
+    n64, s64 = res["fp64"]
+    assert n64 > 0
+    for key in ("mixed", "fp64_bumped"):
+        n, s = res[key]
+        res[key] = (abs(n - n64) / n64, float(np.max(np.abs(s - s64)) / np.max(np.abs(s64))))
+    dn, ds = res["mixed"]
+    fn, fs = res["fp64_bumped"]
+    assert dn <= max(0.005, 3 * fn), res
+    assert ds <= max(1e-4, 3 * fs), res
+
+
+def test_batched_mixed_matches_single_mixed():
+    rows = vh.synthetic_eos_table()
+    cfgs = [vh.hotspot_config(n).copy(precision=vh.VH_PREC_MIXED) for n in (25, 33)]
+    ics = [vh.hotspot_ic(c, rows, seed=9 + i) for i, c in enumerate(cfgs)]
+    evs, ref = [], []
+    for c, st in zip(cfgs, ics):
+        for lst in (evs, ref):
+            e = vh.Event(c, rows)
+            e.set_initial(st)
+            lst.append(e)
+    b = vh.Batch(evs)
+    b.step(20)
+    for c, e, r in zip(cfgs, evs, ref):
+        r.step(20)
+        e.sync()
+        r.sync()
+        assert rel_linf(vh.interior(c, e.field(vh.VH_F_E)), vh.interior(c, r.field(vh.VH_F_E))) <= 1e-9
+    with pytest.raises(vh.VhError):
+        x = vh.Event(vh.hotspot_config(15), rows)
+        x.set_initial(vh.hotspot_ic(x.cfg, rows, seed=1))
+        vh.Batch([evs[0], x])
