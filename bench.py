@@ -77,6 +77,8 @@ def parse():
     ap.add_argument("--workload", default="glauber_3p1d",
                     choices=["glauber_3p1d", "gubser_2p1d", "batch_hotspots_2p1d"])
     ap.add_argument("--events", type=int, default=256, help="batch_hotspots_2p1d: events in the batch")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
+                    help="mixed: FP32 limiter/flux/source arithmetic, FP64 accumulation and root solve")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     return ap.parse_args()
@@ -115,6 +117,45 @@ def batch_workload(n_events):
             "mean peak 20 GeV/fm^3, centres in the b=0 Woods-Saxon overlap, 2000-row synthetic EoS, eta/s=0.08, "
             "Gaussian zeta/s (bulk on), FP64")
     return cfgs, rows, ics, desc
+
+
+def precision_report(cfg, rows, st, steps, ev_mixed):
+    """Error of a mixed-precision event after `steps` steps against the FP64
+    path (bit-identical to the oracle), next to the FP64 path's own
+    sensitivity: the same FP64 run from an initial energy density scaled by
+    (1 + 2^-50).  Relative L-infinity = max|a - b| / max|b|, relative L2 =
+    |a - b|_2 / |b|_2, over the interior cells."""
+    import numpy as np
+    import vh
+    fields = [("e", vh.VH_F_E), ("ut", vh.VH_F_UT), ("ux", vh.VH_F_UT + 1), ("uy", vh.VH_F_UT + 2),
+              ("un", vh.VH_F_UT + 3), ("pixx", 8), ("pixy", 9), ("piyy", 11), ("pinn", 13)]
+    if cfg.bulk:
+        fields.append(("Pi", 14))
+
+    def run(ic):
+        e = vh.Event(cfg.copy(precision=vh.VH_PREC_FP64), rows)
+        e.set_initial(ic)
+        e.step(steps)
+        e.sync()
+        return e
+
+    def errs(a_ev, b_ev):
+        out = {}
+        for name, fid in fields:
+            a = vh.interior(cfg, a_ev.field(fid)).ravel()
+            b = vh.interior(cfg, b_ev.field(fid)).ravel()
+            d = a - b
+            out[name] = {"linf": float(np.max(np.abs(d)) / max(np.max(np.abs(b)), 1e-300)),
+                         "l2": float(np.linalg.norm(d) / max(np.linalg.norm(b), 1e-300))}
+        return out
+
+    ref = run(st)
+    bumped = vh.InitialState(st.e * (1 + 2.0 ** -50), st.p, st.u, st.pi, st.Pi)
+    floor = run(bumped)
+    rep = {"steps": steps, "mixed_vs_fp64": errs(ev_mixed, ref), "fp64_sensitivity": errs(floor, ref)}
+    ref.close()
+    floor.close()
+    return rep
 
 
 def measured_peaks():
@@ -264,6 +305,10 @@ def run_batch(args, torch, world, rank, barrier, max_over_ranks):
     import numpy as np
     import vh
     cfgs, rows, ics, desc = batch_workload(args.events)
+    mixed = args.precision == "mixed"
+    if mixed:
+        cfgs = [c.copy(precision=vh.VH_PREC_MIXED) for c in cfgs]
+        desc = desc.replace("FP64", "mixed precision")
     Ns = [c.nx * c.ny * c.nz for c in cfgs]
     Ntot = sum(Ns)
     evs = []
@@ -311,13 +356,24 @@ def run_batch(args, torch, world, rank, barrier, max_over_ranks):
     alg_bytes = phase_words(cfgs[0].nq())[dom] * 8 * Ntot
     achieved = alg_bytes / launch_s / 1e9
 
-    # the plain single-event path on the same events, one event at a time
+    prec = None
+    if mixed and rank == 0:
+        reps = [precision_report(c.copy(precision=vh.VH_PREC_FP64), rows, st, e.progress()[0], e)
+                for c, st, e in list(zip(cfgs, ics, evs))[:4]]
+        prec = {"members": "the first 4 events of the batch, worst case over them", "steps": reps[0]["steps"]}
+        for key in ("mixed_vs_fp64", "fp64_sensitivity"):
+            prec[key] = {f: {m: max(r[key][f][m] for r in reps) for m in ("linf", "l2")} for f in reps[0][key]}
+
+    # the plain single-event FP64 path on the same events, one event at a time
     solo_steps = max(1, min(args.steps, 10))
-    for e, st in zip(evs, ics):
+    solo = []
+    for c, st in zip(cfgs, ics):
+        e = vh.Event(c.copy(precision=vh.VH_PREC_FP64), rows)
         e.set_initial(st)
+        solo.append(e)
     t_solo = 0.0
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for e in evs:
+    for e in solo:
         es = torch.cuda.ExternalStream(e.stream())
         e.step(1)
         s0.record(es)
@@ -326,6 +382,8 @@ def run_batch(args, torch, world, rank, barrier, max_over_ranks):
         s1.synchronize()
         t_solo += s0.elapsed_time(s1)
     solo_value = Ntot * solo_steps / (t_solo / 1e3)
+    for e in solo:
+        e.close()
 
     e2e = None
     if not args.no_e2e:
@@ -370,15 +428,16 @@ def run_batch(args, torch, world, rank, barrier, max_over_ranks):
     if rank == 0:
         line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32/f64 mixed" if mixed else "f64", "data": "synthetic",
                 "config": {"workload": desc, "events": len(cfgs), "cells": Ntot, "parallelism": f"replicas x{world}",
                            "l2": "batch state > 126 MB L2, no flush", "tuning": tune.describe()},
                 "events_per_s": value / Ntot / EVENT_STEPS * len(cfgs),
                 "events_per_s_note": f"events of {EVENT_STEPS} RK2 steps, from the batched step time",
                 "plain_single_event": {"value": solo_value, "unit": "cell-updates/s",
                                        "events_per_s": solo_value / Ntot / EVENT_STEPS * len(cfgs),
-                                       "how": f"vh_event_step, one event at a time, {solo_steps} steps each, "
+                                       "speedup_of_batch": value / solo_value,
+                                       "how": f"FP64 vh_event_step, one event at a time, {solo_steps} steps each, "
                                               "CUDA events per event"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": None,
@@ -388,6 +447,8 @@ def run_batch(args, torch, world, rank, barrier, max_over_ranks):
                              "note": f"peak: {peak_kind} HBM copy bandwidth; FP64-issue bound"},
                 "phases_ms_per_step": {k: t / args.steps for k, (t, _) in phases.items()},
                 "clocks": clk, "gpu_launches": b.launches_per_step() * args.steps}
+        if prec:
+            line["precision_error"] = prec
         if e2e:
             line["e2e"] = e2e
         if base:
@@ -417,6 +478,10 @@ def main():
         R.close()
         return rc
     cfg, rows, st, variant, desc = workload(args.workload)
+    mixed = args.precision == "mixed"
+    if mixed:
+        cfg = cfg.copy(precision=vh.VH_PREC_MIXED)
+        desc = desc.replace("FP64", "mixed precision") if "FP64" in desc else desc + ", mixed precision"
     N = cfg.nx * cfg.ny * cfg.nz
     px, py, pz = cfg.padded()
     state_mb = (3 * cfg.nq() + 16) * px * py * pz * 8 / 1e6   # q x3, e/p x2, u x3 planes
@@ -496,6 +561,10 @@ def main():
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": outp.nbytes / args.steps,
                "timer": "host wall clock, pinned buffers, IC upload + K steps + e download"}
 
+    prec = None
+    if mixed and rank == 0:
+        prec = precision_report(cfg, rows, st, ev.progress()[0], ev)
+
     base = None
     if rank == 0 and world == 1 and not args.no_baseline:
         base = cpu_baseline(cfg, rows, st, variant)
@@ -503,8 +572,8 @@ def main():
     if rank == 0:
         line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic",
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32/f64 mixed" if mixed else "f64", "data": "synthetic",
                 "config": {"workload": desc, "cells": N, "parallelism": f"replicas x{world}",
                            "l2": l2_note},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -516,6 +585,8 @@ def main():
                                      "step is bound by FP64 issue latency, not HBM"},
                 "phases_ms_per_step": {k: t / args.steps for k, (t, _) in phases.items()},
                 "clocks": clk, "gpu_launches": ev.launches_per_step() * args.steps}
+        if prec:
+            line["precision_error"] = prec
         if e2e:
             line["e2e"] = e2e
         if base:

@@ -245,7 +245,9 @@ __device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, R *rhs, R t, double e
     R beta_Pi = 15 * a2 * (e + p);
     R lambda_Pipi = 8 * a / 5;
     R tauPiInv = R(0.0);
-    if (BULK) tauPiInv = 15 * a2 * T / R(zeta_over_s(Z, double(T)));
+    /* in FP64 for both precisions: zeta/s underflows FP32 far from its peak
+     * while a2 = 0 for both EoS kinds, and 0/0 must not appear */
+    if (BULK) tauPiInv = R(15 * double(a2) * double(T) / zeta_over_s(Z, double(T)));
     R ut2 = ut * ut, un2 = un * un, t2 = t * t, t3 = t * t2;
     const R kThird = R(1.0) / R(3.0), yut = R(1.0) / ut, ydt = R(1.0) / d_dt;
     R dtut = dvr(R(ut_d - utp), d_dt, ydt), dtux = dvr(R(ux_d - uxp), d_dt, ydt), dtuy = dvr(R(uy_d - uyp), d_dt, ydt), dtun = dvr(R(un_d - unp), d_dt, ydt);
