@@ -75,7 +75,9 @@ def parse():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="glauber_3p1d",
-                    choices=["glauber_3p1d", "gubser_2p1d", "batch_hotspots_2p1d"])
+                    choices=["glauber_3p1d", "gubser_2p1d", "batch_hotspots_2p1d", "serve_mix"])
+    ap.add_argument("--rate", type=float, default=6.0, help="serve_mix: Poisson arrival rate (events/s)")
+    ap.add_argument("--max-steps", type=int, default=100, help="serve_mix: RK2 steps after which an event retires")
     ap.add_argument("--events", type=int, default=256, help="batch_hotspots_2p1d: events in the batch")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 limiter/flux/source arithmetic, FP64 accumulation and root solve")
@@ -156,6 +158,105 @@ def precision_report(cfg, rows, st, steps, ev_mixed):
     ref.close()
     floor.close()
     return rep
+
+
+def serve_stream(n_events, rate, seed=2025):
+    """The served mix: 70 % 2+1D lumpy events (n x n, n uniform in 61..201
+    step 20, hotspot initial conditions) and 30 % 3+1D smooth events (n x n x
+    n_eta, n uniform in 101..201 step 20, n_eta in 21..81 step 20, optical
+    Glauber with b uniform in 0-12 fm); Poisson arrivals at `rate`."""
+    import numpy as np
+    import vh
+    rng = np.random.default_rng(seed)
+    rows = vh.synthetic_eos_table()
+    t, out = 0.0, []
+    for i in range(n_events):
+        t += rng.exponential(1.0 / rate)
+        if rng.random() < 0.7:
+            c = vh.hotspot_config(int(rng.choice(np.arange(61, 202, 20))))
+            c.fo_factor = 10
+            st = vh.hotspot_ic(c, rows, seed=10_000 + i)
+        else:
+            n = int(rng.choice(np.arange(101, 202, 20)))
+            c = vh.glauber_config(n, n, int(rng.choice([21, 41, 61, 81])))
+            c.fo_factor = 10
+            st = vh.glauber_ic(c, rows, b=float(rng.uniform(0.0, 12.0)))
+        out.append((t, c, st))
+    desc = (f"serve_mix: {n_events} events, Poisson arrivals at {rate:g}/s (seed {seed}); 70% 2+1D hotspot events "
+            "n x n, n in 61..201 step 20; 30% 3+1D optical-Glauber events n x n x n_eta, n in 101..201 step 20, "
+            "n_eta in 21..81 step 20, b uniform 0-12 fm; freezeout every 10 steps, surfaces to host")
+    return out, rows, desc
+
+
+def pct(xs, q):
+    import numpy as np
+    return float(np.percentile(np.asarray(xs), q)) if len(xs) else None
+
+
+def run_serve(args, rank):
+    """The event server under a Poisson stream, next to the same stream served
+    one event at a time by the plain FP64 path (FCFS queue over the measured
+    per-event service times)."""
+    import numpy as np
+    import vh
+    stream, rows, desc = serve_stream(args.events, args.rate)
+    mixed = args.precision == "mixed"
+    prec = vh.VH_PREC_MIXED if mixed else vh.VH_PREC_FP64
+    srv = vh.Server(rows, hbm_fraction=0.8, max_steps=args.max_steps)
+    # warm the server (tuning, modules) on one small event outside the timed stream
+    wc = vh.hotspot_config(61).copy(precision=prec)
+    srv.submit(wc, vh.hotspot_ic(wc, rows, seed=1), 1 << 40)
+    srv.wait(600)
+    srv.poll()
+    srv.take_surface(1 << 40)
+    t_start = time.perf_counter()
+    base = None
+    for i, (t_arr, c, st) in enumerate(stream):
+        dt = t_arr - (time.perf_counter() - t_start)
+        if dt > 0:
+            time.sleep(dt)
+        srv.submit(c.copy(precision=prec), st, i)
+    srv.wait(3600)
+    done = srv.poll(len(stream) + 16)
+    stats = srv.stats()
+    lat = [d.t_done - d.t_submit for d in done]
+    first = min(d.t_submit for d in done)
+    span = max(d.t_done for d in done) - first
+    cells = sum(d.steps * c.nx * c.ny * c.nz for d, (_, c, _) in zip(sorted(done, key=lambda d: d.tag), stream))
+    bad = [d.tag for d in done if d.status != 0]
+    srv.close()
+
+    # the plain path: each event alone, FP64, same cadence and cap, FCFS
+    service, serial_bad = [], []
+    for i, (_, c, st) in enumerate(stream):
+        t0 = time.perf_counter()
+        _, _, status = vh.run_like_server(c.copy(precision=vh.VH_PREC_FP64), rows, st, max_steps=args.max_steps)
+        service.append(time.perf_counter() - t0)
+        if status:
+            serial_bad.append(i)
+    free_at, slat = 0.0, []
+    for (t_arr, _, _), sv in zip(stream, service):
+        start = max(t_arr, free_at)
+        free_at = start + sv
+        slat.append(free_at - t_arr)
+    serial_span = free_at - stream[0][0]
+
+    line = {"metric": "events/s", "value": len(done) / span, "unit": "events/s", "n_gpus": 1,
+            "steps": None, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32/f64 mixed" if mixed else "f64", "data": "synthetic",
+            "config": {"workload": desc, "events": len(stream), "max_steps": args.max_steps,
+                       "admission": "80% of free HBM", "precision": args.precision},
+            "latency_s": {"p50": pct(lat, 50), "p95": pct(lat, 95), "p99": pct(lat, 99), "max": max(lat)},
+            "cell_updates_per_s": cells / span,
+            "server": {k: stats[k] for k in ("steps", "fo_blocks", "batch_builds")} | {"events_with_device_error": bad},
+            "serial_plain_fp64": {"events_per_s": len(stream) / serial_span,
+                                  "latency_s": {"p50": pct(slat, 50), "p95": pct(slat, 95), "p99": pct(slat, 99)},
+                                  "events_with_device_error": serial_bad,
+                                  "how": "each event alone through vh_event_step/freezeout (FP64), same cadence "
+                                         "and step cap; FCFS queue over the measured service times"}}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
 
 
 def measured_peaks():
@@ -475,6 +576,10 @@ def main():
 
     if args.workload == "batch_hotspots_2p1d":
         rc = run_batch(args, torch, world, rank, barrier, max_over_ranks)
+        R.close()
+        return rc
+    if args.workload == "serve_mix":
+        rc = run_serve(args, rank)
         R.close()
         return rc
     cfg, rows, st, variant, desc = workload(args.workload)

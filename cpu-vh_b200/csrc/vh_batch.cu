@@ -295,6 +295,7 @@ int check_members(vh_batch *b)
     for (size_t m = 0; m < b->mem.size(); ++m) {
         vh_event *ev = b->mem[m];
         if (!ev->initialised) return bfail(VH_ERR_STATE, "batch member " + std::to_string(m) + " has no initial state");
+        if (ev->fo_pending) return bfail(VH_ERR_STATE, "batch member " + std::to_string(m) + " has a freezeout block pending");
         const int c = ev->n & 1;
         if (ev->qc != c || ev->qn != 1 - c || ev->qs != 2 || ev->uc != c || ev->up != 1 - c || ev->us != 2 || ev->ec != 0)
             return bfail(VH_ERR_STATE, "batch member " + std::to_string(m) + ": unexpected buffer roles");

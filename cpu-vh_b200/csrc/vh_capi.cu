@@ -109,6 +109,8 @@ int vh_event_destroy(vh_event *ev)
     cudaFree(ev->fo_slabs);
     cudaFree(ev->fo_scratch);
     cudaFree(ev->fo_elems);
+    if (ev->fo_hdr) cudaFreeHost(ev->fo_hdr);
+    if (ev->fo_done) cudaEventDestroy(ev->fo_done);
     for (auto &m : ev->marks)
         for (cudaEvent_t e : m.ev) cudaEventDestroy(e);
     if (ev->stream) cudaStreamDestroy(ev->stream);
@@ -171,6 +173,7 @@ int vh_event_create(const vh_config *cfg, const double *eos_rows, int eos_nrows,
 
 static int do_init(vh_event *ev, const double *d_e, const double *d_p, const double *d_u, const double *d_pi, const double *d_Pi)
 {
+    if (ev->fo_pending) return fail(VH_ERR_STATE, "new initial state with a freezeout block pending");
     vh::InitArgs a;
     a.e = d_e; a.p = d_p; a.u = d_u; a.pi = d_pi; a.Pi = d_Pi;
     ev->qc = 0; ev->qn = 1; ev->qs = 2; ev->ec = 0; ev->uc = 0; ev->up = 1; ev->us = 2;
@@ -230,6 +233,7 @@ int vh_event_step(vh_event *ev, int nsteps)
 {
     if (!ev || nsteps < 0) return fail(VH_ERR_ARG, "bad argument");
     if (!ev->initialised) return fail(VH_ERR_STATE, "vh_event_step before vh_event_set_initial");
+    if (ev->fo_pending) return fail(VH_ERR_STATE, "vh_event_step with a freezeout block pending");
     const vh_config &c = ev->cfg;
     vh::StageArgs A = vh::stage_args_base(ev);
     const bool mixed = c.precision == VH_PREC_MIXED;
@@ -376,19 +380,10 @@ int vh_event_powf_misses(vh_event *ev, unsigned long long *misses)
 }
 
 /* ------------------------------------------------------------ freezeout */
-int vh_event_freezeout(vh_event *ev, int *n_elements, int *n_above)
+static void fo_args(vh_event *ev, vh::FoArgs &a)
 {
-    if (!ev) return fail(VH_ERR_ARG, "null event");
-    if (!ev->initialised) return fail(VH_ERR_STATE, "freezeout before vh_event_set_initial");
     const vh_config &c = ev->cfg;
     const size_t N = (size_t)ev->N;
-    if (!ev->fo_slabs) {
-        CUDA_TRY(cudaMalloc(&ev->fo_slabs, 2 * 11 * N * sizeof(double)));
-        CUDA_TRY(cudaMemsetAsync(ev->fo_slabs, 0, 2 * 11 * N * sizeof(double), ev->stream));
-        ev->fo_scratch_ints = vh::freezeout_scratch_ints(c.nx, c.ny, c.nz);
-        CUDA_TRY(cudaMalloc(&ev->fo_scratch, ev->fo_scratch_ints * sizeof(int)));
-    }
-    vh::FoArgs a;
     a.q = ev->q[ev->qc]; a.e = ev->ep[ev->ec]; a.u = ev->u[ev->uc];
     a.L = ev->L; a.nx = c.nx; a.ny = c.ny; a.nz = c.nz; a.ncx = ev->ncx; a.ncy = ev->ncy; a.nq = ev->nq;
     a.slab_prev = ev->fo_slabs + (size_t)ev->fo_prev * 11 * N;
@@ -405,31 +400,70 @@ int vh_event_freezeout(vh_event *ev, int *n_elements, int *n_above)
     a.n_total = nullptr;
     a.elems = ev->fo_elems;
     a.cap = ev->fo_cap;
-    /* first pass: counts and the total; grows the element buffer if needed */
-    int total = 0, above = 0;
-    for (int pass = 0; pass < 2; ++pass) {
-        a.elems = ev->fo_elems;
-        a.cap = ev->fo_cap;
-        vh::launch_freezeout(a, ev->stream);
-        CUDA_TRY(cudaGetLastError());
-        int hdr[2];
-        size_t sc = ev->fo_scratch_ints;
-        CUDA_TRY(cudaMemcpyAsync(hdr, ev->fo_scratch + sc - 2, sizeof(hdr), cudaMemcpyDeviceToHost, ev->stream));
-        CUDA_TRY(cudaStreamSynchronize(ev->stream));
-        above = hdr[0];
-        total = hdr[1];
-        if (total <= ev->fo_cap) break;
-        /* not enough room: re-run with a larger buffer from the same slabs */
+}
+
+int vh_event_freezeout_launch(vh_event *ev)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    if (!ev->initialised) return fail(VH_ERR_STATE, "freezeout before vh_event_set_initial");
+    if (ev->fo_pending) return fail(VH_ERR_STATE, "a freezeout block is already pending");
+    const vh_config &c = ev->cfg;
+    const size_t N = (size_t)ev->N;
+    if (!ev->fo_slabs) {
+        CUDA_TRY(cudaMalloc(&ev->fo_slabs, 2 * 11 * N * sizeof(double)));
+        CUDA_TRY(cudaMemsetAsync(ev->fo_slabs, 0, 2 * 11 * N * sizeof(double), ev->stream));
+        ev->fo_scratch_ints = vh::freezeout_scratch_ints(c.nx, c.ny, c.nz);
+        CUDA_TRY(cudaMalloc(&ev->fo_scratch, ev->fo_scratch_ints * sizeof(int)));
+        CUDA_TRY(cudaMallocHost(&ev->fo_hdr, 2 * sizeof(int)));
+        CUDA_TRY(cudaEventCreateWithFlags(&ev->fo_done, cudaEventDisableTiming));
+    }
+    vh::FoArgs a;
+    fo_args(ev, a);
+    vh::launch_freezeout(a, ev->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(ev->fo_hdr, ev->fo_scratch + ev->fo_scratch_ints - 2, 2 * sizeof(int),
+                             cudaMemcpyDeviceToHost, ev->stream));
+    CUDA_TRY(cudaEventRecord(ev->fo_done, ev->stream));
+    ev->fo_pending = true;
+    return VH_OK;
+}
+
+int vh_event_freezeout_finish(vh_event *ev, int *n_elements, int *n_above)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    if (!ev->fo_pending) return fail(VH_ERR_STATE, "no freezeout block pending");
+    ev->fo_pending = false;
+    CUDA_TRY(cudaEventSynchronize(ev->fo_done));
+    int above = ev->fo_hdr[0], total = ev->fo_hdr[1];
+    if (total > ev->fo_cap) {
+        /* not enough room: re-run with a larger buffer from the same slabs
+         * (the slab shift is idempotent) */
         cudaFree(ev->fo_elems);
+        ev->fo_elems = nullptr;
         ev->fo_cap = total + total / 4 + 1024;
         CUDA_TRY(cudaMalloc(&ev->fo_elems, (size_t)ev->fo_cap * VH_FO_COLUMNS * sizeof(double)));
-        a.slab_prev = ev->fo_slabs + (size_t)ev->fo_prev * 11 * N;   /* unchanged: the shift is idempotent */
+        vh::FoArgs a;
+        fo_args(ev, a);
+        vh::launch_freezeout(a, ev->stream);
+        CUDA_TRY(cudaGetLastError());
+        CUDA_TRY(cudaMemcpyAsync(ev->fo_hdr, ev->fo_scratch + ev->fo_scratch_ints - 2, 2 * sizeof(int),
+                                 cudaMemcpyDeviceToHost, ev->stream));
+        CUDA_TRY(cudaStreamSynchronize(ev->stream));
+        above = ev->fo_hdr[0];
+        total = ev->fo_hdr[1];
     }
     ev->fo_prev = 1 - ev->fo_prev;
     ev->fo_count = total;
     if (n_elements) *n_elements = total;
     if (n_above) *n_above = above;
     return VH_OK;
+}
+
+int vh_event_freezeout(vh_event *ev, int *n_elements, int *n_above)
+{
+    int rc = vh_event_freezeout_launch(ev);
+    if (rc != VH_OK) return rc;
+    return vh_event_freezeout_finish(ev, n_elements, n_above);
 }
 
 int vh_event_fetch_surface(vh_event *ev, double *host_out, int cap_elements, int *n_elements)

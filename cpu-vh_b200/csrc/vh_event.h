@@ -65,6 +65,9 @@ struct vh_event {
     double *fo_elems = nullptr;
     int fo_cap = 0;
     int fo_count = 0;
+    int *fo_hdr = nullptr;                /* pinned: n_above, n_total of the last block */
+    cudaEvent_t fo_done = nullptr;
+    bool fo_pending = false;              /* launched, not yet finished */
     /* per-phase timing (vh_event_phase_timing) */
     bool timing = false;
     std::vector<vh::StageMarks> marks;    /* one per stage launched since enabling */

@@ -1,0 +1,423 @@
+/*
+ * vh_server.cpp -- an event server over the C ABI (no counterpart in the
+ * reference, which evolves one event per process, HydroPlugin.cpp:226-307).
+ *
+ * Callers submit events (configuration + host initial condition) at any time;
+ * one worker thread owns the GPU and runs rounds:
+ *
+ *   admit   queued events while their estimated device footprint fits the
+ *           memory budget (a fraction of the free HBM when the server
+ *           started); each becomes a vh_event with its state on the device
+ *           until it is done;
+ *   batch   every active event advanced together by one vh_batch (rebuilt
+ *           when the active set changes; launch configuration tuned once per
+ *           kind of batch and reused);
+ *   freeze  the freezeout blocks of all events queued first, then collected,
+ *           at the reference's cadence (a block before loop index n when
+ *           n % coarseProperTimeFOFactor == 0, HydroPlugin.cpp:249-266); the
+ *           elements of each block are copied to the event's host surface as
+ *           soon as the block is done;
+ *   retire  an event whose blocks found no cell above e_F three times
+ *           (HydroPlugin.cpp:267-281), that reached the step cap, or whose
+ *           device status reports an error, frees its device memory and is
+ *           reported through vh_server_poll.
+ *
+ * Admission happens at round boundaries: a round is the steps up to the next
+ * freezeout block of the members, so every member's blocks fall on its own
+ * cadence.
+ */
+#include <cuda_runtime.h>
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "vh_b200.h"
+#include "vh_internal.h"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Job {
+    unsigned long long tag = 0;
+    vh_config cfg{};
+    std::vector<double> e, p, u, pi, Pi;
+    double t_submit = 0, t_admit = 0;
+    vh_event *ev = nullptr;
+    size_t bytes = 0;
+    int steps = 0;
+    int last_block = -1;            /* step count of the last freezeout block */
+    int zero_blocks = 0;            /* blocks with no cell above e_F (accumulator2) */
+    double t_done = 0;
+    int status = VH_OK;
+    std::vector<double> surface;    /* VH_FO_COLUMNS per element */
+};
+
+size_t estimate_bytes(const vh_config &c)
+{
+    const size_t nq = c.bulk ? 15 : 14;
+    const size_t L = (((size_t)(c.nx + 4) * (c.ny + 4) * (c.nz + 4)) + 31) / 32 * 32;
+    const size_t N = (size_t)c.nx * c.ny * c.nz;
+    size_t b = (3 * nq + 16) * L * 8;          /* state planes */
+    b += 17 * N * 8;                           /* initial-condition staging */
+    b += 22 * N * 8 + 8 * N + (1 << 20);       /* freezeout slabs, scratch */
+    b += (size_t)16 * (c.nx * c.ny + c.ny * c.nz + c.nx * c.nz + 64) * VH_FO_COLUMNS * 8;  /* surface buffer */
+    return b + (2 << 20);
+}
+
+} // namespace
+
+struct vh_server {
+    vh_server_config cfg{};
+    std::vector<double> eos_rows;
+    int device = 0;
+    Clock::time_point t0;
+    std::mutex mu;
+    std::condition_variable cv, cv_done;
+    std::deque<std::unique_ptr<Job>> queue;
+    std::vector<std::unique_ptr<Job>> active;
+    std::deque<std::unique_ptr<Job>> done;
+    std::map<unsigned long long, std::unique_ptr<Job>> fetched;   /* done, polled, surface not yet taken */
+    size_t budget = 0, used = 0;
+    bool stop = false;
+    int fatal = VH_OK;
+    std::string fatal_msg;
+    unsigned long long submitted = 0, finished = 0;
+    vh_server_stats st{};
+    std::map<int, vh_batch_tuning> tunings;    /* per batch kind */
+    std::thread worker;
+
+    double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+};
+
+namespace {
+
+int batch_kind(const std::vector<std::unique_ptr<Job>> &act)
+{
+    bool any3 = false, any2 = false;
+    for (auto &j : act) (j->cfg.nz > 1 ? any3 : any2) = true;
+    const int z = any3 && any2 ? 2 : (any3 ? 1 : 0);
+    const vh_config &c = act.front()->cfg;
+    return z + 3 * (c.bulk ? 1 : 0) + 6 * c.eos_kind + 12 * c.precision;
+}
+
+/* steps until the next freezeout block of member j (the block happens
+ * before loop index n = steps + 1 when n % fac == 0) */
+int steps_to_block(const Job &j)
+{
+    const int fac = std::max(1, j.cfg.fo_factor);
+    int k = (j.last_block == j.steps) ? 1 : 0;
+    while ((j.steps + k + 1) % fac != 0) ++k;
+    return k;
+}
+
+void finish_job(vh_server *S, std::unique_ptr<Job> &j, int status)
+{
+    j->status = status;
+    j->t_done = S->now();
+    j->surface.shrink_to_fit();
+    if (j->ev) vh_event_destroy(j->ev);
+    j->ev = nullptr;
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->used -= j->bytes;
+    S->st.done += 1;
+    S->st.active -= 1;
+    S->done.push_back(std::move(j));
+    S->finished += 1;
+    S->cv_done.notify_all();
+}
+
+void worker_main(vh_server *S)
+{
+    cudaSetDevice(S->device);
+    vh_batch *batch = nullptr;
+    bool membership_changed = false;
+    int held_rounds = 0;        /* rounds an admission waited for alignment */
+    bool waiting = false;       /* events queued after this round's admission */
+    auto set_fatal = [&](int rc, const char *where) {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->fatal = rc;
+        S->fatal_msg = std::string(where) + ": " + vh_last_error();
+        S->cv_done.notify_all();
+    };
+    while (true) {
+        /* ---- admit */
+        std::vector<std::unique_ptr<Job>> admitted;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv.wait(lk, [&] { return S->stop || !S->queue.empty() || !S->active.empty(); });
+            if (S->stop) break;
+            /* admit where every member is fo_factor - 1 steps before its next
+             * block, as a new event is: all blocks then fall in one round
+             * (after two blocked rounds admit anyway: cadences may differ) */
+            bool aligned = true;
+            for (auto &j : S->active) aligned &= steps_to_block(*j) == std::max(1, j->cfg.fo_factor) - 1;
+            const bool admit = aligned || S->queue.empty() || ++held_rounds >= 3;
+            if (admit) held_rounds = 0;
+            while (admit && !S->queue.empty()) {
+                Job &j = *S->queue.front();
+                const size_t need = estimate_bytes(j.cfg);
+                if (S->used + need > S->budget && !(S->active.empty() && admitted.empty())) break;
+                if ((int)(S->active.size() + admitted.size()) >= S->cfg.max_events) break;
+                S->used += need;
+                j.bytes = need;
+                admitted.push_back(std::move(S->queue.front()));
+                S->queue.pop_front();
+                S->st.queued -= 1;
+                S->st.active += 1;
+            }
+            S->st.bytes_in_use = S->used;
+            waiting = !S->queue.empty();
+        }
+        for (auto &j : admitted) {
+            int rc = vh_event_create(&j->cfg, S->eos_rows.empty() ? nullptr : S->eos_rows.data(),
+                                     (int)S->eos_rows.size() / 4, &j->ev);
+            if (rc == VH_OK)
+                rc = vh_event_set_initial(j->ev, j->e.data(), j->p.data(), j->u.data(),
+                                          j->pi.empty() ? nullptr : j->pi.data(), j->Pi.empty() ? nullptr : j->Pi.data());
+            j->t_admit = S->now();
+            std::vector<double>().swap(j->e);
+            std::vector<double>().swap(j->p);
+            std::vector<double>().swap(j->u);
+            std::vector<double>().swap(j->pi);
+            std::vector<double>().swap(j->Pi);
+            if (rc != VH_OK) { finish_job(S, j, rc); continue; }
+            S->active.push_back(std::move(j));
+            membership_changed = true;
+        }
+        if (S->active.empty()) continue;
+
+        /* ---- batch (rebuilt when members changed) */
+        if (membership_changed || !batch) {
+            if (batch) vh_batch_destroy(batch);
+            batch = nullptr;
+            std::vector<vh_event *> evs;
+            for (auto &j : S->active) evs.push_back(j->ev);
+            int rc = vh_batch_create(evs.data(), (int)evs.size(), &batch);
+            if (rc != VH_OK) { set_fatal(rc, "vh_batch_create"); break; }
+            const int kind = batch_kind(S->active);
+            auto it = S->tunings.find(kind);
+            if (it != S->tunings.end()) rc = vh_batch_set_tuning(batch, &it->second);
+            else {
+                vh_batch_tuning t;
+                rc = vh_batch_autotune(batch, &t);
+                if (rc == VH_OK) S->tunings[kind] = t;
+            }
+            if (rc != VH_OK) { set_fatal(rc, "batch tuning"); break; }
+            {
+                std::lock_guard<std::mutex> lk(S->mu);
+                S->st.batch_builds += 1;
+            }
+            membership_changed = false;
+        }
+
+        /* ---- steps up to the earliest freezeout block (0: a block is due now) */
+        int k = 1 << 30;
+        for (auto &j : S->active) k = std::min(k, steps_to_block(*j));
+        /* events are waiting: stop one step after a block, where they can join */
+        if (waiting)
+            for (auto &j : S->active)
+                if (j->last_block == j->steps) k = std::min(k, 1);
+        if (S->cfg.max_steps > 0)
+            for (auto &j : S->active) k = std::min(k, std::max(0, S->cfg.max_steps - j->steps));
+        if (k > 0) {
+            int rc = vh_batch_step(batch, k);
+            if (rc != VH_OK) { set_fatal(rc, "vh_batch_step"); break; }
+            for (auto &j : S->active) j->steps += k;
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->st.steps += k;
+        }
+
+        /* ---- freezeout blocks that are due: queue all, then collect */
+        std::vector<Job *> due;
+        for (auto &j : S->active)
+            if (steps_to_block(*j) == 0) due.push_back(j.get());
+        for (Job *j : due) {
+            int rc = vh_event_freezeout_launch(j->ev);
+            if (rc != VH_OK) j->status = rc;
+        }
+        for (Job *j : due) {
+            if (j->status != VH_OK) continue;
+            j->last_block = j->steps;
+            int nel = 0, nab = 0;
+            int rc = vh_event_freezeout_finish(j->ev, &nel, &nab);
+            if (rc == VH_OK && nel > 0) {
+                const size_t off = j->surface.size();
+                j->surface.resize(off + (size_t)nel * VH_FO_COLUMNS);
+                rc = vh_event_fetch_surface(j->ev, j->surface.data() + off, nel, &nel);
+            }
+            if (rc == VH_OK) rc = vh_event_status(j->ev, nullptr, nullptr);
+            if (rc != VH_OK) { j->status = rc; continue; }
+            if (nab == 0) j->zero_blocks += 1;
+        }
+        if (!due.empty()) {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->st.fo_blocks += (long long)due.size();
+        }
+
+        /* ---- retire */
+        std::vector<std::unique_ptr<Job>> keep;
+        for (auto &j : S->active) {
+            const bool capped = S->cfg.max_steps > 0 && j->steps >= S->cfg.max_steps;
+            if (j->status != VH_OK || j->zero_blocks >= 3 || capped) {
+                finish_job(S, j, j->status);
+                membership_changed = true;
+            } else {
+                keep.push_back(std::move(j));
+            }
+        }
+        S->active.swap(keep);
+        if (membership_changed && batch) {
+            vh_batch_destroy(batch);
+            batch = nullptr;
+        }
+    }
+    if (batch) vh_batch_destroy(batch);
+    for (auto &j : S->active)
+        if (j->ev) vh_event_destroy(j->ev);
+}
+
+} // namespace
+
+extern "C" {
+
+void vh_server_config_default(vh_server_config *c)
+{
+    if (!c) return;
+    std::memset(c, 0, sizeof *c);
+    c->hbm_fraction = 0.8;
+    c->max_events = 4096;
+    c->max_steps = 0;
+}
+
+int vh_server_create(const vh_server_config *cfg, const double *eos_rows, int eos_nrows, vh_server **out)
+{
+    if (!out) return vh::set_error(VH_ERR_ARG, "null argument");
+    *out = nullptr;
+    if (!vh_device_available()) return vh::set_error(VH_ERR_NODEVICE, "no CUDA device");
+    vh_server_config c;
+    vh_server_config_default(&c);
+    if (cfg) c = *cfg;
+    if (!(c.hbm_fraction > 0 && c.hbm_fraction <= 1) || c.max_events < 1 || c.max_steps < 0)
+        return vh::set_error(VH_ERR_ARG, "bad server configuration");
+    auto *S = new vh_server;
+    S->cfg = c;
+    if (eos_rows && eos_nrows > 0) S->eos_rows.assign(eos_rows, eos_rows + 4 * (size_t)eos_nrows);
+    cudaGetDevice(&S->device);
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) { delete S; return vh::set_error(VH_ERR_CUDA, "cudaMemGetInfo"); }
+    S->budget = (size_t)(c.hbm_fraction * (double)fr);
+    S->st.budget_bytes = S->budget;
+    S->t0 = Clock::now();
+    S->worker = std::thread(worker_main, S);
+    *out = S;
+    return VH_OK;
+}
+
+int vh_server_submit(vh_server *S, const vh_config *cfg, const double *e, const double *p, const double *u,
+                     const double *pi, const double *Pi, unsigned long long tag)
+{
+    if (!S || !cfg || !e || !p || !u) return vh::set_error(VH_ERR_ARG, "null argument");
+    if (cfg->eos_kind == VH_EOS_TABLE && S->eos_rows.empty())
+        return vh::set_error(VH_ERR_ARG, "tabulated-EoS event on a server created without EoS rows");
+    auto j = std::make_unique<Job>();
+    j->tag = tag;
+    j->cfg = *cfg;
+    const size_t N = (size_t)cfg->nx * cfg->ny * cfg->nz;
+    j->e.assign(e, e + N);
+    j->p.assign(p, p + N);
+    j->u.assign(u, u + 4 * N);
+    if (pi) j->pi.assign(pi, pi + 10 * N);
+    if (Pi) j->Pi.assign(Pi, Pi + N);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->fatal != VH_OK) return vh::set_error(S->fatal, S->fatal_msg);
+    j->t_submit = S->now();
+    S->queue.push_back(std::move(j));
+    S->submitted += 1;
+    S->st.submitted += 1;
+    S->st.queued += 1;
+    S->cv.notify_all();
+    return VH_OK;
+}
+
+int vh_server_poll(vh_server *S, vh_server_done *out, int max, int *n)
+{
+    if (!S || !n || (max > 0 && !out)) return vh::set_error(VH_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    int k = 0;
+    while (k < max && !S->done.empty()) {
+        auto j = std::move(S->done.front());
+        S->done.pop_front();
+        vh_server_done &d = out[k++];
+        d.tag = j->tag;
+        d.status = j->status;
+        d.steps = j->steps;
+        d.n_elements = (long long)(j->surface.size() / VH_FO_COLUMNS);
+        d.t_submit = j->t_submit;
+        d.t_admit = j->t_admit;
+        d.t_done = j->t_done;
+        S->fetched[j->tag] = std::move(j);
+    }
+    *n = k;
+    if (S->fatal != VH_OK) return vh::set_error(S->fatal, S->fatal_msg);
+    return VH_OK;
+}
+
+int vh_server_take_surface(vh_server *S, unsigned long long tag, double *out, long long cap_elements, long long *n)
+{
+    if (!S || !n) return vh::set_error(VH_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->fetched.find(tag);
+    if (it == S->fetched.end()) return vh::set_error(VH_ERR_ARG, "no polled event with this tag");
+    const long long m = (long long)(it->second->surface.size() / VH_FO_COLUMNS);
+    *n = m;
+    if (m > cap_elements) return vh::set_error(VH_ERR_CAPACITY, "surface buffer too small");
+    if (m > 0) {
+        if (!out) return vh::set_error(VH_ERR_ARG, "null output");
+        std::memcpy(out, it->second->surface.data(), it->second->surface.size() * sizeof(double));
+    }
+    S->fetched.erase(it);
+    return VH_OK;
+}
+
+int vh_server_wait(vh_server *S, double timeout_s)
+{
+    if (!S) return vh::set_error(VH_ERR_ARG, "null server");
+    std::unique_lock<std::mutex> lk(S->mu);
+    bool ok = S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
+                                  [&] { return S->finished == S->submitted || S->fatal != VH_OK; });
+    if (S->fatal != VH_OK) return vh::set_error(S->fatal, S->fatal_msg);
+    return ok ? VH_OK : vh::set_error(VH_ERR_STATE, "timed out waiting for submitted events");
+}
+
+int vh_server_stats_get(vh_server *S, vh_server_stats *out)
+{
+    if (!S || !out) return vh::set_error(VH_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    *out = S->st;
+    out->bytes_in_use = S->used;
+    return VH_OK;
+}
+
+int vh_server_destroy(vh_server *S)
+{
+    if (!S) return VH_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        S->cv.notify_all();
+    }
+    if (S->worker.joinable()) S->worker.join();
+    delete S;
+    return VH_OK;
+}
+
+} /* extern "C" */

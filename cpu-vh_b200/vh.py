@@ -405,6 +405,122 @@ class Batch:
         return s.value or 0
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_fraction", C.c_double), ("max_events", C.c_int), ("max_steps", C.c_int)]
+
+
+class ServerDone(C.Structure):
+    _fields_ = [("tag", C.c_ulonglong), ("status", C.c_int), ("steps", C.c_int), ("n_elements", C.c_longlong),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("queued", C.c_longlong), ("active", C.c_longlong),
+                ("done", C.c_longlong), ("steps", C.c_longlong), ("fo_blocks", C.c_longlong),
+                ("batch_builds", C.c_longlong), ("bytes_in_use", C.c_ulonglong), ("budget_bytes", C.c_ulonglong)]
+
+
+_sig("vh_server_config_default", None, [C.POINTER(ServerConfig)])
+_sig("vh_server_create", C.c_int, [C.POINTER(ServerConfig), C.c_void_p, C.c_int, C.POINTER(C.c_void_p)])
+_sig("vh_server_submit", C.c_int, [C.c_void_p, _cfgp, _dp, _dp, _dp, C.c_void_p, C.c_void_p, C.c_ulonglong])
+_sig("vh_server_poll", C.c_int, [C.c_void_p, C.POINTER(ServerDone), C.c_int, C.POINTER(C.c_int)])
+_sig("vh_server_take_surface", C.c_int, [C.c_void_p, C.c_ulonglong, C.c_void_p, C.c_longlong,
+                                         C.POINTER(C.c_longlong)])
+_sig("vh_server_wait", C.c_int, [C.c_void_p, C.c_double])
+_sig("vh_server_stats_get", C.c_int, [C.c_void_p, C.POINTER(ServerStats)])
+_sig("vh_server_destroy", C.c_int, [C.c_void_p])
+
+
+class Server:
+    """vh_server_*: submit events at any time; a worker thread admits them by
+    free device memory, advances them as one batch, streams their freezeout
+    surfaces to host memory and retires them."""
+
+    def __init__(self, eos_rows=None, hbm_fraction=0.8, max_events=4096, max_steps=0):
+        c = ServerConfig()
+        lib.vh_server_config_default(C.byref(c))
+        c.hbm_fraction, c.max_events, c.max_steps = hbm_fraction, max_events, max_steps
+        self._rows = None if eos_rows is None else np.ascontiguousarray(eos_rows, dtype=np.float64)
+        h = C.c_void_p()
+        check(lib.vh_server_create(C.byref(c), _ptr(self._rows), 0 if self._rows is None else len(self._rows),
+                                   C.byref(h)), "vh_server_create")
+        self.h = h
+
+    def submit(self, cfg: VhConfig, st: InitialState, tag: int):
+        pi = None if st.pi is None else np.ascontiguousarray(st.pi, dtype=np.float64)
+        Pi = None if st.Pi is None else np.ascontiguousarray(st.Pi, dtype=np.float64)
+        check(lib.vh_server_submit(self.h, C.byref(cfg), np.ascontiguousarray(st.e), np.ascontiguousarray(st.p),
+                                   np.ascontiguousarray(st.u).reshape(-1), _ptr(pi), _ptr(Pi), tag),
+              "vh_server_submit")
+
+    def poll(self, max_n: int = 1024) -> list:
+        out = (ServerDone * max_n)()
+        n = C.c_int()
+        check(lib.vh_server_poll(self.h, out, max_n, C.byref(n)), "vh_server_poll")
+        return [out[i] for i in range(n.value)]
+
+    def take_surface(self, tag: int) -> np.ndarray:
+        n = C.c_longlong()
+        lib.vh_server_take_surface(self.h, tag, None, 0, C.byref(n))
+        out = np.zeros((n.value, VH_FO_COLUMNS))
+        check(lib.vh_server_take_surface(self.h, tag, _ptr(out), n.value, C.byref(n)), "vh_server_take_surface")
+        return out
+
+    def wait(self, timeout_s: float = 600.0):
+        check(lib.vh_server_wait(self.h, timeout_s), "vh_server_wait")
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(lib.vh_server_stats_get(self.h, C.byref(st)), "vh_server_stats_get")
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "h", None) and lib is not None:
+            lib.vh_server_destroy(self.h)
+        self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+def run_like_server(cfg: VhConfig, rows, st: InitialState, max_steps: int = 0):
+    """One event alone with the server's cadence: freezeout blocks before loop
+    index n when n % fo_factor == 0, retired after three blocks with no cell
+    above e_F, at max_steps, or when the device reports an error.
+    Returns (steps, surface, status)."""
+    ev = Event(cfg, rows)
+    ev.set_initial(st)
+    fac = max(1, cfg.fo_factor)
+    steps, last, zero, parts, status = 0, -1, 0, [], VH_OK
+
+    def to_block():
+        k = 1 if last == steps else 0
+        while (steps + k + 1) % fac:
+            k += 1
+        return k
+
+    while True:
+        k = to_block()
+        if max_steps:
+            k = min(k, max(0, max_steps - steps))
+        if k:
+            ev.step(k)
+            steps += k
+        if to_block() == 0:
+            last = steps
+            n, na = ev.freezeout()
+            if n:
+                parts.append(ev.surface())
+            status = ev.status()[0]
+            if status != VH_OK:
+                break
+            zero += na == 0
+        if zero >= 3 or (max_steps and steps >= max_steps):
+            break
+    ev.close()
+    return steps, (np.concatenate(parts) if parts else np.zeros((0, VH_FO_COLUMNS))), status
+
+
 def make_tuning(fused: bool, tx: int, persistent: bool) -> BatchTuning:
     t = BatchTuning()
     t.fused = 1 if fused else 0

@@ -147,6 +147,13 @@ int vh_event_get_field(vh_event *ev, int field, double *host_out);
  * the order in which the reference writes them. */
 int vh_event_freezeout(vh_event *ev, int *n_elements, int *n_above);
 
+/* The same block in two halves, so that the host can queue the freezeout of
+ * many events before waiting for any: _launch queues the block on the
+ * event's stream and returns; _finish waits for it and returns what
+ * vh_event_freezeout returns.  The event must not be stepped in between. */
+int vh_event_freezeout_launch(vh_event *ev);
+int vh_event_freezeout_finish(vh_event *ev, int *n_elements, int *n_above);
+
 /* Copy the elements of the last freezeout block to host memory, VH_FO_COLUMNS
  * doubles per element.  Returns VH_ERR_CAPACITY if cap_elements is too small. */
 int vh_event_fetch_surface(vh_event *ev, double *host_out, int cap_elements, int *n_elements);
@@ -218,6 +225,58 @@ int vh_batch_kernel_launches(vh_batch *b, int *per_step);
 int vh_batch_phase_timing(vh_batch *b, int enable);
 int vh_batch_phase_times(vh_batch *b, double ms[VH_NPHASES], long long launches[VH_NPHASES]);
 int vh_batch_stream(vh_batch *b, void **stream);
+
+/* ------------------------------------------------------------------- server
+ * An event server (no counterpart in the reference, which evolves one event
+ * per process): events are submitted with their host initial condition at
+ * any time; a worker thread admits them while their estimated device
+ * footprint fits hbm_fraction of the free device memory, keeps their state on
+ * the device, advances all admitted events as one batch, runs each event's
+ * freezeout blocks at its fo_factor cadence (HydroPlugin.cpp:249-266) and
+ * streams the elements to host memory, and retires an event after three
+ * blocks with no cell above e_F (HydroPlugin.cpp:267-281), at max_steps, or on
+ * a device error.  Events of one server share its EoS rows; precision, bulk
+ * and the EoS kind must agree among the events submitted.
+ */
+typedef struct vh_server vh_server;
+
+typedef struct vh_server_config {
+    double hbm_fraction;     /* share of the free device memory at creation the events may use */
+    int max_events;          /* most events resident at once                                     */
+    int max_steps;           /* RK2 steps after which an event is retired (0: no cap)            */
+} vh_server_config;
+
+typedef struct vh_server_done {
+    unsigned long long tag;  /* the caller's tag from vh_server_submit */
+    int status;              /* VH_OK or the event's error             */
+    int steps;               /* RK2 steps the event took               */
+    long long n_elements;    /* freezeout elements collected           */
+    double t_submit, t_admit, t_done;   /* seconds since vh_server_create */
+} vh_server_done;
+
+typedef struct vh_server_stats {
+    long long submitted, queued, active, done;
+    long long steps;         /* batch steps run          */
+    long long fo_blocks;     /* freezeout blocks run     */
+    long long batch_builds;  /* batches (re)built        */
+    unsigned long long bytes_in_use, budget_bytes;
+} vh_server_stats;
+
+void vh_server_config_default(vh_server_config *c);
+int vh_server_create(const vh_server_config *cfg, const double *eos_rows, int eos_nrows, vh_server **out);
+/* Copies the initial condition (interior arrays as vh_event_set_initial) and
+ * returns at once. */
+int vh_server_submit(vh_server *s, const vh_config *cfg, const double *e, const double *p, const double *u,
+                     const double *pi, const double *Pi, unsigned long long tag);
+/* Up to max finished events, oldest first. */
+int vh_server_poll(vh_server *s, vh_server_done *out, int max, int *n);
+/* The surface of a polled event (VH_FO_COLUMNS doubles per element); the
+ * server drops it once taken. */
+int vh_server_take_surface(vh_server *s, unsigned long long tag, double *out, long long cap_elements, long long *n);
+/* Wait until every submitted event is finished (VH_ERR_STATE on timeout). */
+int vh_server_wait(vh_server *s, double timeout_s);
+int vh_server_stats_get(vh_server *s, vh_server_stats *out);
+int vh_server_destroy(vh_server *s);
 
 /* Device pointer of a padded field (for zero-copy inspection / timing). */
 int vh_event_device_field(vh_event *ev, int field, double **d_ptr);

@@ -1,0 +1,63 @@
+"""The event server (vh_server_*): events submitted together, admitted by
+memory, advanced as one batch and frozen out at their own cadence must give
+exactly the surfaces and step counts of each event run alone with the same
+cadence (FP64 is bit-exact through batching)."""
+import numpy as np
+import pytest
+
+import vh
+
+pytestmark = pytest.mark.gpu
+
+
+def _events(rows):
+    out = []
+    for i, n in enumerate((21, 33, 41, 27)):
+        c = vh.hotspot_config(n)
+        c.fo_factor = 5
+        out.append((c, vh.hotspot_ic(c, rows, seed=100 + i)))
+    g = vh.glauber_config(15, 13, 5)
+    g.dx = g.dy = 0.5
+    g.dz = 0.4
+    g.dt = 0.05
+    g.fo_factor = 4
+    out.append((g, vh.glauber_ic(g, rows, b=3.0)))
+    return out
+
+
+@pytest.mark.parametrize("hbm_fraction", [0.5, 1e-9])
+def test_server_matches_single_event_runs(hbm_fraction):
+    rows = vh.synthetic_eos_table()
+    evs = _events(rows)
+    srv = vh.Server(rows, hbm_fraction=hbm_fraction, max_steps=60)
+    for tag, (c, st) in enumerate(evs):
+        srv.submit(c, st, tag)
+    srv.wait(300)
+    done = {d.tag: d for d in srv.poll()}
+    assert sorted(done) == list(range(len(evs)))
+    stats = srv.stats()
+    assert stats["done"] == len(evs) and stats["queued"] == 0 and stats["active"] == 0
+    if hbm_fraction < 1e-6:
+        assert stats["batch_builds"] >= len(evs)      # admitted one at a time
+    for tag, (c, st) in enumerate(evs):
+        d = done[tag]
+        assert d.t_submit <= d.t_admit <= d.t_done
+        surf = srv.take_surface(tag)
+        steps, ref, status = vh.run_like_server(c, rows, st, max_steps=60)
+        assert d.status == status == 0
+        assert d.steps == steps
+        assert surf.shape == ref.shape and d.n_elements == len(ref)
+        assert np.array_equal(surf.view(np.uint64), ref.view(np.uint64))
+    srv.close()
+
+
+def test_server_reports_incompatible_events():
+    rows = vh.synthetic_eos_table()
+    srv = vh.Server(rows, max_steps=20)
+    a = vh.hotspot_config(17)
+    b = vh.hotspot_config(19).copy(precision=vh.VH_PREC_MIXED)
+    srv.submit(a, vh.hotspot_ic(a, rows, seed=1), 1)
+    srv.submit(b, vh.hotspot_ic(b, rows, seed=2), 2)
+    with pytest.raises(vh.VhError):
+        srv.wait(120)
+    srv.close()
