@@ -508,6 +508,90 @@ __device__ __forceinline__ void stage_body_m(const StageArgs &A, int i, int j, i
     put_with_ghosts<NQ>(A, i, j, k, s, acc, P);
 }
 
+/* ---------------------------------------------------------------------
+ * Face-once flux (mixed precision).  The reference evaluates every face twice
+ * -- once for each adjacent cell, each time with that cell's e as the root
+ * solve's starting point (SemiDiscreteKurganovTadmorScheme.cpp:14-62 called
+ * from both neighbours) -- which bit parity requires.  The mixed path
+ * evaluates each face once, starting the root solve from the e of the cell on
+ * the face's upper side, and hands the face flux to both cells through shared
+ * memory: half the root solves and extrapolations, and the flux leaving one
+ * cell is exactly the flux entering its neighbour.  Where the two cells lie
+ * on different sides of the root solve's e <= 0.1 branch (the dilute edge)
+ * the lower cell evaluates its forward face itself, as the reference does.
+ *
+ * A block of TX x TY threads covers a tile of faces: along x the faces
+ * i0 - 1/2 .. i0 + TX - 3/2 of TY rows and the cells i0 .. i0 + TX - 2; along
+ * y (eta) the block's second index runs along y (eta) and the last row of
+ * threads only computes faces.
+ * --------------------------------------------------------------------- */
+template <int NQ, int EOS>
+__device__ __forceinline__ void face_H_m(const StageArgs &A, long long b, long long st, int dir, double ePrev,
+                                         double *__restrict__ H, bool &bad)
+{
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) H[n] = 0.0;
+    face_flux_m<NQ, EOS>(A, b, st, dir, false, ePrev, H, bad);
+}
+
+/* one tile of the face-once flux along DIR; (i0, j0, k0) interior coordinates
+ * of the block's first face-owning cell; sm holds NQ * TX * TY doubles */
+template <int NQ, int EOS, int DIR, int TX, int TY>
+__device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int j0, int k0, double *__restrict__ sm)
+{
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
+    const int i = i0 + tx + 2;
+    const int j = (DIR == 3) ? j0 + 2 : j0 + ty + 2;
+    const int k = (DIR == 3) ? k0 + ty + 2 : k0 + 2;
+    const long long sxy = (long long)A.ncx * A.ncy;
+    const long long st = (DIR == 1) ? 1 : (DIR == 2) ? (long long)A.ncx : sxy;
+    const int along = (DIR == 1) ? i : (DIR == 2) ? j : k;             /* padded index along DIR */
+    const int n_along = (DIR == 1) ? A.nx : (DIR == 2) ? A.ny : A.nz;
+    const bool across_ok = (DIR == 1) ? (j < A.ny + 2 && k < A.nz + 2)
+                         : (DIR == 2) ? (i < A.nx + 2 && k < A.nz + 2)
+                                      : (i < A.nx + 2 && j < A.ny + 2);
+    /* this thread's face lies between cells along - 1 and along; the faces up
+     * to the one after the last interior cell are needed (its stencil reaches
+     * the second ghost layer, index n_along + 3) */
+    const bool face_ok = across_ok && along <= n_along + 2;
+    const long long s = i + (long long)A.ncx * j + sxy * k;
+    bool bad = false;
+    double H[NQ];
+    if (face_ok) {
+        face_H_m<NQ, EOS>(A, s - st, st, DIR, __ldg(A.ein + s), H, bad);
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) sm[n * (TX * TY) + tid] = H[n];
+    }
+    __syncthreads();
+    const bool last = (DIR == 1) ? (tx == TX - 1) : (ty == TY - 1);
+    if (face_ok && !last && along <= n_along + 1) {
+        const int nxt = (DIR == 1) ? tid + 1 : tid + TX;
+        const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
+        const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
+        double r[NQ];
+        const double e_self = __ldg(A.ein + s), e_next = __ldg(A.ein + s + st);
+        if ((e_self <= 0.1) != (e_next <= 0.1)) {
+            double F[NQ];
+            face_H_m<NQ, EOS>(A, s, st, DIR, e_self, F, bad);
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) r[n] = H[n] - F[n];
+        } else {
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) r[n] = H[n] - sm[n * (TX * TY) + nxt];
+        }
+        double S[4];
+        dir_sources<NQ>(A, s, st, d, DIR, S);
+#pragma unroll
+        for (int n = 0; n < 4; ++n) r[n] = (r[n] * yd + S[n]) * A.dt;
+#pragma unroll
+        for (int n = 4; n < NQ; ++n) r[n] *= yd * A.dt;
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] += r[n];
+    }
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+    __syncthreads();
+}
+
 /* launch-form independent selection of the per-cell bodies: MIXED picks the
  * mixed-precision source, flux and fused bodies; finalize is FP64 in both */
 template <int NQ, int EOS, bool MIXED>

@@ -58,6 +58,29 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_kernel(const
     flux_phase<NQ, EOS, DIR, MIXED>(A, s);
 }
 
+/* face-once flux (mixed precision): 32 x 8 threads, each face computed once
+ * and shared with both adjacent cells through shared memory */
+constexpr int kFaceTX = 32, kFaceTY = 8;
+
+template <int NQ, int EOS, int DIR>
+__global__ void __launch_bounds__(kFaceTX * kFaceTY, 2) kt_flux_face_kernel(const __grid_constant__ StageArgs A)
+{
+    __shared__ double sm[NQ * kFaceTX * kFaceTY];
+    int i0, j0, k0;
+    if (DIR == 1) { i0 = blockIdx.x * (kFaceTX - 1); j0 = blockIdx.y * kFaceTY; k0 = blockIdx.z; }
+    else if (DIR == 2) { i0 = blockIdx.x * kFaceTX; j0 = blockIdx.y * (kFaceTY - 1); k0 = blockIdx.z; }
+    else { i0 = blockIdx.x * kFaceTX; j0 = blockIdx.y; k0 = blockIdx.z * (kFaceTY - 1); }
+    flux_faces_tile<NQ, EOS, DIR, kFaceTX, kFaceTY>(A, i0, j0, k0, sm);
+}
+
+template <int DIR>
+static inline dim3 face_grid(const StageArgs &a)
+{
+    if (DIR == 1) return dim3((a.nx + kFaceTX - 2) / (kFaceTX - 1), (a.ny + kFaceTY - 1) / kFaceTY, a.nz);
+    if (DIR == 2) return dim3((a.nx + kFaceTX - 1) / kFaceTX, (a.ny + kFaceTY - 2) / (kFaceTY - 1), a.nz);
+    return dim3((a.nx + kFaceTX - 1) / kFaceTX, a.ny, (a.nz + kFaceTY - 2) / (kFaceTY - 1));
+}
+
 template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
 __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_final_kernel(const __grid_constant__ StageArgs A)
 {
@@ -103,11 +126,20 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
     }
     kt_source_kernel<NQ, EOS, MIXED><<<grid, block, 0, s>>>(a);
     mark(0);
-    kt_flux_kernel<NQ, EOS, 1, MIXED><<<grid, block, 0, s>>>(a);
-    mark(1);
-    kt_flux_kernel<NQ, EOS, 2, MIXED><<<grid, block, 0, s>>>(a);
-    mark(2);
-    if (z) { kt_flux_kernel<NQ, EOS, 3, MIXED><<<grid, block, 0, s>>>(a); mark(3); }
+    if constexpr (MIXED) {
+        const dim3 fb(kFaceTX, kFaceTY, 1);
+        kt_flux_face_kernel<NQ, EOS, 1><<<face_grid<1>(a), fb, 0, s>>>(a);
+        mark(1);
+        kt_flux_face_kernel<NQ, EOS, 2><<<face_grid<2>(a), fb, 0, s>>>(a);
+        mark(2);
+        if (z) { kt_flux_face_kernel<NQ, EOS, 3><<<face_grid<3>(a), fb, 0, s>>>(a); mark(3); }
+    } else {
+        kt_flux_kernel<NQ, EOS, 1, MIXED><<<grid, block, 0, s>>>(a);
+        mark(1);
+        kt_flux_kernel<NQ, EOS, 2, MIXED><<<grid, block, 0, s>>>(a);
+        mark(2);
+        if (z) { kt_flux_kernel<NQ, EOS, 3, MIXED><<<grid, block, 0, s>>>(a); mark(3); }
+    }
     if (z && st2) kt_final_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
     else if (z) kt_final_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
     else if (st2) kt_final_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);

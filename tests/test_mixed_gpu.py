@@ -137,3 +137,19 @@ def test_batched_mixed_matches_single_mixed():
         x = vh.Event(vh.hotspot_config(15), rows)
         x.set_initial(vh.hotspot_ic(x.cfg, rows, seed=1))
         vh.Batch([evs[0], x])
+
+
+def test_mixed_split_face_once_vs_fp64():
+    """a lattice above the fused/split threshold (2^18 cells): the mixed split
+    stage evaluates each face once; after 20 steps its error against the FP64
+    path must stay within 1e-4 relative L-infinity in e (the velocity, whose
+    largest deviations sit in the dilute edge, within 1e-2)"""
+    cfg = vh.glauber_config(81, 81, 41)
+    rows = vh.synthetic_eos_table()
+    st = vh.glauber_ic(cfg, rows)
+    mixed = _run(cfg, rows, st, 20, True)
+    ref = _run(cfg, rows, st, 20, False)
+    assert mixed.launches_per_step() == 10          # the phase-split form ran
+    err = _errors(cfg, mixed, ref)
+    assert err["e"] <= 1e-4, err
+    assert max(err[k] for k in ("ut", "ux", "uy")) <= 1e-2, err
