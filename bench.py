@@ -61,7 +61,8 @@ def phase_words(nq):
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
 # ncu capture kept in profiles/kt_stage_kernels_glauber_131x131x61.md
-NCU_TRAFFIC = {("glauber_3p1d", "flux"): 387.02e6, ("glauber_3p1d", "source"): 336.17e6}
+NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 387.02e6, ("glauber_3p1d", "fp64", "source"): 336.17e6,
+               ("glauber_3p1d", "mixed", "flux"): 387.33e6, ("glauber_3p1d", "mixed", "source"): 322.01e6}
 
 
 KERNEL_NAMES = {"source": "kt_source_kernel", "flux": "kt_flux_kernel (x, y, eta)",
@@ -633,7 +634,7 @@ def main():
     peak, peak_kind = measured_peaks()
     alg_bytes = phase_words(ev.nq)[dom] * 8 * N
     achieved = alg_bytes / launch_s / 1e9
-    traffic = NCU_TRAFFIC.get((args.workload, dom))
+    traffic = NCU_TRAFFIC.get((args.workload, args.precision, dom))
 
     e2e = None
     if not args.no_e2e:
@@ -683,11 +684,12 @@ def main():
                            "l2": l2_note},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic,
-                             "kernel": KERNEL_NAMES[dom], "launches": dom_n,
+                             "kernel": ("kt_flux_face_kernel (x, y, eta)" if mixed and dom == "flux" and
+                                        ev.launches_per_step() > 2 else KERNEL_NAMES[dom]), "launches": dom_n,
                              "launch_us": launch_s * 1e6, "algorithmic_bytes": alg_bytes,
                              "share": dom_ms / sum(t for t, _ in kern.values()),
-                             "note": f"peak: {peak_kind} HBM copy bandwidth; the strict-parity FP64 "
-                                     "step is bound by FP64 issue latency, not HBM"},
+                             "note": f"peak: {peak_kind} HBM copy bandwidth; the step is bound by "
+                                     "FP64/FP32 issue latency (memory and barrier stalls), not HBM"},
                 "phases_ms_per_step": {k: t / args.steps for k, (t, _) in phases.items()},
                 "clocks": clk, "gpu_launches": ev.launches_per_step() * args.steps}
         if prec:
