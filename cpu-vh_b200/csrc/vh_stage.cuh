@@ -98,6 +98,155 @@ __device__ __forceinline__ void dir_sources(const StageArgs &A, long long s, lon
 #undef DER
 }
 
+/* ---------------------------------------------------------------------
+ * The flux phase reading q from a tile staged in shared memory: the same
+ * arithmetic as face_flux / dir_sources, with every read of the conserved
+ * variables going to the tile (index = position in the tile, stride along
+ * the axis = the tile's stride), so the results are bit-identical.
+ * --------------------------------------------------------------------- */
+struct QTile {
+    const double *__restrict__ q;
+    int P;                   /* doubles per component plane of the tile */
+    __device__ __forceinline__ double operator()(int n, int i) const { return q[n * P + i]; }
+};
+
+__device__ __forceinline__ void extrapolate_t(const QTile &qt, int n, int b, int st, double th, double &qR, double &qL)
+{
+    double A = qt(n, b - st), B = qt(n, b), C = qt(n, b + st), D = qt(n, b + 2 * st);
+    qR = C - approx_deriv(th, B, C, D) / 2;
+    qL = B + approx_deriv(th, A, B, C) / 2;
+}
+
+template <int NQ, int EOS>
+__device__ __forceinline__ void face_flux_t(const StageArgs &A, const QTile &qt, int b, int st, int dir, bool fwd,
+                                            double ePrev, double *__restrict__ r, bool &bad)
+{
+    const double th = A.theta;
+    double qRs[8], qLs[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) extrapolate_t(qt, c, b, st, th, qRs[c], qLs[c]);
+    double PiR = 0, PiL = 0;
+    if (NQ == 15) extrapolate_t(qt, 14, b, st, th, PiR, PiL);
+    Prim R = infer<EOS, true>(A.eos, A.t, qRs[0] - qRs[4], qRs[1] - qRs[5], qRs[2] - qRs[6], qRs[3] - qRs[7], PiR, ePrev, bad);
+    Prim Lf = infer<EOS, true>(A.eos, A.t, qLs[0] - qLs[4], qLs[1] - qLs[5], qLs[2] - qLs[6], qLs[3] - qLs[7], PiL, ePrev, bad);
+    const double vR = (dir == 1) ? R.ux : (dir == 2) ? R.uy : R.un;
+    const double vL = (dir == 1) ? Lf.ux : (dir == 2) ? Lf.uy : Lf.un;
+    const double rhoLeft = fabs(vL / Lf.ut);
+    const double rhoRight = fabs(vR / R.ut);
+    const double a = fmax(rhoLeft, rhoRight);
+    const double yR = 1.0 / R.ut, yL = 1.0 / Lf.ut;
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) {
+        double qR, qL;
+        if (n < 8) { qR = qRs[n]; qL = qLs[n]; }
+        else if (n == 14) { qR = PiR; qL = PiL; }
+        else extrapolate_t(qt, n, b, st, th, qR, qL);
+        double FqR = div_rcp(vR * qR, R.ut, yR);
+        double FqL = div_rcp(vL * qL, Lf.ut, yL);
+        double res = FqR + FqL - a * (qR - qL);
+        res /= 2;
+        r[n] = fwd ? -res : r[n] + res;
+    }
+}
+
+/* dir_sources with q from the tile at ts +- tst and u at the padded cell s */
+template <int NQ>
+__device__ __forceinline__ void dir_sources_t(const StageArgs &A, const QTile &qt, int ts, int tst, long long s,
+                                              double d, int dir, double *S)
+{
+    const long long L = A.L;
+    const double fac = 1 / d / 2;
+    const double ut = __ldg(A.uin + s);
+    const double v = __ldg(A.uin + dir * L + s);
+    const double vv = v / ut;
+#define DER(n) ((qt(n, ts + tst) - qt(n, ts - tst)) * fac)
+    const double dpitt = DER(4), dpitx = DER(5), dpity = DER(6), dpitn = DER(7);
+    if (dir == 1) {
+        double dpixx = DER(8), dpixy = DER(9), dpixn = DER(10);
+        if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpitx - vv * dPi; S[1] = dpitx * vv - dpixx - dPi; }
+        else { S[0] = dpitt * vv - dpitx; S[1] = dpitx * vv - dpixx; }
+        S[2] = dpity * vv - dpixy;
+        S[3] = dpitn * vv - dpixn;
+    } else if (dir == 2) {
+        double dpixy = DER(9), dpiyy = DER(11), dpiyn = DER(12);
+        if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpity - vv * dPi; S[2] = dpity * vv - dpiyy - dPi; }
+        else { S[0] = dpitt * vv - dpity; S[2] = dpity * vv - dpiyy; }
+        S[1] = dpitx * vv - dpixy;
+        S[3] = dpitn * vv - dpiyn;
+    } else {
+        double dpixn = DER(10), dpiyn = DER(12), dpinn = DER(13);
+        if (NQ == 15) { double dPi = DER(14); S[0] = dpitt * vv - dpitn - vv * dPi; S[3] = dpitn * vv - dpinn - dPi / A.t2pow; }
+        else { S[0] = dpitt * vv - dpitn; S[3] = dpitn * vv - dpinn; }
+        S[1] = dpitx * vv - dpixn;
+        S[2] = dpity * vv - dpiyn;
+    }
+#undef DER
+}
+
+/* copy 8 bytes global -> shared without staging through registers */
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem)
+{
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+/* One block of the staged flux along DIR: TX x TY cells (x by y for DIR 1
+ * and 2, x by eta for DIR 3, at the block's fixed third coordinate) and the
+ * 2-cell halo along DIR, all NQ components, copied asynchronously into sm
+ * (NQ * (TX + 4 [DIR 1]) * (TY + 4 [DIR 2, 3]) doubles), then the flux of
+ * every interior cell of the tile as flux_body computes it. */
+template <int NQ, int EOS, int DIR, int TX, int TY>
+__device__ __forceinline__ void flux_staged_tile(const StageArgs &A, int i0, int j0, int k0, double *__restrict__ sm)
+{
+    constexpr int BX = TX + (DIR == 1 ? 4 : 0), BY = TY + (DIR == 1 ? 0 : 4), P = BX * BY;
+    const int tid = threadIdx.x + TX * threadIdx.y;
+    const long long sxy = (long long)A.ncx * A.ncy;
+    /* padded coordinates of the tile's first box element; the box's second
+     * axis is y (DIR 1, 2) or eta (DIR 3) */
+    const int bx0 = i0 + 2 - (DIR == 1 ? 2 : 0);
+    const int by0 = (DIR == 3) ? k0 : j0;            /* = first cell - 2 for DIR 2, 3 */
+    const int b2lim = (DIR == 3) ? A.nz + 4 : A.ny + 4;
+    const int by_first = (DIR == 1) ? j0 + 2 : by0;
+    for (int e = tid; e < NQ * P; e += TX * TY) {
+        const int n = e / P, rr = e - n * P, bxi = rr % BX, byi = rr / BX;
+        const int x = bx0 + bxi, yk = by_first + byi;
+        if (x < A.ncx && yk < b2lim) {
+            const long long g = (DIR == 3) ? x + (long long)A.ncx * (j0 + 2) + sxy * yk
+                                           : x + (long long)A.ncx * yk + sxy * (k0 + 2);
+            cp_async8(sm + e, A.qin + n * A.L + g);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const int i = i0 + threadIdx.x + 2;
+    const int j = (DIR == 3) ? j0 + 2 : j0 + threadIdx.y + 2;
+    const int k = (DIR == 3) ? k0 + threadIdx.y + 2 : k0 + 2;
+    if (i >= A.nx + 2 || j >= A.ny + 2 || k >= A.nz + 2) return;
+    const long long s = i + (long long)A.ncx * j + sxy * k;
+    const int ts = (threadIdx.x + (DIR == 1 ? 2 : 0)) + BX * (threadIdx.y + (DIR == 1 ? 0 : 2));
+    const int tst = (DIR == 1) ? 1 : BX;
+    const QTile qt{sm, P};
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
+    const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
+    double r[NQ];
+#pragma unroll 1
+    for (int f = 0; f < 2; ++f) face_flux_t<NQ, EOS>(A, qt, f == 0 ? ts : ts - tst, tst, DIR, f == 0, ePrev, r, bad);
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) r[n] = div_rcp(r[n], d, yd);
+    double S[4];
+    dir_sources_t<NQ>(A, qt, ts, tst, s, d, DIR, S);
+#pragma unroll
+    for (int n = 0; n < 4; ++n) { r[n] += S[n]; r[n] *= A.dt; }
+#pragma unroll
+    for (int n = 4; n < NQ; ++n) r[n] *= A.dt;
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] += r[n];
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+}
+
 /* eulerStepKernelX/Y/Z (FullyDiscreteKurganovTadmorScheme.cpp:300-634), the
  * axes in the reference's order x, y, eta. */
 template <int NQ, int EOS, bool HAS_Z>

@@ -58,6 +58,30 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_kernel(const
     flux_phase<NQ, EOS, DIR, MIXED>(A, s);
 }
 
+/* FP64 flux with the stencil tile staged in shared memory (cp.async): the
+ * block's 32 x 4 cells and their 2-cell halo along DIR, all components */
+template <int NQ, int EOS, int DIR>
+__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_staged_kernel(const __grid_constant__ StageArgs A)
+{
+    constexpr int TX = 32, TY = 4;
+    __shared__ double sm[NQ * (TX + (DIR == 1 ? 4 : 0)) * (TY + (DIR == 1 ? 0 : 4))];
+    const int i0 = blockIdx.x * TX;
+    int j0, k0;
+    if (DIR == 3) { j0 = blockIdx.y; k0 = blockIdx.z * TY; } else { j0 = blockIdx.y * TY; k0 = blockIdx.z; }
+    flux_staged_tile<NQ, EOS, DIR, TX, TY>(A, i0, j0, k0, sm);
+}
+
+/* staged flux on (default) or off: VH_FLUX_STAGED=0 selects the kernel that
+ * reads the stencil straight from device memory */
+static inline bool flux_staged()
+{
+    static int on = [] {
+        const char *e = getenv("VH_FLUX_STAGED");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return on == 1;
+}
+
 /* face-once flux (mixed precision): 32 x 8 threads, each face computed once
  * and shared with both adjacent cells through shared memory */
 constexpr int kFaceTX = 32, kFaceTY = 8;
@@ -133,6 +157,13 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
         kt_flux_face_kernel<NQ, EOS, 2><<<face_grid<2>(a), fb, 0, s>>>(a);
         mark(2);
         if (z) { kt_flux_face_kernel<NQ, EOS, 3><<<face_grid<3>(a), fb, 0, s>>>(a); mark(3); }
+    } else if (flux_staged()) {
+        const dim3 g3((a.nx + 31) / 32, a.ny, (a.nz + 3) / 4);
+        kt_flux_staged_kernel<NQ, EOS, 1><<<grid, block, 0, s>>>(a);
+        mark(1);
+        kt_flux_staged_kernel<NQ, EOS, 2><<<grid, block, 0, s>>>(a);
+        mark(2);
+        if (z) { kt_flux_staged_kernel<NQ, EOS, 3><<<g3, block, 0, s>>>(a); mark(3); }
     } else {
         kt_flux_kernel<NQ, EOS, 1, MIXED><<<grid, block, 0, s>>>(a);
         mark(1);

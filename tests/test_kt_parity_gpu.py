@@ -68,3 +68,48 @@ def test_glauber_table_bulk_bitexact(dims, steps):
         gpu.sync()
         bad = _compare(cfg, gpu, orc, FIELDS_15)
         assert not bad, f"after {s} steps, bit-differing cells per field: {bad}"
+
+
+_SPLIT_CHECK = r"""
+import sys, numpy as np
+import vh
+from oracle import OracleEvent
+cfg = vh.glauber_config(65, 65, 63)
+cfg.dx = cfg.dy = 0.3
+cfg.dz = 0.25
+cfg.dt = 0.03
+rows = vh.synthetic_eos_table()
+st = vh.glauber_ic(cfg, rows)
+gpu, orc = vh.Event(cfg, rows), OracleEvent(cfg, rows)
+gpu.set_initial(st)
+orc.set_initial(st)
+fields = list(range(15)) + [100, 101, 102, 103, 200, 201]
+bad = 0
+for n in (1, 2):
+    gpu.step(n)
+    assert orc.step(n) == 0
+    gpu.sync()
+    for f in fields:
+        A, B = vh.face_cells(cfg, gpu.field(f)), vh.face_cells(cfg, orc.field(f))
+        bad += int(np.count_nonzero(A.view(np.uint64) != B.view(np.uint64)))
+print("LAUNCHES", gpu.launches_per_step(), "BAD", bad)
+"""
+
+
+@pytest.mark.parametrize("env", [{}, {"VH_FLUX_STAGED": "0"}, {"VH_STAGE_MODE": "fused"}],
+                         ids=["split-staged", "split-global", "fused"])
+def test_large_lattice_forms_bitexact(env):
+    """above 2^18 cells the stage runs phase-split, its flux reading a
+    shared-memory tile by default; every form must equal the oracle bit for
+    bit (run in a child process: the form is chosen once per process)"""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    e = dict(os.environ, **env)
+    e["PYTHONPATH"] = os.pathsep.join([os.path.join(root, "cpu-vh_b200"), os.path.join(root, "oracle"), root])
+    out = subprocess.run([sys.executable, "-c", _SPLIT_CHECK], env=e, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    line = [l for l in out.stdout.splitlines() if l.startswith("LAUNCHES")][-1].split()
+    assert int(line[1]) == (2 if env.get("VH_STAGE_MODE") == "fused" else 10)
+    assert int(line[3]) == 0, line
