@@ -110,6 +110,7 @@ int vh_event_destroy(vh_event *ev)
     cudaFree(ev->fo_scratch);
     cudaFree(ev->fo_elems);
     if (ev->fo_hdr) cudaFreeHost(ev->fo_hdr);
+    cudaFree(ev->vort);
     if (ev->fo_done) cudaEventDestroy(ev->fo_done);
     for (auto &m : ev->marks)
         for (cudaEvent_t e : m.ev) cudaEventDestroy(e);
@@ -217,6 +218,18 @@ int vh_event_set_initial_device(vh_event *ev, const double *d_e, const double *d
     return do_init(ev, d_e, d_p, d_u, d_pi, d_Pi);
 }
 
+static void launch_vort(vh_event *ev)
+{
+    vh::VortArgs a;
+    a.u = ev->u[ev->uc]; a.up = ev->u[ev->up]; a.e = ev->ep[ev->ec];
+    a.w = ev->vort; a.L = ev->L;
+    a.nx = ev->cfg.nx; a.ny = ev->cfg.ny; a.nz = ev->cfg.nz; a.ncx = ev->ncx; a.ncy = ev->ncy;
+    a.dt = ev->cfg.dt; a.dx = ev->cfg.dx; a.dy = ev->cfg.dy; a.dz = ev->cfg.dz;
+    a.eos = dev_eos(ev);
+    a.eos_kind = ev->cfg.eos_kind;
+    vh::launch_vorticity(a, ev->stream);
+}
+
 static vh::StageMarks *next_marks(vh_event *ev)
 {
     if (!ev->timing) return nullptr;
@@ -261,6 +274,7 @@ int vh_event_step(vh_event *ev, int nsteps)
         launch(A, next_marks(ev));
         std::swap(ev->qc, ev->qn);
         std::swap(ev->uc, ev->up);
+        if (ev->vort_on) launch_vort(ev);        /* HydroPlugin.cpp:302-305 */
         ev->n += 1;
         ev->t = c.t0 + ev->n * c.dt;
     }
@@ -301,6 +315,8 @@ static const double *field_ptr(const vh_event *ev, int field)
     if (field >= VH_F_UPT && field < VH_F_UPT + 4) return ev->u[ev->up] + (long long)(field - VH_F_UPT) * ev->L;
     if (field == VH_F_E) return ev->ep[ev->ec];
     if (field == VH_F_P) return ev->ep[ev->ec] + ev->L;
+    if (ev->vort && field >= VH_F_W && field < VH_F_W + 6) return ev->vort + (long long)(field - VH_F_W) * ev->L;
+    if (ev->vort && field >= VH_F_BETA && field < VH_F_BETA + 4) return ev->vort + (long long)(6 + field - VH_F_BETA) * ev->L;
     return nullptr;
 }
 
@@ -321,6 +337,22 @@ int vh_event_device_field(vh_event *ev, int field, double **d_ptr)
     const double *src = field_ptr(ev, field);
     if (!src) return fail(VH_ERR_ARG, "unknown field id");
     *d_ptr = const_cast<double *>(src);
+    return VH_OK;
+}
+
+int vh_event_vorticity(vh_event *ev, int enable)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    if (!ev->initialised) return fail(VH_ERR_STATE, "vh_event_vorticity before vh_event_set_initial");
+    ev->vort_on = enable != 0;
+    if (!ev->vort_on) return VH_OK;
+    if (!ev->vort) {
+        const size_t B = (size_t)10 * ev->L * sizeof(double);
+        CUDA_TRY(cudaMalloc(&ev->vort, B));
+        CUDA_TRY(cudaMemsetAsync(ev->vort, 0, B, ev->stream));
+    }
+    launch_vort(ev);                              /* HydroPlugin.cpp:197-199 */
+    CUDA_TRY(cudaGetLastError());
     return VH_OK;
 }
 

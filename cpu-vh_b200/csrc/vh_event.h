@@ -68,6 +68,9 @@ struct vh_event {
     int *fo_hdr = nullptr;                /* pinned: n_above, n_total of the last block */
     cudaEvent_t fo_done = nullptr;
     bool fo_pending = false;              /* launched, not yet finished */
+    /* thermal vorticity (vh_event_vorticity): 6 w planes then 4 beta planes */
+    double *vort = nullptr;
+    bool vort_on = false;
     /* per-phase timing (vh_event_phase_timing) */
     bool timing = false;
     std::vector<vh::StageMarks> marks;    /* one per stage launched since enabling */

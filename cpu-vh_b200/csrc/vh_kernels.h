@@ -46,6 +46,18 @@ struct InitArgs {
 };
 
 void launch_init(const InitArgs &a, cudaStream_t s);
+
+/* Thermal vorticity of the current state (Vorticity.cpp:6-171) */
+struct VortArgs {
+    const double *u, *up, *e;           /* current u, previous-step u, e (padded planes) */
+    double *w;                          /* 6 planes wtx wty wtn wxy wxn wyn, then 4 planes beta t x y n */
+    long long L;
+    int nx, ny, nz, ncx, ncy;
+    double dt, dx, dy, dz;
+    DevEos eos;
+    int eos_kind;
+};
+void launch_vorticity(const VortArgs &a, cudaStream_t s);
 void launch_math_check(int which, const double *a, const double *b, int n, double *out, const PowfTab &pq, cudaStream_t s);
 /* Optional per-phase timing marks of one stage: ev[0] is recorded before the
  * first kernel, ev[n+1] after kernel n, whose phase id is phase[n]

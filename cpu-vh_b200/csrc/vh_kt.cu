@@ -65,6 +65,63 @@ __global__ void init_kernel(const __grid_constant__ InitArgs A)
     if (kk == A.nz + 1) { put(s + sxy); put(s + 2 * sxy); }
 }
 
+/* Vorticity.cpp:6-171 for one interior cell: beta_mu = u_mu / T with
+ * u_mu = (u^t, -u^x, -u^y, -u^eta) and T = T(e) of the cell (the neighbours'
+ * velocities are divided by this cell's T too), a backward time difference
+ * against the previous step's velocity and central spatial differences;
+ * w_{mu nu} = -(d_mu beta_nu - d_nu beta_mu) / 2.  Every quotient by T uses
+ * the cell's rounded reciprocal through div_rcp, which equals the IEEE
+ * quotient bit for bit. */
+template <int EOS>
+__global__ void vorticity_kernel(const __grid_constant__ VortArgs A)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    const int k = blockIdx.z + 2;
+    if (i >= A.nx + 2 || j >= A.ny + 2) return;
+    const long long L = A.L, sxy = (long long)A.ncx * A.ncy;
+    const long long s = i + (long long)A.ncx * j + sxy * k;
+    const double T = eos_T<EOS>(A.eos, __ldg(A.e + s));
+    const double yT = 1.0 / T;
+    const long long nb[6] = {s - 1, s + 1, s - A.ncx, s + A.ncx, s - sxy, s + sxy};
+    double b[4], ddt[4], dd[3][4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const double *uc = A.u + c * L, *upc = A.up + c * L;
+        const double u0 = (c == 0) ? __ldg(uc + s) : __ldg(uc + s) * -1.0;
+        const double p0 = (c == 0) ? __ldg(upc + s) : __ldg(upc + s) * -1.0;
+        double bn[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+            const double un = (c == 0) ? __ldg(uc + nb[m]) : __ldg(uc + nb[m]) * -1.0;
+            bn[m] = div_rcp(un, T, yT);
+        }
+        b[c] = div_rcp(u0, T, yT);
+        const double bp = div_rcp(p0, T, yT);
+        ddt[c] = (b[c] - bp) / A.dt;
+        dd[0][c] = (bn[1] - bn[0]) / (2.0 * A.dx);
+        dd[1][c] = (bn[3] - bn[2]) / (2.0 * A.dy);
+        dd[2][c] = (bn[5] - bn[4]) / (2.0 * A.dz);
+    }
+    double *w = A.w;
+    w[0 * L + s] = (-1.0 / 2.0) * (ddt[1] - dd[0][0]);
+    w[1 * L + s] = (-1.0 / 2.0) * (ddt[2] - dd[1][0]);
+    w[2 * L + s] = (-1.0 / 2.0) * (ddt[3] - dd[2][0]);
+    w[3 * L + s] = (-1.0 / 2.0) * (dd[0][2] - dd[1][1]);
+    w[4 * L + s] = (-1.0 / 2.0) * (dd[0][3] - dd[2][1]);
+    w[5 * L + s] = (-1.0 / 2.0) * (dd[1][3] - dd[2][2]);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) w[(6 + c) * L + s] = b[c];
+}
+
+void launch_vorticity(const VortArgs &a, cudaStream_t s)
+{
+    dim3 block(32, 4, 1);
+    dim3 grid((a.nx + 31) / 32, (a.ny + 3) / 4, a.nz);
+    if (a.eos_kind == 1) vorticity_kernel<1><<<grid, block, 0, s>>>(a);
+    else vorticity_kernel<0><<<grid, block, 0, s>>>(a);
+}
+
 /* device math self-check: 0 vh_tanh(a), 1 div_rcp(a, b, RN(1/b)), 2 IEEE a/b,
  * 3 powf_quarter(float(a)) */
 __global__ void math_check_kernel(int which, const double *a, const double *b, int n, double *out, PowfTab pq)

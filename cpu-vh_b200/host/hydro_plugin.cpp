@@ -471,6 +471,9 @@ void run(void *latticeParams, void *initCondParams, void *hydroParams, const cha
     die_on(vh_event_create(&cfg, rows.empty() ? nullptr : rows.data(), (int)(rows.size() / 4), &ev), "vh_event_create");
     die_on(vh_event_set_initial(ev, ic.e.data(), ic.p.data(), ic.u.data(), ic.pi.data(), cfg.bulk ? ic.Pi.data() : nullptr),
            "vh_event_set_initial");
+    /* thermal vorticity after the initial condition and after every step
+     * (THERMAL_VORTICITY is on in the reference, HydroPlugin.cpp:197-199, :302-305) */
+    die_on(vh_event_vorticity(ev, 1), "vh_event_vorticity");
 
     std::ofstream surf(std::string(outputDir) + "/surface.dat");
     std::vector<double> el;
@@ -497,6 +500,9 @@ void run(void *latticeParams, void *initCondParams, void *hydroParams, const cha
             dump_field(ev, 9, "pixy", t, outputDir, L);
             dump_field(ev, 13, "pinn", t, outputDir, L);
             if (cfg.bulk) dump_field(ev, 14, "Pi", t, outputDir, L);
+            dump_field(ev, VH_F_W + 3, "wxy", t, outputDir, L);
+            dump_field(ev, VH_F_BETA + 1, "beta_x", t, outputDir, L);
+            dump_field(ev, VH_F_BETA + 2, "beta_y", t, outputDir, L);
         }
         if (n % fac == 0) {
             int nel = 0, nabove = 0;

@@ -37,6 +37,7 @@ VH_EOS_CONFORMAL, VH_EOS_TABLE = 0, 1
 VH_ZETA_REFERENCE, VH_ZETA_GAUSSIAN = 0, 1
 VH_PREC_FP64, VH_PREC_MIXED = 0, 1
 VH_F_UT, VH_F_UPT, VH_F_E, VH_F_P = 100, 110, 200, 201
+VH_F_W, VH_F_BETA = 300, 310
 VH_FO_COLUMNS = 20
 PHASES = ("source", "flux_x", "flux_y", "flux_eta", "final", "fused")
 HBARC = 0.197326938
@@ -98,6 +99,7 @@ _sig("vh_event_fetch_surface", C.c_int, [_evp, C.c_void_p, C.c_int, C.POINTER(C.
 _sig("vh_event_stream", C.c_int, [_evp, C.POINTER(C.c_void_p)])
 _sig("vh_event_kernel_launches", C.c_int, [_evp, C.POINTER(C.c_int)])
 _sig("vh_event_phase_timing", C.c_int, [_evp, C.c_int])
+_sig("vh_event_vorticity", C.c_int, [_evp, C.c_int])
 _sig("vh_event_phase_times", C.c_int, [_evp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)])
 _btp = C.c_void_p
 _sig("vh_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(_btp)])
@@ -305,6 +307,10 @@ class Event:
 
     def phase_timing(self, enable: bool = True) -> None:
         check(lib.vh_event_phase_timing(self.h, 1 if enable else 0), "vh_event_phase_timing")
+
+    def vorticity(self, enable: bool = True) -> None:
+        """thermal vorticity now and after every step (fields VH_F_W.., VH_F_BETA..)"""
+        check(lib.vh_event_vorticity(self.h, 1 if enable else 0), "vh_event_vorticity")
 
     def phase_times(self) -> dict:
         """{phase name: (total ms, launches)} since phase_timing(True) or the last call."""

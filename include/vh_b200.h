@@ -59,6 +59,8 @@ extern "C" {
 #define VH_F_UPT         110   /* 110..113: previous-step u (the reference's `up`) */
 #define VH_F_E           200
 #define VH_F_P           201
+#define VH_F_W           300   /* 300..305: thermal vorticity w_tx w_ty w_tn w_xy w_xn w_yn (vh_event_vorticity) */
+#define VH_F_BETA        310   /* 310..313: thermal velocity beta_t beta_x beta_y beta_n = u_mu / T */
 
 /* columns of one freezeout element, the 20 columns of surface.dat
  * (FreezeOut.cpp:265-270): tau x y eta  ds0 ds1 ds2 ds3  ux uy un  e T P
@@ -162,6 +164,14 @@ int vh_event_fetch_surface(vh_event *ev, double *host_out, int cap_elements, int
  * one fused kernel on small lattices, or the source, x, y, [eta] flux and
  * finalize phase kernels on large ones). */
 int vh_event_kernel_launches(vh_event *ev, int *per_step);
+
+/* Thermal vorticity (calculateThermalVorticity, Vorticity.cpp:6-171, which
+ * the reference runs after the initial condition and after every step,
+ * HydroPlugin.cpp:197-199, :302-305).  Enabling computes it for the current
+ * state and then after every vh_event_step; the fields VH_F_W.. and
+ * VH_F_BETA.. hold it (interior cells; ghost cells are 0).  Batched steps do
+ * not update it. */
+int vh_event_vorticity(vh_event *ev, int enable);
 
 /* Per-phase device timing of the RK stages (no counterpart in the reference,
  * which times the whole loop, HydroPlugin.cpp:284-297).  While enabled,

@@ -70,6 +70,7 @@ def oracle_lib():
         L.vho_step.argtypes = [C.c_void_p, C.c_int]
         L.vho_get.argtypes = [C.c_void_p, C.c_int, _dp]
         L.vho_destroy.argtypes = [C.c_void_p]
+        L.vho_vorticity.argtypes = [C.c_void_p]
         for f in ("vho_eos_p", "vho_eos_T", "vho_eos_cs2", "vho_eos_e"):
             getattr(L, f).argtypes = [C.c_void_p, C.c_double]
             getattr(L, f).restype = C.c_double
@@ -112,6 +113,10 @@ class OracleEvent:
 
     def step(self, n=1):
         return self.L.vho_step(self.h, n)
+
+    def vorticity(self):
+        """thermal vorticity and velocity of the current state (fields 300+, 310+)"""
+        self.L.vho_vorticity(self.h)
 
     def field(self, fid):
         ncx, ncy, ncz = self.cfg.nx + 4, self.cfg.ny + 4, self.cfg.nz + 4
@@ -186,6 +191,10 @@ class RefEvent:
     def step(self, n=1):
         with _stdout_to_stderr():
             self.L.vhref_step(n)
+
+    def vorticity(self):
+        with _stdout_to_stderr():
+            self.L.vhref_vorticity()
 
     def time_steps(self, n):
         with _stdout_to_stderr():

@@ -32,6 +32,7 @@
 #endif
 
 #include "DynamicalVariables.h"
+#include "Vorticity.h"
 #include "LatticeParameters.h"
 #include "HydroParameters.h"
 #include "InitialConditionParameters.h"
@@ -402,9 +403,26 @@ int vhref_get(int which, double *out)
     else if (which >= 110 && which < 114) src = ufield(up, which - 110);
     else if (which == 200) src = e;
     else if (which == 201) src = p;
+    else if (which == 300) src = wmunu->wtx;
+    else if (which == 301) src = wmunu->wty;
+    else if (which == 302) src = wmunu->wtn;
+    else if (which == 303) src = wmunu->wxy;
+    else if (which == 304) src = wmunu->wxn;
+    else if (which == 305) src = wmunu->wyn;
+    else if (which == 310) src = beta_mu->beta_t;
+    else if (which == 311) src = beta_mu->beta_x;
+    else if (which == 312) src = beta_mu->beta_y;
+    else if (which == 313) src = beta_mu->beta_n;
     if (!src) return -1;
     memcpy(out, src, sizeof(double) * (size_t)len);
     return 0;
+}
+
+/* The thermal vorticity as the driver computes it after the initial
+ * condition and after every step (HydroPlugin.cpp:197-199, :302-305). */
+void vhref_vorticity(void)
+{
+    calculateThermalVorticity(g_t, g_lat.latticeSpacingProperTime, q, Q, &g_lat, &g_hydro);
 }
 
 /* One freezeout block of the driver loop (HydroPlugin.cpp:242-266) for loop

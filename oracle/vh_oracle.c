@@ -47,6 +47,8 @@ typedef struct {
     /* freezeout slabs: 2 x [11][N] (e, ux, uy, un, e, pixx, pixy, pixn, piyy, piyn, Pi) */
     double *slab[2];
     int fo_prev;
+    /* thermal vorticity (allocated by the first vho_vorticity): wtx wty wtn wxy wxn wyn, beta t x y n */
+    double *w[6], *beta[4];
 } vho_t;
 
 /* ------------------------------------------------------------------ EoS */
@@ -699,7 +701,52 @@ int vho_step(vho_t *h, int nsteps)
     return h->nan_flag;
 }
 
-/* which: 0..nq-1 -> q; 100+c -> u; 110+c -> up; 200 -> e; 201 -> p (padded arrays) */
+/* Vorticity.cpp:6-171: thermal velocity beta_mu = u_mu / T and the thermal
+ * vorticity w_{mu nu} = -(d_mu beta_nu - d_nu beta_mu) / 2 with a backward
+ * time difference (u against the previous step's up, both divided by the
+ * cell's T) and central spatial differences (neighbours' u over the cell's
+ * T), on the interior; u_mu = (u^t, -u^x, -u^y, -u^eta). */
+void vho_vorticity(vho_t *h)
+{
+    size_t len = (size_t)h->ncx * h->ncy * h->ncz;
+    if (!h->w[0]) {
+        for (int c = 0; c < 6; ++c) h->w[c] = (double *)calloc(len, 8);
+        for (int c = 0; c < 4; ++c) h->beta[c] = (double *)calloc(len, 8);
+    }
+    const double dt = h->dt, dx = h->dx, dy = h->dy, dz = h->dz;
+    for (int k = 2; k < h->ncz - 2; ++k)
+        for (int j = 2; j < h->ncy - 2; ++j)
+            for (int i = 2; i < h->ncx - 2; ++i) {
+                const int s = IDX(h, i, j, k);
+                const int nb[6] = {IDX(h, i - 1, j, k), IDX(h, i + 1, j, k), IDX(h, i, j - 1, k),
+                                   IDX(h, i, j + 1, k), IDX(h, i, j, k - 1), IDX(h, i, j, k + 1)};
+                const double T = eos_T(h, h->e[s]);
+                double b[4], bp[4], bn[6][4];
+                for (int c = 0; c < 4; ++c) {
+                    const double sg = (c == 0) ? 1.0 : -1.0;
+                    b[c] = (c == 0 ? h->u[c][s] : h->u[c][s] * sg) / T;
+                    bp[c] = (c == 0 ? h->up[c][s] : h->up[c][s] * sg) / T;
+                    for (int m = 0; m < 6; ++m) bn[m][c] = (c == 0 ? h->u[c][nb[m]] : h->u[c][nb[m]] * sg) / T;
+                }
+                for (int c = 0; c < 4; ++c) h->beta[c][s] = b[c];
+                double ddt[4], ddx[4], ddy[4], ddn[4];
+                for (int c = 0; c < 4; ++c) {
+                    ddt[c] = (b[c] - bp[c]) / dt;
+                    ddx[c] = (bn[1][c] - bn[0][c]) / (2.0 * dx);
+                    ddy[c] = (bn[3][c] - bn[2][c]) / (2.0 * dy);
+                    ddn[c] = (bn[5][c] - bn[4][c]) / (2.0 * dz);
+                }
+                h->w[0][s] = (-1.0 / 2.0) * (ddt[1] - ddx[0]);
+                h->w[1][s] = (-1.0 / 2.0) * (ddt[2] - ddy[0]);
+                h->w[2][s] = (-1.0 / 2.0) * (ddt[3] - ddn[0]);
+                h->w[3][s] = (-1.0 / 2.0) * (ddx[2] - ddy[1]);
+                h->w[4][s] = (-1.0 / 2.0) * (ddx[3] - ddn[1]);
+                h->w[5][s] = (-1.0 / 2.0) * (ddy[3] - ddn[2]);
+            }
+}
+
+/* which: 0..nq-1 -> q; 100+c -> u; 110+c -> up; 200 -> e; 201 -> p;
+ * 300+c -> w (tx ty tn xy xn yn); 310+c -> beta (t x y n) (padded arrays) */
 int vho_get(vho_t *h, int which, double *out)
 {
     size_t len = (size_t)h->ncx * h->ncy * h->ncz;
@@ -709,6 +756,8 @@ int vho_get(vho_t *h, int which, double *out)
     else if (which >= 110 && which < 114) src = h->up[which - 110];
     else if (which == 200) src = h->e;
     else if (which == 201) src = h->p;
+    else if (which >= 300 && which < 306) src = h->w[which - 300];
+    else if (which >= 310 && which < 314) src = h->beta[which - 310];
     if (!src) return -1;
     memcpy(out, src, 8 * len);
     return 0;
@@ -723,6 +772,8 @@ void vho_destroy(vho_t *h)
     free(h->e); free(h->p);
     for (int c = 0; c < 4; ++c) { free(h->u[c]); free(h->up[c]); free(h->uS[c]); }
     for (int s = 0; s < 2; ++s) free(h->slab[s]);
+    for (int c = 0; c < 6; ++c) free(h->w[c]);
+    for (int c = 0; c < 4; ++c) free(h->beta[c]);
     free(h->p_tb); free(h->T_tb);
     free(h);
 }

@@ -67,3 +67,5 @@ def test_cpu_vh_executable_runs_ideal_gubser(tmp_path):
     surf = open(os.path.join(tmp, "out", "surface.dat")).read().splitlines()
     assert len(surf) > 0 and all(len(ln.split()) == 20 for ln in surf[:50])
     assert os.path.exists(os.path.join(tmp, "out", "e_1.000.dat"))
+    for name in ("wxy", "beta_x", "beta_y"):      # the reference's vorticity dumps (HydroPlugin.cpp:66-70)
+        assert os.path.exists(os.path.join(tmp, "out", f"{name}_1.000.dat")), name

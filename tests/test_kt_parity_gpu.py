@@ -113,3 +113,33 @@ def test_large_lattice_forms_bitexact(env):
     line = [l for l in out.stdout.splitlines() if l.startswith("LAUNCHES")][-1].split()
     assert int(line[1]) == (2 if env.get("VH_STAGE_MODE") == "fused" else 10)
     assert int(line[3]) == 0, line
+
+
+@pytest.mark.parametrize("case", ["gubser", "glauber"])
+def test_thermal_vorticity_bitexact(case):
+    """thermal vorticity and velocity after the initial condition and after
+    steps equal the oracle's (itself equal to the reference's) on the interior"""
+    if case == "gubser":
+        cfg, rows = vh.gubser_config(41, 37), None
+        st = vh.gubser_ic(cfg)
+    else:
+        cfg = vh.glauber_config(27, 25, 9)
+        cfg.dx = cfg.dy = 0.5
+        cfg.dz = 0.4
+        cfg.dt = 0.05
+        rows = vh.synthetic_eos_table()
+        st = vh.glauber_ic(cfg, rows)
+    gpu, orc = vh.Event(cfg, rows), OracleEvent(cfg, rows)
+    gpu.set_initial(st)
+    orc.set_initial(st)
+    gpu.vorticity(True)
+    for n in (0, 1, 4):
+        if n:
+            gpu.step(n)
+            assert orc.step(n) == 0
+        orc.vorticity()
+        gpu.sync()
+        for f in list(range(vh.VH_F_W, vh.VH_F_W + 6)) + list(range(vh.VH_F_BETA, vh.VH_F_BETA + 4)):
+            a, b = vh.interior(cfg, gpu.field(f)), vh.interior(cfg, orc.field(f))
+            assert np.count_nonzero(np.ascontiguousarray(a).view(np.uint64) !=
+                                    np.ascontiguousarray(b).view(np.uint64)) == 0, (case, n, f)

@@ -130,3 +130,32 @@ def test_cornelius_known_answers(dim):
     assert n == gold["elements"]
     txt = K.format_elements(out[:n]).encode()
     assert hashlib.sha256(txt).hexdigest() == gold["sha256"]
+
+
+W_FIELDS = list(range(300, 306)) + list(range(310, 314))
+
+
+@pytest.mark.parametrize("case,variant", [("gubser", "conf"), ("glauber", "table")])
+def test_vorticity_bitexact_vs_reference(case, variant):
+    """thermal vorticity and velocity (Vorticity.cpp:6-171) after the initial
+    condition and after steps, as the driver computes them, on the interior
+    (the reference's ghost-cell routine also copies w and beta into the ghost
+    layers during the RK stages, i.e. the previous step's values; nothing reads
+    them)"""
+    if not O.ref_available(variant):
+        pytest.skip("reference build not present")
+    cfg, rows, st = CASES[case]()
+    ref = O.RefEvent(variant, cfg, rows, threads=1)
+    orc = O.OracleEvent(cfg, rows)
+    ref.set_initial(st)
+    orc.set_initial(st)
+    for n in (0, 1, 3):
+        if n:
+            ref.step(n)
+            assert orc.step(n) == 0
+        ref.vorticity()
+        orc.vorticity()
+        for f in W_FIELDS:
+            a, b = vh.interior(cfg, ref.field(f)), vh.interior(cfg, orc.field(f))
+            assert np.count_nonzero(a.view(np.uint64) != b.view(np.uint64)) == 0, (case, n, f)
+        assert np.any(orc.field(303) != 0) or n == 0
