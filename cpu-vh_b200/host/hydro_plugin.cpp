@@ -11,8 +11,12 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <fstream>
+#include <mutex>
+#include <thread>
 #include <getopt.h>
 #include <iostream>
 #include <string>
@@ -265,6 +269,65 @@ bool build_ic(IC &ic, const LatticeParameters &L, const InitialConditionParamete
     }
 }
 
+/* surface.dat on a thread of its own: the run loop hands each freezeout
+ * block's elements over (moved, not copied) and goes on stepping while they
+ * are formatted with the reference's stream formatting (FreezeOut.cpp:265-270:
+ * default precision, space separated, one element per line), so the text
+ * formatting is off the evolution's critical path and the file's bytes are
+ * the same as when written in line. */
+class SurfaceWriter {
+ public:
+    explicit SurfaceWriter(const std::string &path) : out_(path), th_([this] { loop(); }) {}
+    ~SurfaceWriter() { close(); }
+    void push(std::vector<double> &&block)
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            q_.push_back(std::move(block));
+        }
+        cv_.notify_one();
+    }
+    void close()
+    {
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            done_ = true;
+        }
+        cv_.notify_one();
+        if (th_.joinable()) th_.join();
+        if (out_.is_open()) out_.close();
+    }
+
+ private:
+    void loop()
+    {
+        for (;;) {
+            std::vector<double> b;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [&] { return done_ || !q_.empty(); });
+                if (q_.empty()) return;
+                b = std::move(q_.front());
+                q_.pop_front();
+            }
+            for (size_t i = 0; i + VH_FO_COLUMNS <= b.size(); i += VH_FO_COLUMNS) {
+                const double *o = &b[i];
+                for (int c = 0; c < VH_FO_COLUMNS; ++c) {
+                    if (c) out_ << " ";
+                    out_ << o[c];
+                }
+                out_ << '\n';
+            }
+        }
+    }
+    std::ofstream out_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<std::vector<double>> q_;
+    bool done_ = false;
+    std::thread th_;
+};
+
 void dump_field(vh_event *ev, int field, const char *name, double t, const char *dir, const LatticeParameters &L)
 {
     const int nx = L.numLatticePointsX, ny = L.numLatticePointsY, nz = L.numLatticePointsRapidity;
@@ -475,8 +538,7 @@ void run(void *latticeParams, void *initCondParams, void *hydroParams, const cha
      * (THERMAL_VORTICITY is on in the reference, HydroPlugin.cpp:197-199, :302-305) */
     die_on(vh_event_vorticity(ev, 1), "vh_event_vorticity");
 
-    std::ofstream surf(std::string(outputDir) + "/surface.dat");
-    std::vector<double> el;
+    SurfaceWriter surf(std::string(outputDir) + "/surface.dat");
     const int ncx = nx + 4, ncy = ny + 4, ncz = nz + 4;
     const int ictr = (nx % 2 == 0) ? ncx / 2 : (ncx - 1) / 2, jctr = (ny % 2 == 0) ? ncy / 2 : (ncy - 1) / 2;
     const int kctr = (nz % 2 == 0) ? ncz / 2 : (ncz - 1) / 2;
@@ -508,16 +570,9 @@ void run(void *latticeParams, void *initCondParams, void *hydroParams, const cha
             int nel = 0, nabove = 0;
             die_on(vh_event_freezeout(ev, &nel, &nabove), "vh_event_freezeout");
             if (H.doFreezeOut && nel > 0) {
-                el.resize((size_t)nel * VH_FO_COLUMNS);
+                std::vector<double> el((size_t)nel * VH_FO_COLUMNS);
                 die_on(vh_event_fetch_surface(ev, el.data(), nel, &nel), "vh_event_fetch_surface");
-                for (int i = 0; i < nel; ++i) {
-                    const double *o = &el[(size_t)i * VH_FO_COLUMNS];
-                    /* FreezeOut.cpp:265-270 */
-                    surf << o[0] << " " << o[1] << " " << o[2] << " " << o[3] << " " << o[4] << " " << o[5] << " " << o[6]
-                         << " " << o[7] << " " << o[8] << " " << o[9] << " " << o[10] << " " << o[11] << " " << o[12] << " "
-                         << o[13] << " " << o[14] << " " << o[15] << " " << o[16] << " " << o[17] << " " << o[18] << " "
-                         << o[19] << std::endl;
-                }
+                surf.push(std::move(el));
             }
             if (nabove == 0) acc2 += 1;
             if (acc2 >= 3 && icp.initialConditionType != 12) {
