@@ -165,7 +165,9 @@ def serve_stream(n_events, rate, seed=2025):
     """The served mix: 70 % 2+1D lumpy events (n x n, n uniform in 61..201
     step 20, hotspot initial conditions) and 30 % 3+1D smooth events (n x n x
     n_eta, n uniform in 101..201 step 20, n_eta in 21..81 step 20, optical
-    Glauber with b uniform in 0-12 fm); Poisson arrivals at `rate`."""
+    Glauber with b uniform in 0-12 fm); Poisson arrivals at `rate`.  Each
+    event is (arrival time, config, generator kind, generator argument): the
+    initial states are made on the device when the event is admitted."""
     import numpy as np
     import vh
     rng = np.random.default_rng(seed)
@@ -176,17 +178,23 @@ def serve_stream(n_events, rate, seed=2025):
         if rng.random() < 0.7:
             c = vh.hotspot_config(int(rng.choice(np.arange(61, 202, 20))))
             c.fo_factor = 10
-            st = vh.hotspot_ic(c, rows, seed=10_000 + i)
+            out.append((t, c, "hotspots", 10_000 + i))
         else:
             n = int(rng.choice(np.arange(101, 202, 20)))
             c = vh.glauber_config(n, n, int(rng.choice([21, 41, 61, 81])))
             c.fo_factor = 10
-            st = vh.glauber_ic(c, rows, b=float(rng.uniform(0.0, 12.0)))
-        out.append((t, c, st))
+            out.append((t, c, "glauber", float(rng.uniform(0.0, 12.0))))
     desc = (f"serve_mix: {n_events} events, Poisson arrivals at {rate:g}/s (seed {seed}); 70% 2+1D hotspot events "
             "n x n, n in 61..201 step 20; 30% 3+1D optical-Glauber events n x n x n_eta, n in 101..201 step 20, "
-            "n_eta in 21..81 step 20, b uniform 0-12 fm; freezeout every 10 steps, surfaces to host")
+            "n_eta in 21..81 step 20, b uniform 0-12 fm; initial states generated on the device; freezeout every "
+            "10 steps, surfaces to host")
     return out, rows, desc
+
+
+def _init_of(kind, arg):
+    if kind == "hotspots":
+        return lambda ev: ev.init_hotspots(seed=arg)
+    return lambda ev: ev.init_glauber(b=arg)
 
 
 def pct(xs, q):
@@ -212,31 +220,35 @@ def run_serve(args, rank):
     srv.take_surface(1 << 40)
     t_start = time.perf_counter()
     base = None
-    for i, (t_arr, c, st) in enumerate(stream):
+    for i, (t_arr, c, kind, arg) in enumerate(stream):
         dt = t_arr - (time.perf_counter() - t_start)
         if dt > 0:
             time.sleep(dt)
-        srv.submit(c.copy(precision=prec), st, i)
+        if kind == "hotspots":
+            srv.submit_hotspots(c.copy(precision=prec), i, seed=arg)
+        else:
+            srv.submit_glauber(c.copy(precision=prec), i, b=arg)
     srv.wait(3600)
     done = srv.poll(len(stream) + 16)
     stats = srv.stats()
     lat = [d.t_done - d.t_submit for d in done]
     first = min(d.t_submit for d in done)
     span = max(d.t_done for d in done) - first
-    cells = sum(d.steps * c.nx * c.ny * c.nz for d, (_, c, _) in zip(sorted(done, key=lambda d: d.tag), stream))
+    cells = sum(d.steps * c.nx * c.ny * c.nz for d, (_, c, _, _) in zip(sorted(done, key=lambda d: d.tag), stream))
     bad = [d.tag for d in done if d.status != 0]
     srv.close()
 
     # the plain path: each event alone, FP64, same cadence and cap, FCFS
     service, serial_bad = [], []
-    for i, (_, c, st) in enumerate(stream):
+    for i, (_, c, kind, arg) in enumerate(stream):
         t0 = time.perf_counter()
-        _, _, status = vh.run_like_server(c.copy(precision=vh.VH_PREC_FP64), rows, st, max_steps=args.max_steps)
+        _, _, status = vh.run_like_server(c.copy(precision=vh.VH_PREC_FP64), rows, _init_of(kind, arg),
+                                          max_steps=args.max_steps)
         service.append(time.perf_counter() - t0)
         if status:
             serial_bad.append(i)
     free_at, slat = 0.0, []
-    for (t_arr, _, _), sv in zip(stream, service):
+    for (t_arr, _, _, _), sv in zip(stream, service):
         start = max(t_arr, free_at)
         free_at = start + sv
         slat.append(free_at - t_arr)
@@ -249,7 +261,8 @@ def run_serve(args, rank):
                        "admission": "80% of free HBM", "precision": args.precision},
             "latency_s": {"p50": pct(lat, 50), "p95": pct(lat, 95), "p99": pct(lat, 99), "max": max(lat)},
             "cell_updates_per_s": cells / span,
-            "server": {k: stats[k] for k in ("steps", "fo_blocks", "batch_builds")} | {"events_with_device_error": bad},
+            "server": {k: stats[k] for k in ("steps", "fo_blocks", "batch_builds", "t_admit_s", "t_build_s",
+                                             "t_step_s", "t_fo_s")} | {"events_with_device_error": bad},
             "serial_plain_fp64": {"events_per_s": len(stream) / serial_span,
                                   "latency_s": {"p50": pct(slat, 50), "p95": pct(slat, 95), "p99": pct(slat, 99)},
                                   "events_with_device_error": serial_bad,

@@ -212,6 +212,53 @@ int vh_event_set_initial(vh_event *ev, const double *e, const double *p, const d
     return do_init(ev, d, d + N, d + 2 * N, pi ? d + 6 * N : nullptr, Pi ? d + 16 * N : nullptr);
 }
 
+int vh_event_init_glauber(vh_event *ev, double R, double a, double sigma_nn, double b, double e0_GeV,
+                          double eta_flat, double eta_sigma)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    if (!(R > 0 && a > 0 && sigma_nn > 0 && e0_GeV > 0 && eta_sigma > 0)) return fail(VH_ERR_ARG, "bad Glauber parameters");
+    const size_t N = (size_t)ev->N;
+    double *d = ev->ic;
+    vh::GlauberArgs g;
+    g.nx = ev->cfg.nx; g.ny = ev->cfg.ny; g.nz = ev->cfg.nz;
+    g.dx = ev->cfg.dx; g.dy = ev->cfg.dy; g.dz = ev->cfg.dz;
+    g.R = R; g.a = a; g.sigma_nn = sigma_nn; g.b = b; g.e0 = e0_GeV / vh::kHbarc;
+    g.eta_flat = eta_flat; g.eta_sigma = eta_sigma;
+    g.eos = dev_eos(ev);
+    g.eos_kind = ev->cfg.eos_kind;
+    /* staging: e, p, u(4) as vh_event_set_initial; the participant density and
+     * its maximum borrow the (unused) pi and Pi slots */
+    vh::launch_glauber_ic(g, d + 6 * N, reinterpret_cast<unsigned long long *>(d + 16 * N), d, d + N, d + 2 * N,
+                          ev->stream);
+    CUDA_TRY(cudaGetLastError());
+    return do_init(ev, d, d + N, d + 2 * N, nullptr, nullptr);
+}
+
+int vh_event_init_hotspots(vh_event *ev, unsigned long long seed, double mean_spots, double w, double k_gamma,
+                           double amp_mean_GeV, double R, double a)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    if (ev->cfg.nz != 1 || k_gamma < 1.0 || !(w > 0) || !(mean_spots >= 0))
+        return fail(VH_ERR_ARG, "hotspot events are 2+1D, with k_gamma >= 1 and w > 0");
+    std::vector<double> cx, cy, amp;
+    vh::draw_hotspots(seed, mean_spots, k_gamma, amp_mean_GeV, R, a, cx, cy, amp);
+    const size_t N = (size_t)ev->N, ns = cx.size();
+    if (3 * ns > 10 * N) return fail(VH_ERR_ARG, "lattice too small for the number of hotspots drawn");
+    std::vector<double> spots(3 * ns);
+    for (size_t k = 0; k < ns; ++k) { spots[k] = cx[k]; spots[ns + k] = cy[k]; spots[2 * ns + k] = amp[k]; }
+    double *d = ev->ic;
+    if (ns) CUDA_TRY(cudaMemcpyAsync(d + 6 * N, spots.data(), 3 * ns * sizeof(double), cudaMemcpyHostToDevice, ev->stream));
+    vh::HotspotArgs h;
+    h.nx = ev->cfg.nx; h.ny = ev->cfg.ny; h.dx = ev->cfg.dx; h.dy = ev->cfg.dy; h.w = w;
+    h.spots = d + 6 * N;
+    h.nspots = (int)ns;
+    h.eos = dev_eos(ev);
+    h.eos_kind = ev->cfg.eos_kind;
+    vh::launch_hotspot_ic(h, d, d + N, d + 2 * N, ev->stream);
+    CUDA_TRY(cudaGetLastError());
+    return do_init(ev, d, d + N, d + 2 * N, nullptr, nullptr);
+}
+
 int vh_event_set_initial_device(vh_event *ev, const double *d_e, const double *d_p, const double *d_u, const double *d_pi, const double *d_Pi)
 {
     if (!ev || !d_e || !d_p || !d_u) return fail(VH_ERR_ARG, "null argument");

@@ -47,6 +47,26 @@ struct InitArgs {
 
 void launch_init(const InitArgs &a, cudaStream_t s);
 
+/* Initial conditions on the device (vh_ic.cu) into interior planes e, p, u */
+struct GlauberArgs {
+    int nx, ny, nz;
+    double dx, dy, dz;
+    double R, a, sigma_nn, b, e0, eta_flat, eta_sigma;   /* e0 in fm^-4 */
+    DevEos eos;
+    int eos_kind;
+};
+struct HotspotArgs {
+    int nx, ny;
+    double dx, dy, w;
+    const double *spots;     /* device: x[n], y[n], amplitude[n] (fm^-4) */
+    int nspots;
+    DevEos eos;
+    int eos_kind;
+};
+void launch_glauber_ic(const GlauberArgs &g, double *npart, unsigned long long *mx, double *e, double *p, double *u,
+                       cudaStream_t s);
+void launch_hotspot_ic(const HotspotArgs &h, double *e, double *p, double *u, cudaStream_t s);
+
 /* Thermal vorticity of the current state (Vorticity.cpp:6-171) */
 struct VortArgs {
     const double *u, *up, *e;           /* current u, previous-step u, e (padded planes) */

@@ -338,21 +338,24 @@ struct CounterRng {
     }
 };
 
-int vh_ic_hotspots(const vh_config *cfg, const double *rows, int nrows, uint64_t seed, double mean_spots,
-                   double w, double k_gamma, double amp_mean_GeV, double R, double a,
-                   double *e, double *p, double *u)
+} /* extern "C" */
+
+/* The random part of the hotspot initial condition: Poisson(mean_spots)
+ * centres accepted with the b = 0 Woods-Saxon participant density, Gamma(k)
+ * amplitudes scaled to a mean of amp_mean_GeV; shared by the host generator
+ * and the device one (vh_event_init_hotspots). */
+void vh::draw_hotspots(uint64_t seed, double mean_spots, double k_gamma, double amp_mean_GeV, double R, double a,
+                       std::vector<double> &cx, std::vector<double> &cy, std::vector<double> &amp)
 {
-    if (!cfg || !e || !p || !u || cfg->nz != 1 || k_gamma < 1.0) return VH_ERR_ARG;
-    vh::HostEos eos;
-    eos.init(*cfg, rows, nrows);
     CounterRng rng(seed);
     const double sigma_nn = 4.2;
     const double box = R + 3. * a;
-    /* participant density at b = 0 as the acceptance weight */
     const double TA0 = ws_thickness(0.0, R, a);
     const double wmax = 2. * TA0 * (1. - std::exp(-sigma_nn * TA0));
     int nspots = rng.poisson(mean_spots);
-    std::vector<double> cx(nspots), cy(nspots), amp(nspots);
+    cx.assign(nspots, 0.0);
+    cy.assign(nspots, 0.0);
+    amp.assign(nspots, 0.0);
     for (int s = 0; s < nspots; ++s) {
         for (int tries = 0; tries < 100000; ++tries) {
             double x = (2. * rng.uniform() - 1.) * box, y = (2. * rng.uniform() - 1.) * box;
@@ -362,6 +365,20 @@ int vh_ic_hotspots(const vh_config *cfg, const double *rows, int nrows, uint64_t
         }
         amp[s] = amp_mean_GeV / kHbarc * rng.gamma(k_gamma) / k_gamma;
     }
+}
+
+extern "C" {
+
+int vh_ic_hotspots(const vh_config *cfg, const double *rows, int nrows, uint64_t seed, double mean_spots,
+                   double w, double k_gamma, double amp_mean_GeV, double R, double a,
+                   double *e, double *p, double *u)
+{
+    if (!cfg || !e || !p || !u || cfg->nz != 1 || k_gamma < 1.0) return VH_ERR_ARG;
+    vh::HostEos eos;
+    eos.init(*cfg, rows, nrows);
+    std::vector<double> cx, cy, amp;
+    vh::draw_hotspots(seed, mean_spots, k_gamma, amp_mean_GeV, R, a, cx, cy, amp);
+    const int nspots = (int)cx.size();
     const int nx = cfg->nx, ny = cfg->ny;
     const size_t N = (size_t)nx * ny;
     const double inv2w2 = 1. / (2. * w * w);

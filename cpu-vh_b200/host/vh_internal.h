@@ -5,6 +5,7 @@
 #ifndef VH_INTERNAL_H
 #define VH_INTERNAL_H
 
+#include <cstdint>
 #include <string>
 #include <vector>
 #include "vh_b200.h"
@@ -46,6 +47,10 @@ const PowfQuarterTable &powf_quarter_table();
 
 /* records msg as the calling thread's vh_last_error() and returns code */
 int set_error(int code, const std::string &msg);
+
+/* the random draws of the hotspot initial condition (centres, amplitudes in fm^-4) */
+void draw_hotspots(uint64_t seed, double mean_spots, double k_gamma, double amp_mean_GeV, double R, double a,
+                   std::vector<double> &cx, std::vector<double> &cy, std::vector<double> &amp);
 
 } // namespace vh
 

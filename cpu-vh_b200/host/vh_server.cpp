@@ -50,6 +50,9 @@ struct Job {
     unsigned long long tag = 0;
     vh_config cfg{};
     std::vector<double> e, p, u, pi, Pi;
+    int ic_kind = 0;                /* 0 host arrays, 1 device Glauber, 2 device hotspots */
+    double icp[8] = {0};            /* generator parameters */
+    unsigned long long seed = 0;
     double t_submit = 0, t_admit = 0;
     vh_event *ev = nullptr;
     size_t bytes = 0;
@@ -141,6 +144,12 @@ void worker_main(vh_server *S)
     vh_batch *batch = nullptr;
     bool membership_changed = false;
     int held_rounds = 0;        /* rounds an admission waited for alignment */
+    auto tick = [] { return Clock::now(); };
+    auto add = [&](double &acc, Clock::time_point a) {
+        const double d = std::chrono::duration<double>(Clock::now() - a).count();
+        std::lock_guard<std::mutex> lk(S->mu);
+        acc += d;
+    };
     bool waiting = false;       /* events queued after this round's admission */
     auto set_fatal = [&](int rc, const char *where) {
         std::lock_guard<std::mutex> lk(S->mu);
@@ -177,12 +186,21 @@ void worker_main(vh_server *S)
             S->st.bytes_in_use = S->used;
             waiting = !S->queue.empty();
         }
+        const auto t_adm = tick();
         for (auto &j : admitted) {
             int rc = vh_event_create(&j->cfg, S->eos_rows.empty() ? nullptr : S->eos_rows.data(),
                                      (int)S->eos_rows.size() / 4, &j->ev);
-            if (rc == VH_OK)
-                rc = vh_event_set_initial(j->ev, j->e.data(), j->p.data(), j->u.data(),
-                                          j->pi.empty() ? nullptr : j->pi.data(), j->Pi.empty() ? nullptr : j->Pi.data());
+            if (rc == VH_OK) {
+                if (j->ic_kind == 1)
+                    rc = vh_event_init_glauber(j->ev, j->icp[0], j->icp[1], j->icp[2], j->icp[3], j->icp[4], j->icp[5],
+                                               j->icp[6]);
+                else if (j->ic_kind == 2)
+                    rc = vh_event_init_hotspots(j->ev, j->seed, j->icp[0], j->icp[1], j->icp[2], j->icp[3], j->icp[4],
+                                                j->icp[5]);
+                else
+                    rc = vh_event_set_initial(j->ev, j->e.data(), j->p.data(), j->u.data(),
+                                              j->pi.empty() ? nullptr : j->pi.data(), j->Pi.empty() ? nullptr : j->Pi.data());
+            }
             j->t_admit = S->now();
             std::vector<double>().swap(j->e);
             std::vector<double>().swap(j->p);
@@ -193,9 +211,11 @@ void worker_main(vh_server *S)
             S->active.push_back(std::move(j));
             membership_changed = true;
         }
+        if (!admitted.empty()) add(S->st.t_admit_s, t_adm);
         if (S->active.empty()) continue;
 
         /* ---- batch (rebuilt when members changed) */
+        const auto t_bld = tick();
         if (membership_changed || !batch) {
             if (batch) vh_batch_destroy(batch);
             batch = nullptr;
@@ -217,6 +237,7 @@ void worker_main(vh_server *S)
                 S->st.batch_builds += 1;
             }
             membership_changed = false;
+            add(S->st.t_build_s, t_bld);
         }
 
         /* ---- steps up to the earliest freezeout block (0: a block is due now) */
@@ -229,8 +250,13 @@ void worker_main(vh_server *S)
         if (S->cfg.max_steps > 0)
             for (auto &j : S->active) k = std::min(k, std::max(0, S->cfg.max_steps - j->steps));
         if (k > 0) {
+            const auto t_st = tick();
             int rc = vh_batch_step(batch, k);
             if (rc != VH_OK) { set_fatal(rc, "vh_batch_step"); break; }
+            void *bs = nullptr;
+            vh_batch_stream(batch, &bs);
+            cudaStreamSynchronize((cudaStream_t)bs);
+            add(S->st.t_step_s, t_st);
             for (auto &j : S->active) j->steps += k;
             std::lock_guard<std::mutex> lk(S->mu);
             S->st.steps += k;
@@ -240,6 +266,7 @@ void worker_main(vh_server *S)
         std::vector<Job *> due;
         for (auto &j : S->active)
             if (steps_to_block(*j) == 0) due.push_back(j.get());
+        const auto t_fo = tick();
         for (Job *j : due) {
             int rc = vh_event_freezeout_launch(j->ev);
             if (rc != VH_OK) j->status = rc;
@@ -259,6 +286,7 @@ void worker_main(vh_server *S)
             if (nab == 0) j->zero_blocks += 1;
         }
         if (!due.empty()) {
+            add(S->st.t_fo_s, t_fo);
             std::lock_guard<std::mutex> lk(S->mu);
             S->st.fo_blocks += (long long)due.size();
         }
@@ -322,21 +350,8 @@ int vh_server_create(const vh_server_config *cfg, const double *eos_rows, int eo
     return VH_OK;
 }
 
-int vh_server_submit(vh_server *S, const vh_config *cfg, const double *e, const double *p, const double *u,
-                     const double *pi, const double *Pi, unsigned long long tag)
+static int enqueue(vh_server *S, std::unique_ptr<Job> j)
 {
-    if (!S || !cfg || !e || !p || !u) return vh::set_error(VH_ERR_ARG, "null argument");
-    if (cfg->eos_kind == VH_EOS_TABLE && S->eos_rows.empty())
-        return vh::set_error(VH_ERR_ARG, "tabulated-EoS event on a server created without EoS rows");
-    auto j = std::make_unique<Job>();
-    j->tag = tag;
-    j->cfg = *cfg;
-    const size_t N = (size_t)cfg->nx * cfg->ny * cfg->nz;
-    j->e.assign(e, e + N);
-    j->p.assign(p, p + N);
-    j->u.assign(u, u + 4 * N);
-    if (pi) j->pi.assign(pi, pi + 10 * N);
-    if (Pi) j->Pi.assign(Pi, Pi + N);
     std::lock_guard<std::mutex> lk(S->mu);
     if (S->fatal != VH_OK) return vh::set_error(S->fatal, S->fatal_msg);
     j->t_submit = S->now();
@@ -346,6 +361,62 @@ int vh_server_submit(vh_server *S, const vh_config *cfg, const double *e, const 
     S->st.queued += 1;
     S->cv.notify_all();
     return VH_OK;
+}
+
+static int check_submit(vh_server *S, const vh_config *cfg)
+{
+    if (!S || !cfg) return vh::set_error(VH_ERR_ARG, "null argument");
+    if (cfg->eos_kind == VH_EOS_TABLE && S->eos_rows.empty())
+        return vh::set_error(VH_ERR_ARG, "tabulated-EoS event on a server created without EoS rows");
+    return VH_OK;
+}
+
+int vh_server_submit(vh_server *S, const vh_config *cfg, const double *e, const double *p, const double *u,
+                     const double *pi, const double *Pi, unsigned long long tag)
+{
+    if (!e || !p || !u) return vh::set_error(VH_ERR_ARG, "null argument");
+    int rc = check_submit(S, cfg);
+    if (rc != VH_OK) return rc;
+    auto j = std::make_unique<Job>();
+    j->tag = tag;
+    j->cfg = *cfg;
+    const size_t N = (size_t)cfg->nx * cfg->ny * cfg->nz;
+    j->e.assign(e, e + N);
+    j->p.assign(p, p + N);
+    j->u.assign(u, u + 4 * N);
+    if (pi) j->pi.assign(pi, pi + 10 * N);
+    if (Pi) j->Pi.assign(Pi, Pi + N);
+    return enqueue(S, std::move(j));
+}
+
+int vh_server_submit_glauber(vh_server *S, const vh_config *cfg, double R, double a, double sigma_nn, double b,
+                             double e0_GeV, double eta_flat, double eta_sigma, unsigned long long tag)
+{
+    int rc = check_submit(S, cfg);
+    if (rc != VH_OK) return rc;
+    auto j = std::make_unique<Job>();
+    j->tag = tag;
+    j->cfg = *cfg;
+    j->ic_kind = 1;
+    const double v[7] = {R, a, sigma_nn, b, e0_GeV, eta_flat, eta_sigma};
+    std::copy(v, v + 7, j->icp);
+    return enqueue(S, std::move(j));
+}
+
+int vh_server_submit_hotspots(vh_server *S, const vh_config *cfg, unsigned long long seed, double mean_spots, double w,
+                              double k_gamma, double amp_mean_GeV, double R, double a, unsigned long long tag)
+{
+    int rc = check_submit(S, cfg);
+    if (rc != VH_OK) return rc;
+    if (cfg->nz != 1) return vh::set_error(VH_ERR_ARG, "hotspot events are 2+1D");
+    auto j = std::make_unique<Job>();
+    j->tag = tag;
+    j->cfg = *cfg;
+    j->ic_kind = 2;
+    j->seed = seed;
+    const double v[6] = {mean_spots, w, k_gamma, amp_mean_GeV, R, a};
+    std::copy(v, v + 6, j->icp);
+    return enqueue(S, std::move(j));
 }
 
 int vh_server_poll(vh_server *S, vh_server_done *out, int max, int *n)

@@ -100,6 +100,8 @@ _sig("vh_event_stream", C.c_int, [_evp, C.POINTER(C.c_void_p)])
 _sig("vh_event_kernel_launches", C.c_int, [_evp, C.POINTER(C.c_int)])
 _sig("vh_event_phase_timing", C.c_int, [_evp, C.c_int])
 _sig("vh_event_vorticity", C.c_int, [_evp, C.c_int])
+_sig("vh_event_init_glauber", C.c_int, [_evp] + [C.c_double] * 7)
+_sig("vh_event_init_hotspots", C.c_int, [_evp, C.c_ulonglong] + [C.c_double] * 6)
 _sig("vh_event_phase_times", C.c_int, [_evp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)])
 _btp = C.c_void_p
 _sig("vh_batch_create", C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.POINTER(_btp)])
@@ -308,6 +310,14 @@ class Event:
     def phase_timing(self, enable: bool = True) -> None:
         check(lib.vh_event_phase_timing(self.h, 1 if enable else 0), "vh_event_phase_timing")
 
+    def init_glauber(self, R=6.38, a=0.535, sigma_nn=4.2, b=7.0, e0=30.0, eta_flat=3.0, eta_sigma=1.3):
+        """optical-Glauber initial state generated on the device (see glauber_ic)"""
+        check(lib.vh_event_init_glauber(self.h, R, a, sigma_nn, b, e0, eta_flat, eta_sigma), "vh_event_init_glauber")
+
+    def init_hotspots(self, seed: int, mean_spots=200.0, w=0.4, k_gamma=1.6, amp=20.0, R=6.38, a=0.535):
+        """hotspot initial state generated on the device (see hotspot_ic)"""
+        check(lib.vh_event_init_hotspots(self.h, seed, mean_spots, w, k_gamma, amp, R, a), "vh_event_init_hotspots")
+
     def vorticity(self, enable: bool = True) -> None:
         """thermal vorticity now and after every step (fields VH_F_W.., VH_F_BETA..)"""
         check(lib.vh_event_vorticity(self.h, 1 if enable else 0), "vh_event_vorticity")
@@ -423,12 +433,15 @@ class ServerDone(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_longlong), ("queued", C.c_longlong), ("active", C.c_longlong),
                 ("done", C.c_longlong), ("steps", C.c_longlong), ("fo_blocks", C.c_longlong),
-                ("batch_builds", C.c_longlong), ("bytes_in_use", C.c_ulonglong), ("budget_bytes", C.c_ulonglong)]
+                ("batch_builds", C.c_longlong), ("bytes_in_use", C.c_ulonglong), ("budget_bytes", C.c_ulonglong),
+                ("t_admit_s", C.c_double), ("t_build_s", C.c_double), ("t_step_s", C.c_double), ("t_fo_s", C.c_double)]
 
 
 _sig("vh_server_config_default", None, [C.POINTER(ServerConfig)])
 _sig("vh_server_create", C.c_int, [C.POINTER(ServerConfig), C.c_void_p, C.c_int, C.POINTER(C.c_void_p)])
 _sig("vh_server_submit", C.c_int, [C.c_void_p, _cfgp, _dp, _dp, _dp, C.c_void_p, C.c_void_p, C.c_ulonglong])
+_sig("vh_server_submit_glauber", C.c_int, [C.c_void_p, _cfgp] + [C.c_double] * 7 + [C.c_ulonglong])
+_sig("vh_server_submit_hotspots", C.c_int, [C.c_void_p, _cfgp, C.c_ulonglong] + [C.c_double] * 6 + [C.c_ulonglong])
 _sig("vh_server_poll", C.c_int, [C.c_void_p, C.POINTER(ServerDone), C.c_int, C.POINTER(C.c_int)])
 _sig("vh_server_take_surface", C.c_int, [C.c_void_p, C.c_ulonglong, C.c_void_p, C.c_longlong,
                                          C.POINTER(C.c_longlong)])
@@ -458,6 +471,18 @@ class Server:
         check(lib.vh_server_submit(self.h, C.byref(cfg), np.ascontiguousarray(st.e), np.ascontiguousarray(st.p),
                                    np.ascontiguousarray(st.u).reshape(-1), _ptr(pi), _ptr(Pi), tag),
               "vh_server_submit")
+
+    def submit_glauber(self, cfg: VhConfig, tag: int, R=6.38, a=0.535, sigma_nn=4.2, b=7.0, e0=30.0,
+                       eta_flat=3.0, eta_sigma=1.3):
+        """an optical-Glauber event whose initial state is generated on the device at admission"""
+        check(lib.vh_server_submit_glauber(self.h, C.byref(cfg), R, a, sigma_nn, b, e0, eta_flat, eta_sigma, tag),
+              "vh_server_submit_glauber")
+
+    def submit_hotspots(self, cfg: VhConfig, tag: int, seed: int, mean_spots=200.0, w=0.4, k_gamma=1.6, amp=20.0,
+                        R=6.38, a=0.535):
+        """a hotspot event whose initial state is generated on the device at admission"""
+        check(lib.vh_server_submit_hotspots(self.h, C.byref(cfg), seed, mean_spots, w, k_gamma, amp, R, a, tag),
+              "vh_server_submit_hotspots")
 
     def poll(self, max_n: int = 1024) -> list:
         out = (ServerDone * max_n)()
@@ -489,13 +514,17 @@ class Server:
         self.close()
 
 
-def run_like_server(cfg: VhConfig, rows, st: InitialState, max_steps: int = 0):
+def run_like_server(cfg: VhConfig, rows, st, max_steps: int = 0):
     """One event alone with the server's cadence: freezeout blocks before loop
     index n when n % fo_factor == 0, retired after three blocks with no cell
-    above e_F, at max_steps, or when the device reports an error.
+    above e_F, at max_steps, or when the device reports an error.  st is an
+    InitialState or a callable that initialises the Event (a device generator).
     Returns (steps, surface, status)."""
     ev = Event(cfg, rows)
-    ev.set_initial(st)
+    if callable(st):
+        st(ev)
+    else:
+        ev.set_initial(st)
     fac = max(1, cfg.fo_factor)
     steps, last, zero, parts, status = 0, -1, 0, [], VH_OK
 

@@ -165,6 +165,17 @@ int vh_event_fetch_surface(vh_event *ev, double *host_out, int cap_elements, int
  * finalize phase kernels on large ones). */
 int vh_event_kernel_launches(vh_event *ev, int *per_step);
 
+/* Initial conditions generated on the device directly into the event (no
+ * host arrays), the same fields as vh_ic_glauber / vh_ic_hotspots followed by
+ * vh_event_set_initial (pi = 0, Pi = 0); the values may differ from the host
+ * generators' in the last bits (device exp).  Optical Glauber: the
+ * reference's thickness geometry (GlauberModel.cpp:26-108) and longitudinal
+ * plateau (InitialConditions.cpp:1046-1063); hotspots: 2+1D events only. */
+int vh_event_init_glauber(vh_event *ev, double R, double a, double sigma_nn, double b, double e0_GeV,
+                          double eta_flat, double eta_sigma);
+int vh_event_init_hotspots(vh_event *ev, unsigned long long seed, double mean_spots, double w, double k_gamma,
+                           double amp_mean_GeV, double R, double a);
+
 /* Thermal vorticity (calculateThermalVorticity, Vorticity.cpp:6-171, which
  * the reference runs after the initial condition and after every step,
  * HydroPlugin.cpp:197-199, :302-305).  Enabling computes it for the current
@@ -270,6 +281,10 @@ typedef struct vh_server_stats {
     long long fo_blocks;     /* freezeout blocks run     */
     long long batch_builds;  /* batches (re)built        */
     unsigned long long bytes_in_use, budget_bytes;
+    double t_admit_s;        /* worker wall time: creating and initialising events */
+    double t_build_s;        /*   (re)building and tuning batches                  */
+    double t_step_s;         /*   batch steps, launch to completion                */
+    double t_fo_s;           /*   freezeout blocks and surface copies              */
 } vh_server_stats;
 
 void vh_server_config_default(vh_server_config *c);
@@ -278,6 +293,13 @@ int vh_server_create(const vh_server_config *cfg, const double *eos_rows, int eo
  * returns at once. */
 int vh_server_submit(vh_server *s, const vh_config *cfg, const double *e, const double *p, const double *u,
                      const double *pi, const double *Pi, unsigned long long tag);
+/* The same with the initial condition generated on the device when the event
+ * is admitted (vh_event_init_glauber / vh_event_init_hotspots): nothing but
+ * the parameters crosses from the host. */
+int vh_server_submit_glauber(vh_server *s, const vh_config *cfg, double R, double a, double sigma_nn, double b,
+                             double e0_GeV, double eta_flat, double eta_sigma, unsigned long long tag);
+int vh_server_submit_hotspots(vh_server *s, const vh_config *cfg, unsigned long long seed, double mean_spots, double w,
+                              double k_gamma, double amp_mean_GeV, double R, double a, unsigned long long tag);
 /* Up to max finished events, oldest first. */
 int vh_server_poll(vh_server *s, vh_server_done *out, int max, int *n);
 /* The surface of a polled event (VH_FO_COLUMNS doubles per element); the

@@ -61,3 +61,31 @@ def test_server_reports_incompatible_events():
     with pytest.raises(vh.VhError):
         srv.wait(120)
     srv.close()
+
+
+def test_server_device_generated_events():
+    """events submitted as generator parameters (initial state made on the
+    device at admission) equal the same events run alone"""
+    rows = vh.synthetic_eos_table()
+    h = [vh.hotspot_config(n) for n in (29, 37)]
+    for c in h:
+        c.fo_factor = 5
+    g = vh.glauber_config(21, 19, 7)
+    g.dx = g.dy = 0.5
+    g.dz = 0.4
+    g.dt = 0.05
+    g.fo_factor = 4
+    srv = vh.Server(rows, max_steps=40)
+    srv.submit_hotspots(h[0], 0, seed=5)
+    srv.submit_hotspots(h[1], 1, seed=6)
+    srv.submit_glauber(g, 2, b=2.0)
+    srv.wait(300)
+    done = {d.tag: d for d in srv.poll()}
+    inits = [(h[0], lambda ev: ev.init_hotspots(seed=5)), (h[1], lambda ev: ev.init_hotspots(seed=6)),
+             (g, lambda ev: ev.init_glauber(b=2.0))]
+    for tag, (c, init) in enumerate(inits):
+        steps, ref, status = vh.run_like_server(c, rows, init, max_steps=40)
+        surf = srv.take_surface(tag)
+        assert done[tag].status == status == 0 and done[tag].steps == steps
+        assert surf.shape == ref.shape and np.array_equal(surf.view(np.uint64), ref.view(np.uint64))
+    srv.close()
