@@ -348,13 +348,19 @@ int autotune(vh_batch *b)
         if (rc != VH_OK) return rc;
     }
     launch_prep(b, 0);
-    const int rounds = 2;
+    /* a second timing round only where a stage is short enough for launch
+     * noise to matter (under 2 ms); large batches are timed once */
+    const int max_rounds = 2;
     const int ncand = kNumShapes * 2;
-    std::vector<vh::StageMarks> mk((size_t)rounds * ncand * 2);
+    std::vector<vh::StageMarks> mk((size_t)max_rounds * ncand * 2);
     for (auto &m : mk)
         for (cudaEvent_t &e : m.ev) BTRY(cudaEventCreate(&e));
+    double best[VH_NPHASES];
+    int best_c[VH_NPHASES];
+    for (int ph = 0; ph < VH_NPHASES; ++ph) { best[ph] = 1e30; best_c[ph] = 0; }
     size_t used = 0;
-    for (int r = 0; r < rounds; ++r)
+    for (int r = 0; r < max_rounds; ++r) {
+        const size_t first = used;
         for (int s = 0; s < kNumShapes; ++s)
             for (int p = 0; p < 2; ++p) {
                 vh_batch_tuning t{};
@@ -364,23 +370,21 @@ int autotune(vh_batch *b)
                 t.fused = 1;
                 launch_stage(b, 0, t, &mk[used++]);
             }
-    BTRY(cudaGetLastError());
-    BTRY(cudaStreamSynchronize(b->stream));
-    /* best[phase] over candidates: min over rounds */
-    double best[VH_NPHASES];
-    int best_c[VH_NPHASES];
-    for (int ph = 0; ph < VH_NPHASES; ++ph) { best[ph] = 1e30; best_c[ph] = 0; }
-    used = 0;
-    for (int r = 0; r < rounds; ++r)
+        BTRY(cudaGetLastError());
+        BTRY(cudaStreamSynchronize(b->stream));
+        /* best[phase] over candidates: min over rounds */
+        size_t k = first;
         for (int cnd = 0; cnd < ncand; ++cnd)
             for (int f = 0; f < 2; ++f) {
-                const vh::StageMarks &m = mk[used++];
+                const vh::StageMarks &m = mk[k++];
                 for (int n = 0; n < m.n; ++n) {
                     float ms = 0;
                     BTRY(cudaEventElapsedTime(&ms, m.ev[n], m.ev[n + 1]));
                     if (ms < best[m.phase[n]]) { best[m.phase[n]] = ms; best_c[m.phase[n]] = cnd; }
                 }
             }
+        if (best[VH_PHASE_FUSED] > 2.0) break;
+    }
     for (auto &m : mk)
         for (cudaEvent_t e : m.ev) cudaEventDestroy(e);
     double split = best[VH_PHASE_SOURCE] + best[VH_PHASE_FLUX_X] + best[VH_PHASE_FLUX_Y] + best[VH_PHASE_FINAL] +

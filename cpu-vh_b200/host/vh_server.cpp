@@ -144,6 +144,9 @@ void worker_main(vh_server *S)
     vh_batch *batch = nullptr;
     bool membership_changed = false;
     int held_rounds = 0;        /* rounds an admission waited for alignment */
+    /* pinned staging for surface copies (a pageable destination halves the copy rate) */
+    double *pin = nullptr;
+    size_t pin_cap = 0;
     auto tick = [] { return Clock::now(); };
     auto add = [&](double &acc, Clock::time_point a) {
         const double d = std::chrono::duration<double>(Clock::now() - a).count();
@@ -277,9 +280,20 @@ void worker_main(vh_server *S)
             int nel = 0, nab = 0;
             int rc = vh_event_freezeout_finish(j->ev, &nel, &nab);
             if (rc == VH_OK && nel > 0) {
+                const size_t need = (size_t)nel * VH_FO_COLUMNS;
+                if (need > pin_cap) {
+                    if (pin) cudaFreeHost(pin);
+                    pin_cap = std::max(need, 2 * pin_cap);
+                    if (cudaMallocHost(&pin, pin_cap * sizeof(double)) != cudaSuccess) { pin = nullptr; pin_cap = 0; }
+                }
                 const size_t off = j->surface.size();
-                j->surface.resize(off + (size_t)nel * VH_FO_COLUMNS);
-                rc = vh_event_fetch_surface(j->ev, j->surface.data() + off, nel, &nel);
+                j->surface.resize(off + need);
+                if (pin) {
+                    rc = vh_event_fetch_surface(j->ev, pin, nel, &nel);
+                    if (rc == VH_OK) std::copy(pin, pin + need, j->surface.data() + off);
+                } else {
+                    rc = vh_event_fetch_surface(j->ev, j->surface.data() + off, nel, &nel);
+                }
             }
             if (rc == VH_OK) rc = vh_event_status(j->ev, nullptr, nullptr);
             if (rc != VH_OK) { j->status = rc; continue; }
@@ -309,6 +323,7 @@ void worker_main(vh_server *S)
         }
     }
     if (batch) vh_batch_destroy(batch);
+    if (pin) cudaFreeHost(pin);
     for (auto &j : S->active)
         if (j->ev) vh_event_destroy(j->ev);
 }
