@@ -60,12 +60,13 @@ def phase_words(nq):
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
-# ncu capture kept in profiles/kt_stage_kernels_glauber_131x131x61.md
-NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 387.02e6, ("glauber_3p1d", "fp64", "source"): 336.17e6,
-               ("glauber_3p1d", "mixed", "flux"): 387.33e6, ("glauber_3p1d", "mixed", "source"): 322.01e6}
+# ncu captures kept in profiles/kt_stage_kernels_glauber_131x131x61.md and
+# profiles/kt_flux_face_kernel_glauber_131x131x61_mixed.md
+NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 385.30e6, ("glauber_3p1d", "fp64", "source"): 336.17e6,
+               ("glauber_3p1d", "mixed", "flux"): 388.30e6, ("glauber_3p1d", "mixed", "source"): 322.01e6}
 
 
-KERNEL_NAMES = {"source": "kt_source_kernel", "flux": "kt_flux_kernel (x, y, eta)",
+KERNEL_NAMES = {"source": "kt_source_kernel", "flux": "kt_flux_staged_kernel (x, y, eta)",
                 "final": "kt_final_kernel", "fused": "kt_stage_kernel"}
 
 
