@@ -741,6 +741,94 @@ __device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int 
     __syncthreads();
 }
 
+/* ---------------------------------------------------------------------
+ * Face-parallel stage for small lattices.  A single event of ~10^4 cells is
+ * latency-bound: one thread per cell carries the whole stage.  Here each cell
+ * gets 1 + 2 * ndir threads: thread 0 evaluates the source term, thread 1 +
+ * 2 (dir - 1) + f the face f (0 forward, 1 backward) of axis dir, all with the
+ * cell's e as the root solve's start; the face results go through shared
+ * memory and thread 0 combines them in flux_update's order -- r = (-H_fwd) +
+ * H_bwd per axis, the same operations as the one-thread stage, so the result
+ * is bit-identical (the backward face is accumulated onto -0.0, which leaves
+ * every value, signed zeros included, unchanged).
+ * --------------------------------------------------------------------- */
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2, bool MIXED>
+__device__ __forceinline__ void stage_faces_cell(const StageArgs &A, int i, int j, int k, bool valid,
+                                                 double *__restrict__ sm /* [2 ndir][NQ][TX] */, int TX)
+{
+    constexpr int ND = HAS_Z ? 3 : 2;
+    const int tx = threadIdx.x, role = threadIdx.y;
+    const long long sxy = (long long)A.ncx * A.ncy;
+    const long long s = i + (long long)A.ncx * j + sxy * k;
+    bool bad = false;
+    double acc[NQ];
+    if (valid && role > 0) {
+        const int dir = 1 + (role - 1) / 2;
+        const bool fwd = ((role - 1) % 2) == 0;
+        const long long st = (dir == 1) ? 1 : (dir == 2) ? (long long)A.ncx : sxy;
+        const double ePrev = __ldg(A.ein + s);
+        double r[NQ];
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) r[n] = -0.0;
+        if constexpr (MIXED) face_flux_m<NQ, EOS>(A, fwd ? s : s - st, st, dir, fwd, ePrev, r, bad);
+        else face_flux<NQ, EOS>(A, fwd ? s : s - st, st, dir, fwd, ePrev, r, bad);
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) sm[((role - 1) * NQ + n) * TX + tx] = r[n];
+    } else if (valid) {
+        if constexpr (MIXED) source_update_m<NQ, EOS>(A, s, acc);
+        else source_update<NQ, EOS>(A, s, acc);
+    }
+    __syncthreads();
+    if (valid && role == 0) {
+        const double ePrev = __ldg(A.ein + s);
+#pragma unroll 1
+        for (int dir = 1; dir <= ND; ++dir) {
+            const long long st = (dir == 1) ? 1 : (dir == 2) ? (long long)A.ncx : sxy;
+            const double d = (dir == 1) ? A.dx : (dir == 2) ? A.dy : A.dz;
+            const double yd = (dir == 1) ? A.inv_dx : (dir == 2) ? A.inv_dy : A.inv_dz;
+            const double *hf = sm + (2 * (dir - 1)) * NQ * TX, *hb = sm + (2 * (dir - 1) + 1) * NQ * TX;
+            double r[NQ];
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) r[n] = hf[n * TX + tx] + hb[n * TX + tx];
+            double S[4];
+            dir_sources<NQ>(A, s, st, d, dir, S);
+            if constexpr (MIXED) {
+#pragma unroll
+                for (int n = 0; n < 4; ++n) acc[n] += (r[n] * yd + S[n]) * A.dt;
+#pragma unroll
+                for (int n = 4; n < NQ; ++n) acc[n] += r[n] * yd * A.dt;
+            } else {
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) r[n] = div_rcp(r[n], d, yd);
+#pragma unroll
+                for (int n = 0; n < 4; ++n) { r[n] += S[n]; r[n] *= A.dt; }
+#pragma unroll
+                for (int n = 4; n < NQ; ++n) r[n] *= A.dt;
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) acc[n] += r[n];
+            }
+        }
+        if (!HAS_Z && !MIXED) {
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) acc[n] += 0.0;
+        }
+        if (STAGE2) {
+            if constexpr (MIXED) {
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) acc[n] = (acc[n] + __ldg(A.qbase + n * A.L + s)) * 0.5;
+            } else {
+#pragma unroll
+                for (int n = 0; n < NQ; ++n) { acc[n] += __ldg(A.qbase + n * A.L + s); acc[n] /= 2; }
+            }
+        }
+        Prim P = infer<EOS, true>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
+                                  (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
+        regulate<NQ>(A, acc, P, bad);
+        put_with_ghosts<NQ>(A, i, j, k, s, acc, P);
+    }
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+}
+
 /* launch-form independent selection of the per-cell bodies: MIXED picks the
  * mixed-precision source, flux and fused bodies; finalize is FP64 in both */
 template <int NQ, int EOS, bool MIXED>

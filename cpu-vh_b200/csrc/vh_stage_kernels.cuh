@@ -58,6 +58,32 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_kernel(const
     flux_phase<NQ, EOS, DIR, MIXED>(A, s);
 }
 
+/* face-parallel fused stage (small lattices): 32 cells of one row per block,
+ * 1 + 2 ndir threads per cell */
+constexpr int kFacesTX = 32;
+
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2, bool MIXED>
+__global__ void __launch_bounds__(kFacesTX * 7, 2) kt_stage_faces_kernel(const __grid_constant__ StageArgs A)
+{
+    constexpr int ND = HAS_Z ? 3 : 2;
+    __shared__ double sm[2 * ND * NQ * kFacesTX];
+    const int i = blockIdx.x * kFacesTX + threadIdx.x + 2;
+    const int j = blockIdx.y + 2;
+    const int k = blockIdx.z + 2;
+    stage_faces_cell<NQ, EOS, HAS_Z, STAGE2, MIXED>(A, i, j, k, i < A.nx + 2, sm, kFacesTX);
+}
+
+/* face-parallel (default) or one-thread-per-cell fused stage: VH_STAGE_FACES=0
+ * selects the latter */
+static inline bool stage_faces()
+{
+    static int on = [] {
+        const char *e = getenv("VH_STAGE_FACES");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return on == 1;
+}
+
 /* FP64 flux with the stencil tile staged in shared memory (cp.async): the
  * block's 32 x 4 cells and their 2-cell halo along DIR, all components */
 template <int NQ, int EOS, int DIR>
@@ -140,6 +166,16 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
         m->phase[m->n] = phase;
         cudaEventRecord(m->ev[++m->n], s);
     };
+    if (!use_split(a) && stage_faces()) {
+        const dim3 gf((a.nx + kFacesTX - 1) / kFacesTX, a.ny, a.nz);
+        const dim3 bf(kFacesTX, z ? 7 : 5, 1);
+        if (z && st2) kt_stage_faces_kernel<NQ, EOS, true, true, MIXED><<<gf, bf, 0, s>>>(a);
+        else if (z) kt_stage_faces_kernel<NQ, EOS, true, false, MIXED><<<gf, bf, 0, s>>>(a);
+        else if (st2) kt_stage_faces_kernel<NQ, EOS, false, true, MIXED><<<gf, bf, 0, s>>>(a);
+        else kt_stage_faces_kernel<NQ, EOS, false, false, MIXED><<<gf, bf, 0, s>>>(a);
+        mark(5);
+        return;
+    }
     if (!use_split(a)) {
         if (z && st2) kt_stage_kernel<NQ, EOS, true, true, MIXED><<<grid, block, 0, s>>>(a);
         else if (z) kt_stage_kernel<NQ, EOS, true, false, MIXED><<<grid, block, 0, s>>>(a);
