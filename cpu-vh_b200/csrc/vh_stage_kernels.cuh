@@ -140,10 +140,11 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_final_kernel(cons
     final_body<NQ, EOS, HAS_Z, STAGE2>(A, i, j, k, s);
 }
 
-/* Fused for small lattices (launch- and latency-bound: one wave of threads,
- * each carrying a whole stage), phase-split from 2^18 interior cells up
- * (measured on B200: 131x131x61 split 5.43 ms/step vs fused 6.82; 101x101x1
- * fused 0.120 ms vs split 0.163).  VH_STAGE_MODE=fused|split overrides. */
+/* Fused (face-parallel) for small lattices, which are latency-bound;
+ * phase-split from 2^15 interior cells up.  Measured on B200 (FP64, table EoS,
+ * ms/step fused vs split): 101^2 0.095 vs 0.253; 201^2 0.309 vs 0.285; 41^3
+ * 1.07 vs 0.62; 131x131x61 12.98 vs 5.18.  VH_STAGE_MODE=fused|split
+ * overrides. */
 static inline bool use_split(const StageArgs &a)
 {
     static int forced = [] {
@@ -151,7 +152,7 @@ static inline bool use_split(const StageArgs &a)
         return !e ? -1 : (e[0] == 'f' ? 0 : 1);
     }();
     if (forced >= 0) return forced == 1;
-    return (long long)a.nx * a.ny * a.nz >= (1LL << 18);
+    return (long long)a.nx * a.ny * a.nz >= (1LL << 15);
 }
 
 template <int NQ, int EOS, bool MIXED>

@@ -100,7 +100,7 @@ print("LAUNCHES", gpu.launches_per_step(), "BAD", bad)
                                  {"VH_STAGE_MODE": "fused", "VH_STAGE_FACES": "0"}],
                          ids=["split-staged", "split-global", "fused-faces", "fused-one-thread"])
 def test_large_lattice_forms_bitexact(env):
-    """above 2^18 cells the stage runs phase-split, its flux reading a
+    """above 2^15 cells the stage runs phase-split, its flux reading a
     shared-memory tile by default; below, fused with one thread per face; every
     form must equal the oracle bit for bit on the same lattice (run in a child
     process: the form is chosen once per process)"""

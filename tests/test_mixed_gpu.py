@@ -142,7 +142,7 @@ def test_batched_mixed_matches_single_mixed():
 
 
 def test_mixed_split_face_once_vs_fp64():
-    """a lattice above the fused/split threshold (2^18 cells): the mixed split
+    """a lattice above the fused/split threshold (2^15 cells): the mixed split
     stage evaluates each face once; after 20 steps its error against the FP64
     path must stay within 1e-4 relative L-infinity in e (the velocity, whose
     largest deviations sit in the dilute edge, within 1e-2)"""
