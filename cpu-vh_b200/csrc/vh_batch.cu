@@ -593,6 +593,15 @@ int vh_batch_step(vh_batch *b, int nsteps)
     int need = 0;
     for (vh_event *ev : b->mem) need = std::max(need, ev->n + nsteps + 1);
     if ((rc = ensure_times(b, need)) != VH_OK) return rc;
+    /* a member's dynamical sources may have been set or removed since */
+    bool changed = false;
+    for (size_t m = 0; m < b->mem.size(); ++m) {
+        const double *src = b->mem[m]->src_on ? b->mem[m]->src : nullptr;
+        if (b->h_mem[m].base.src != src) { b->h_mem[m].base.src = src; changed = true; }
+    }
+    if (changed)
+        BTRY(cudaMemcpyAsync(b->d_mem, b->h_mem.data(), b->h_mem.size() * sizeof(vh::BatchMember),
+                             cudaMemcpyHostToDevice, b->stream));
     if ((rc = upload_steps(b)) != VH_OK) return rc;
     if ((rc = join_members(b)) != VH_OK) return rc;
     if (!b->tuned && (rc = autotune(b)) != VH_OK) return rc;

@@ -82,6 +82,7 @@ vh::StageArgs vh::stage_args_base(const vh_event *ev)
     A.eos = dev_eos(ev);
     A.zeta.law = c.zeta_law; A.zeta.norm = c.zeta_norm; A.zeta.T0 = c.zeta_T0_GeV; A.zeta.w = c.zeta_width_GeV;
     A.err.code = ev->err; A.err.step = ev->err + 1; A.err.cell = ev->err_cell;
+    A.src = ev->src_on ? ev->src : nullptr;
     return A;
 }
 
@@ -111,6 +112,7 @@ int vh_event_destroy(vh_event *ev)
     cudaFree(ev->fo_elems);
     if (ev->fo_hdr) cudaFreeHost(ev->fo_hdr);
     cudaFree(ev->vort);
+    cudaFree(ev->src);
     if (ev->fo_done) cudaEventDestroy(ev->fo_done);
     for (auto &m : ev->marks)
         for (cudaEvent_t e : m.ev) cudaEventDestroy(e);
@@ -384,6 +386,29 @@ int vh_event_device_field(vh_event *ev, int field, double **d_ptr)
     const double *src = field_ptr(ev, field);
     if (!src) return fail(VH_ERR_ARG, "unknown field id");
     *d_ptr = const_cast<double *>(src);
+    return VH_OK;
+}
+
+int vh_event_set_sources(vh_event *ev, const double *st, const double *sx, const double *sy, const double *sn)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    if (!st) { ev->src_on = false; return VH_OK; }
+    if (!sx || !sy || !sn) return fail(VH_ERR_ARG, "all four source components are needed");
+    const size_t N = (size_t)ev->N, B = N * sizeof(double);
+    if (!ev->src) {
+        const size_t P = (size_t)4 * ev->L * sizeof(double);
+        CUDA_TRY(cudaMalloc(&ev->src, P));
+        CUDA_TRY(cudaMemsetAsync(ev->src, 0, P, ev->stream));
+    }
+    /* through the initial-condition staging planes (free between initial states) */
+    double *d = ev->ic;
+    CUDA_TRY(cudaMemcpyAsync(d, st, B, cudaMemcpyHostToDevice, ev->stream));
+    CUDA_TRY(cudaMemcpyAsync(d + N, sx, B, cudaMemcpyHostToDevice, ev->stream));
+    CUDA_TRY(cudaMemcpyAsync(d + 2 * N, sy, B, cudaMemcpyHostToDevice, ev->stream));
+    CUDA_TRY(cudaMemcpyAsync(d + 3 * N, sn, B, cudaMemcpyHostToDevice, ev->stream));
+    vh::launch_scatter_interior(d, ev->src, 4, ev->L, ev->cfg.nx, ev->cfg.ny, ev->cfg.nz, ev->ncx, ev->ncy, ev->stream);
+    CUDA_TRY(cudaGetLastError());
+    ev->src_on = true;
     return VH_OK;
 }
 

@@ -71,6 +71,9 @@ struct vh_event {
     /* thermal vorticity (vh_event_vorticity): 6 w planes then 4 beta planes */
     double *vort = nullptr;
     bool vort_on = false;
+    /* dynamical sources (vh_event_set_sources): 4 padded planes, ghosts 0 */
+    double *src = nullptr;
+    bool src_on = false;
     /* per-phase timing (vh_event_phase_timing) */
     bool timing = false;
     std::vector<vh::StageMarks> marks;    /* one per stage launched since enabling */

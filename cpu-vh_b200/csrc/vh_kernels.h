@@ -30,6 +30,7 @@ struct StageArgs {
     double dt, dx, dy, dz, theta, etabar, e_reg;
     double inv_dx, inv_dy, inv_dz;   /* RN(1/dx) etc. for div_rcp                      */
     double inv_t;          /* RN(1/t)                                                  */
+    const double *src;     /* dynamical sources t, x, y, eta (4 planes) or null        */
     int step;              /* step index for error reports                             */
     DevEos eos;
     Zeta zeta;
@@ -46,6 +47,9 @@ struct InitArgs {
 };
 
 void launch_init(const InitArgs &a, cudaStream_t s);
+/* interior arrays (nplanes x nx*ny*nz) -> the interior of padded planes */
+void launch_scatter_interior(const double *in, double *out, int nplanes, long long L, int nx, int ny, int nz,
+                             int ncx, int ncy, cudaStream_t s);
 
 /* Initial conditions on the device (vh_ic.cu) into interior planes e, p, u */
 struct GlauberArgs {

@@ -141,6 +141,27 @@ void launch_math_check(int which, const double *a, const double *b, int n, doubl
     math_check_kernel<<<(n + 255) / 256, 256, 0, s>>>(which, a, b, n, out, pq);
 }
 
+__global__ void scatter_interior_kernel(const double *in, double *out, int nplanes, long long L, int nx, int ny, int nz,
+                                        int ncx, int ncy)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;
+    const int k = blockIdx.z;
+    if (i >= nx || j >= ny) return;
+    const long long N = (long long)nx * ny * nz;
+    const long long m = i + (long long)nx * (j + (long long)ny * k);
+    const long long s = (i + 2) + (long long)ncx * ((j + 2) + (long long)ncy * (k + 2));
+    for (int c = 0; c < nplanes; ++c) out[c * L + s] = in[c * N + m];
+}
+
+void launch_scatter_interior(const double *in, double *out, int nplanes, long long L, int nx, int ny, int nz,
+                             int ncx, int ncy, cudaStream_t s)
+{
+    dim3 block(32, 4, 1);
+    dim3 grid((nx + 31) / 32, (ny + 3) / 4, nz);
+    scatter_interior_kernel<<<grid, block, 0, s>>>(in, out, nplanes, L, nx, ny, nz, ncx, ncy);
+}
+
 void launch_init(const InitArgs &a, cudaStream_t s)
 {
     dim3 block(32, 4, 1);

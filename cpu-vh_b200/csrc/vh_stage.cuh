@@ -317,10 +317,14 @@ __device__ __forceinline__ void source_update(const StageArgs &A, long long s, d
     const double dnvn = div_rcp(dnun - vn * dnut, ut, yut);
     const double dkvk = dxvx + dyvy + dnvn;
     double S[NQ];
-    S[0] = 0.0 - (div_rcp(Qv[0], t, yt) + t * tnn) + dkvk * (Qv[4] - p - Pi) - vx * dxp - vy * dyp - vn * dnp;
-    S[1] = 0.0 - div_rcp(Qv[1], t, yt) - dxp + dkvk * Qv[5];
-    S[2] = 0.0 - div_rcp(Qv[2], t, yt) - dyp + dkvk * Qv[6];
-    S[3] = 0.0 - div_rcp(3 * Qv[3], t, yt) - dnp / A.t2pow + dkvk * Qv[7];
+    /* the dynamical sources, SourceTerms.cpp:584-587 (0 without them) */
+    const double *__restrict__ sv = A.src;
+    const double s0 = sv ? __ldg(sv + s) : 0.0, s1 = sv ? __ldg(sv + L + s) : 0.0;
+    const double s2 = sv ? __ldg(sv + 2 * L + s) : 0.0, s3 = sv ? __ldg(sv + 3 * L + s) : 0.0;
+    S[0] = s0 - (div_rcp(Qv[0], t, yt) + t * tnn) + dkvk * (Qv[4] - p - Pi) - vx * dxp - vy * dyp - vn * dnp;
+    S[1] = s1 - div_rcp(Qv[1], t, yt) - dxp + dkvk * Qv[5];
+    S[2] = s2 - div_rcp(Qv[2], t, yt) - dyp + dkvk * Qv[6];
+    S[3] = s3 - div_rcp(3 * Qv[3], t, yt) - dnp / A.t2pow + dkvk * Qv[7];
     pimunu_rhs<double, EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, e, p, ut, ux, uy, un,
                               __ldg(A.upin + s), __ldg(A.upin + L + s), __ldg(A.upin + 2 * L + s), __ldg(A.upin + 3 * L + s),
                               Qv + 4, Pi, dxut, dyut, dnut, dxux, dyux, dnux, dxuy, dyuy, dnuy, dxun, dyun, dnun, dkvk,
@@ -577,10 +581,13 @@ __device__ __forceinline__ void source_update_m(const StageArgs &A, long long s,
     const float vx = ux * yut, vy = uy * yut, vn = un * yut;
     const float dkvk = (dxux - vx * dxut) * yut + (dyuy - vy * dyut) * yut + (dnun - vn * dnut) * yut;
     float S[NQ];
-    S[0] = -((float)Qv[0] * yt + t * tnn) + dkvk * ((float)Qv[4] - (float)p - Pi) - vx * dxp - vy * dyp - vn * dnp;
-    S[1] = -(float)Qv[1] * yt - dxp + dkvk * (float)Qv[5];
-    S[2] = -(float)Qv[2] * yt - dyp + dkvk * (float)Qv[6];
-    S[3] = -3.f * (float)Qv[3] * yt - dnp / (float)A.t2pow + dkvk * (float)Qv[7];
+    const double *__restrict__ sv = A.src;
+    const float s0 = sv ? (float)__ldg(sv + s) : 0.f, s1 = sv ? (float)__ldg(sv + L + s) : 0.f;
+    const float s2 = sv ? (float)__ldg(sv + 2 * L + s) : 0.f, s3 = sv ? (float)__ldg(sv + 3 * L + s) : 0.f;
+    S[0] = s0 - ((float)Qv[0] * yt + t * tnn) + dkvk * ((float)Qv[4] - (float)p - Pi) - vx * dxp - vy * dyp - vn * dnp;
+    S[1] = s1 - (float)Qv[1] * yt - dxp + dkvk * (float)Qv[5];
+    S[2] = s2 - (float)Qv[2] * yt - dyp + dkvk * (float)Qv[6];
+    S[3] = s3 - 3.f * (float)Qv[3] * yt - dnp / (float)A.t2pow + dkvk * (float)Qv[7];
     float pvf[10];
 #pragma unroll
     for (int n = 0; n < 10; ++n) pvf[n] = (float)Qv[4 + n];

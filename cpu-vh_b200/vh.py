@@ -100,6 +100,7 @@ _sig("vh_event_stream", C.c_int, [_evp, C.POINTER(C.c_void_p)])
 _sig("vh_event_kernel_launches", C.c_int, [_evp, C.POINTER(C.c_int)])
 _sig("vh_event_phase_timing", C.c_int, [_evp, C.c_int])
 _sig("vh_event_vorticity", C.c_int, [_evp, C.c_int])
+_sig("vh_event_set_sources", C.c_int, [_evp] + [C.c_void_p] * 4)
 _sig("vh_event_init_glauber", C.c_int, [_evp] + [C.c_double] * 7)
 _sig("vh_event_init_hotspots", C.c_int, [_evp, C.c_ulonglong] + [C.c_double] * 6)
 _sig("vh_event_phase_times", C.c_int, [_evp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)])
@@ -317,6 +318,14 @@ class Event:
     def init_hotspots(self, seed: int, mean_spots=200.0, w=0.4, k_gamma=1.6, amp=20.0, R=6.38, a=0.535):
         """hotspot initial state generated on the device (see hotspot_ic)"""
         check(lib.vh_event_init_hotspots(self.h, seed, mean_spots, w, k_gamma, amp, R, a), "vh_event_init_hotspots")
+
+    def set_sources(self, src) -> None:
+        """dynamical sources: (4, N) interior array (t, x, y, eta components) or None"""
+        if src is None:
+            check(lib.vh_event_set_sources(self.h, None, None, None, None), "vh_event_set_sources")
+            return
+        self._src = np.ascontiguousarray(src, dtype=np.float64)
+        check(lib.vh_event_set_sources(self.h, *[_ptr(self._src[c]) for c in range(4)]), "vh_event_set_sources")
 
     def vorticity(self, enable: bool = True) -> None:
         """thermal vorticity now and after every step (fields VH_F_W.., VH_F_BETA..)"""

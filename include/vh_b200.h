@@ -176,6 +176,14 @@ int vh_event_init_glauber(vh_event *ev, double R, double a, double sigma_nn, dou
 int vh_event_init_hotspots(vh_event *ev, unsigned long long seed, double mean_spots, double w, double k_gamma,
                            double amp_mean_GeV, double R, double a);
 
+/* Dynamical sources J^mu of the energy-momentum equations (the reference's
+ * Source arrays, SourceTerms.cpp:584-587, filled from HDF5 files by
+ * DynamicalSources.cpp for jet sources): interior arrays of the t, x, y, eta
+ * components, nx*ny*nz values each, used by every following step until
+ * replaced; st == NULL removes them.  A batch picks up a member's sources at
+ * its next vh_batch_step. */
+int vh_event_set_sources(vh_event *ev, const double *st, const double *sx, const double *sy, const double *sn);
+
 /* Thermal vorticity (calculateThermalVorticity, Vorticity.cpp:6-171, which
  * the reference runs after the initial condition and after every step,
  * HydroPlugin.cpp:197-199, :302-305).  Enabling computes it for the current

@@ -71,6 +71,7 @@ def oracle_lib():
         L.vho_get.argtypes = [C.c_void_p, C.c_int, _dp]
         L.vho_destroy.argtypes = [C.c_void_p]
         L.vho_vorticity.argtypes = [C.c_void_p]
+        L.vho_set_sources.argtypes = [C.c_void_p] + [C.c_void_p] * 4
         for f in ("vho_eos_p", "vho_eos_T", "vho_eos_cs2", "vho_eos_e"):
             getattr(L, f).argtypes = [C.c_void_p, C.c_double]
             getattr(L, f).restype = C.c_double
@@ -117,6 +118,14 @@ class OracleEvent:
     def vorticity(self):
         """thermal vorticity and velocity of the current state (fields 300+, 310+)"""
         self.L.vho_vorticity(self.h)
+
+    def set_sources(self, src):
+        """dynamical sources: (4, N) interior array (t, x, y, eta) or None"""
+        if src is None:
+            self.L.vho_set_sources(self.h, None, None, None, None)
+            return
+        self._src = np.ascontiguousarray(src, dtype=np.float64)
+        self.L.vho_set_sources(self.h, *[_p(self._src[c]) for c in range(4)])
 
     def field(self, fid):
         ncx, ncy, ncz = self.cfg.nx + 4, self.cfg.ny + 4, self.cfg.nz + 4
@@ -195,6 +204,11 @@ class RefEvent:
     def vorticity(self):
         with _stdout_to_stderr():
             self.L.vhref_vorticity()
+
+    def set_sources(self, src):
+        self._src = np.ascontiguousarray(src, dtype=np.float64)
+        self.L.vhref_set_sources.argtypes = [_dp] * 4
+        self.L.vhref_set_sources(*[np.ascontiguousarray(self._src[c]) for c in range(4)])
 
     def time_steps(self, n):
         with _stdout_to_stderr():

@@ -351,6 +351,12 @@ void vhref_init(void)
         allocateHostMemory(len);
         g_allocated = len;
     }
+    /* no dynamical sources unless vhref_set_sources gives them (the arrays
+     * outlive an event in this process) */
+    memset(Source->sourcet, 0, sizeof(double) * (size_t)len);
+    memset(Source->sourcex, 0, sizeof(double) * (size_t)len);
+    memset(Source->sourcey, 0, sizeof(double) * (size_t)len);
+    memset(Source->sourcen, 0, sizeof(double) * (size_t)len);
     inject_ic();
     g_n = 0;
     g_t = g_hydro.initialProperTimePoint;
@@ -416,6 +422,24 @@ int vhref_get(int which, double *out)
     if (!src) return -1;
     memcpy(out, src, sizeof(double) * (size_t)len);
     return 0;
+}
+
+/* Fills the reference's dynamical source arrays (Source->sourcet..sourcen,
+ * SourceTerms.cpp:584-587) from interior arrays; the ghost cells stay 0. */
+void vhref_set_sources(const double *st, const double *sx, const double *sy, const double *sn)
+{
+    int nx = g_lat.numLatticePointsX, ny = g_lat.numLatticePointsY, nz = g_lat.numLatticePointsRapidity;
+    int ncx = nx + 4, ncy = ny + 4;
+    for (int k = 0; k < nz; ++k)
+        for (int j = 0; j < ny; ++j)
+            for (int i = 0; i < nx; ++i) {
+                int s = (i + 2) + ncx * ((j + 2) + ncy * (k + 2));
+                size_t m = i + (size_t)nx * (j + (size_t)ny * k);
+                Source->sourcet[s] = st[m];
+                Source->sourcex[s] = sx[m];
+                Source->sourcey[s] = sy[m];
+                Source->sourcen[s] = sn[m];
+            }
 }
 
 /* The thermal vorticity as the driver computes it after the initial

@@ -49,6 +49,8 @@ typedef struct {
     int fo_prev;
     /* thermal vorticity (allocated by the first vho_vorticity): wtx wty wtn wxy wxn wyn, beta t x y n */
     double *w[6], *beta[4];
+    /* dynamical sources (vho_set_sources): t, x, y, eta components, padded; NULL when none */
+    double *src[4];
 } vho_t;
 
 /* ------------------------------------------------------------------ EoS */
@@ -372,7 +374,7 @@ static void pimunu_sources(const vho_t *h, double *rhs, double t, double e, doub
 }
 
 /* SourceTerms.cpp:421-612 (USE_APPROX_DERIVATIVE branch, no Cartesian override;
- * the dynamical source arrays are identically zero, DynamicalVariables.cpp:47-52). */
+ * the dynamical source arrays are zero unless vho_set_sources gave them). */
 static void sources2(const vho_t *h, const double *Qv, double *S, double **uu,
                      double utp, double uxp, double uyp, double unp, double t, double e, const double *pvec, int s)
 {
@@ -408,10 +410,12 @@ static void sources2(const vho_t *h, const double *Qv, double *S, double **uu,
     double dnvn = (dnun - vn * dnut) / ut;
     double dkvk = dxvx + dyvy + dnvn;
     double t2pow = pow(t, 2);
-    S[0] = 0.0 - (ttt / t + t * tnn) + dkvk * (pitt - p - Pi) - vx * dxp - vy * dyp - vn * dnp;
-    S[1] = 0.0 - ttx / t - dxp + dkvk * pitx;
-    S[2] = 0.0 - tty / t - dyp + dkvk * pity;
-    S[3] = 0.0 - 3 * ttn / t - dnp / t2pow + dkvk * pitn;
+    const double s0 = h->src[0] ? h->src[0][s] : 0.0, s1 = h->src[0] ? h->src[1][s] : 0.0;
+    const double s2 = h->src[0] ? h->src[2][s] : 0.0, s3 = h->src[0] ? h->src[3][s] : 0.0;
+    S[0] = s0 - (ttt / t + t * tnn) + dkvk * (pitt - p - Pi) - vx * dxp - vy * dyp - vn * dnp;
+    S[1] = s1 - ttx / t - dxp + dkvk * pitx;
+    S[2] = s2 - tty / t - dyp + dkvk * pity;
+    S[3] = s3 - 3 * ttn / t - dnp / t2pow + dkvk * pitn;
     double rhs[11];
     pimunu_sources(h, rhs, t, e, p, ut, ux, uy, un, utp, uxp, uyp, unp,
                    pitt, pitx, pity, pitn, pixx, pixy, pixn, piyy, piyn, pinn, Pi,
@@ -701,6 +705,25 @@ int vho_step(vho_t *h, int nsteps)
     return h->nan_flag;
 }
 
+/* Dynamical sources (the Source arrays of SourceTerms.cpp:584-587): interior
+ * arrays t, x, y, eta of nx*ny*nz values each; st == NULL removes them. */
+void vho_set_sources(vho_t *h, const double *st, const double *sx, const double *sy, const double *sn)
+{
+    size_t len = (size_t)h->ncx * h->ncy * h->ncz;
+    if (!st) {
+        for (int c = 0; c < 4; ++c) { free(h->src[c]); h->src[c] = NULL; }
+        return;
+    }
+    const double *in[4] = {st, sx, sy, sn};
+    for (int c = 0; c < 4; ++c) {
+        if (!h->src[c]) h->src[c] = (double *)calloc(len, 8);
+        for (int k = 0; k < h->nz; ++k)
+            for (int j = 0; j < h->ny; ++j)
+                for (int i = 0; i < h->nx; ++i)
+                    h->src[c][IDX(h, i + 2, j + 2, k + 2)] = in[c][i + (size_t)h->nx * (j + (size_t)h->ny * k)];
+    }
+}
+
 /* Vorticity.cpp:6-171: thermal velocity beta_mu = u_mu / T and the thermal
  * vorticity w_{mu nu} = -(d_mu beta_nu - d_nu beta_mu) / 2 with a backward
  * time difference (u against the previous step's up, both divided by the
@@ -773,6 +796,7 @@ void vho_destroy(vho_t *h)
     for (int c = 0; c < 4; ++c) { free(h->u[c]); free(h->up[c]); free(h->uS[c]); }
     for (int s = 0; s < 2; ++s) free(h->slab[s]);
     for (int c = 0; c < 6; ++c) free(h->w[c]);
+    for (int c = 0; c < 4; ++c) free(h->src[c]);
     for (int c = 0; c < 4; ++c) free(h->beta[c]);
     free(h->p_tb); free(h->T_tb);
     free(h);

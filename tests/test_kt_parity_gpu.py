@@ -145,3 +145,41 @@ def test_thermal_vorticity_bitexact(case):
             a, b = vh.interior(cfg, gpu.field(f)), vh.interior(cfg, orc.field(f))
             assert np.count_nonzero(np.ascontiguousarray(a).view(np.uint64) !=
                                     np.ascontiguousarray(b).view(np.uint64)) == 0, (case, n, f)
+
+
+@pytest.mark.parametrize("case", ["gubser", "glauber", "glauber-split"])
+def test_dynamical_sources_bitexact(case):
+    """dynamical sources entering the evolution: single event (fused and
+    split lattices) and batch members equal the oracle bit for bit"""
+    if case == "gubser":
+        cfg, rows = vh.gubser_config(41, 37), None
+        st = vh.gubser_ic(cfg)
+    else:
+        cfg = vh.glauber_config(27, 25, 9) if case == "glauber" else vh.glauber_config(41, 39, 21)
+        cfg.dx = cfg.dy = 0.5
+        cfg.dz = 0.4
+        cfg.dt = 0.05
+        rows = vh.synthetic_eos_table()
+        st = vh.glauber_ic(cfg, rows)
+    N = cfg.nx * cfg.ny * cfg.nz
+    rng = np.random.default_rng(9)
+    src = rng.normal(0.0, 0.5, size=(4, N)) * np.abs(st.e)[None, :] / (1.0 + np.abs(st.e).max())
+    gpu, orc = vh.Event(cfg, rows), OracleEvent(cfg, rows)
+    gpu.set_initial(st)
+    orc.set_initial(st)
+    gpu.set_sources(src)
+    orc.set_sources(src)
+    gpu.step(3)
+    assert orc.step(3) == 0
+    gpu.sync()
+    fields = FIELDS_15 if cfg.bulk else FIELDS_14
+    bad = _compare(cfg, gpu, orc, fields)
+    assert not bad, bad
+    # the same through a batch, sources set after the batch was built
+    mem = vh.Event(cfg, rows)
+    mem.set_initial(st)
+    b = vh.Batch([mem])
+    mem.set_sources(src)
+    b.step(3)
+    mem.sync()
+    assert not _compare(cfg, mem, orc, fields)

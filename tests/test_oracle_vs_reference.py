@@ -159,3 +159,24 @@ def test_vorticity_bitexact_vs_reference(case, variant):
             a, b = vh.interior(cfg, ref.field(f)), vh.interior(cfg, orc.field(f))
             assert np.count_nonzero(a.view(np.uint64) != b.view(np.uint64)) == 0, (case, n, f)
         assert np.any(orc.field(303) != 0) or n == 0
+
+
+@pytest.mark.parametrize("case,variant", [("gubser", "conf"), ("glauber", "table")])
+def test_dynamical_sources_bitexact_vs_reference(case, variant):
+    """the Source arrays (SourceTerms.cpp:584-587) entering the evolution"""
+    if not O.ref_available(variant):
+        pytest.skip("reference build not present")
+    cfg, rows, st = CASES[case]()
+    N = cfg.nx * cfg.ny * cfg.nz
+    rng = np.random.default_rng(5)
+    src = rng.normal(0.0, 0.5, size=(4, N)) * np.abs(st.e)[None, :] / (1.0 + np.abs(st.e).max())
+    ref = O.RefEvent(variant, cfg, rows, threads=1)
+    orc = O.OracleEvent(cfg, rows)
+    ref.set_initial(st)
+    orc.set_initial(st)
+    ref.set_sources(src)
+    orc.set_sources(src)
+    ref.step(4)
+    assert orc.step(4) == 0
+    for f in FIELDS(orc.nq):
+        assert _same(cfg, ref.field(f), orc.field(f)) == 0, (case, f)
