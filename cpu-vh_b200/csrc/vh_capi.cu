@@ -83,6 +83,7 @@ vh::StageArgs vh::stage_args_base(const vh_event *ev)
     A.zeta.law = c.zeta_law; A.zeta.norm = c.zeta_norm; A.zeta.T0 = c.zeta_T0_GeV; A.zeta.w = c.zeta_width_GeV;
     A.err.code = ev->err; A.err.step = ev->err + 1; A.err.cell = ev->err_cell;
     A.src = ev->src_on ? ev->src : nullptr;
+    A.regfac = ev->regfac_on ? ev->regfac : nullptr;
     return A;
 }
 
@@ -113,6 +114,7 @@ int vh_event_destroy(vh_event *ev)
     if (ev->fo_hdr) cudaFreeHost(ev->fo_hdr);
     cudaFree(ev->vort);
     cudaFree(ev->src);
+    cudaFree(ev->regfac);
     if (ev->fo_done) cudaEventDestroy(ev->fo_done);
     for (auto &m : ev->marks)
         for (cudaEvent_t e : m.ev) cudaEventDestroy(e);
@@ -366,6 +368,7 @@ static const double *field_ptr(const vh_event *ev, int field)
     if (field == VH_F_P) return ev->ep[ev->ec] + ev->L;
     if (ev->vort && field >= VH_F_W && field < VH_F_W + 6) return ev->vort + (long long)(field - VH_F_W) * ev->L;
     if (ev->vort && field >= VH_F_BETA && field < VH_F_BETA + 4) return ev->vort + (long long)(6 + field - VH_F_BETA) * ev->L;
+    if (ev->regfac && field >= VH_F_REGFAC && field < VH_F_REGFAC + 2) return ev->regfac + (long long)(field - VH_F_REGFAC) * ev->L;
     return nullptr;
 }
 
@@ -409,6 +412,18 @@ int vh_event_set_sources(vh_event *ev, const double *st, const double *sx, const
     vh::launch_scatter_interior(d, ev->src, 4, ev->L, ev->cfg.nx, ev->cfg.ny, ev->cfg.nz, ev->ncx, ev->ncy, ev->stream);
     CUDA_TRY(cudaGetLastError());
     ev->src_on = true;
+    return VH_OK;
+}
+
+int vh_event_keep_regulation(vh_event *ev, int enable)
+{
+    if (!ev) return fail(VH_ERR_ARG, "null event");
+    ev->regfac_on = enable != 0;
+    if (ev->regfac_on && !ev->regfac) {
+        const size_t P = (size_t)2 * ev->L * sizeof(double);
+        CUDA_TRY(cudaMalloc(&ev->regfac, P));
+        CUDA_TRY(cudaMemsetAsync(ev->regfac, 0, P, ev->stream));   /* as calloc'd before the first step */
+    }
     return VH_OK;
 }
 

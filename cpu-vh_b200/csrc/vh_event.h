@@ -74,6 +74,9 @@ struct vh_event {
     /* dynamical sources (vh_event_set_sources): 4 padded planes, ghosts 0 */
     double *src = nullptr;
     bool src_on = false;
+    /* regulation factors (vh_event_keep_regulation): shear, bulk planes */
+    double *regfac = nullptr;
+    bool regfac_on = false;
     /* per-phase timing (vh_event_phase_timing) */
     bool timing = false;
     std::vector<vh::StageMarks> marks;    /* one per stage launched since enabling */

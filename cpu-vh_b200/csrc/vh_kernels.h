@@ -31,6 +31,7 @@ struct StageArgs {
     double inv_dx, inv_dy, inv_dz;   /* RN(1/dx) etc. for div_rcp                      */
     double inv_t;          /* RN(1/t)                                                  */
     const double *src;     /* dynamical sources t, x, y, eta (4 planes) or null        */
+    double *regfac;        /* regulation factors shear, bulk (2 planes) or null        */
     int step;              /* step index for error reports                             */
     DevEos eos;
     Zeta zeta;

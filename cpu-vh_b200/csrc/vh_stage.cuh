@@ -337,9 +337,14 @@ __device__ __forceinline__ void source_update(const StageArgs &A, long long s, d
  * When e > e_reg both factors are exactly 1 and the reference's multiplies are
  * identities, so the block is skipped. */
 template <int NQ>
-__device__ __forceinline__ void regulate(const StageArgs &A, double *__restrict__ acc, const Prim &P, bool &bad)
+__device__ __forceinline__ void regulate(const StageArgs &A, double *__restrict__ acc, const Prim &P, bool &bad,
+                                         long long s)
 {
-    if (P.e > A.e_reg) return;
+    if (P.e > A.e_reg) {
+        /* regFacShear / regFacBulk of the reference (kept only when asked for) */
+        if (A.regfac) { A.regfac[s] = 1.0; if (NQ == 15) A.regfac[A.L + s] = 1.0; }
+        return;
+    }
     const double t = A.t_inf, t2 = t * t;
     const double pitt = acc[4], pitx = acc[5], pity = acc[6], pitn = acc[7], pixx = acc[8];
     const double pixy = acc[9], pixn = acc[10], piyy = acc[11], piyn = acc[12], pinn = acc[13];
@@ -366,12 +371,14 @@ __device__ __forceinline__ void regulate(const StageArgs &A, double *__restrict_
 #pragma unroll
     for (int n = 4; n < 14; ++n) acc[n] *= facShear;
     if (isnan(facShear)) bad = true;
+    if (A.regfac) A.regfac[s] = facShear;
     if (NQ == 15) {
         double rhoBulk = fabs(Pi) / P.p;
         double facBulk = vh_tanh(rhoBulk) / rhoBulk;
         if (fabs(rhoBulk) < 1.e-7) facBulk = 1.0;
         acc[14] *= facBulk;
         if (isnan(facBulk)) bad = true;
+        if (A.regfac) A.regfac[A.L + s] = facBulk;
     }
 }
 
@@ -426,7 +433,7 @@ __device__ __forceinline__ void stage_body(const StageArgs &A, int i, int j, int
     /* setInferredVariablesKernel (EnergyMomentumTensor.cpp:235-287) with ePrev = e[s] */
     Prim P = infer<EOS>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
                         (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
-    regulate<NQ>(A, acc, P, bad);
+    regulate<NQ>(A, acc, P, bad, s);
     if (bad) raise_error(A.err, kErrNan, s, A.step);
     put_with_ghosts<NQ>(A, i, j, k, s, acc, P);
 }
@@ -486,7 +493,7 @@ __device__ __forceinline__ void final_body(const StageArgs &A, int i, int j, int
     }
     Prim P = infer<EOS, true>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
                               (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
-    regulate<NQ>(A, acc, P, bad);
+    regulate<NQ>(A, acc, P, bad, s);
     if (bad) raise_error(A.err, kErrNan, s, A.step);
     put_with_ghosts<NQ>(A, i, j, k, s, acc, P);
 }
@@ -659,7 +666,7 @@ __device__ __forceinline__ void stage_body_m(const StageArgs &A, int i, int j, i
     }
     Prim P = infer<EOS>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
                         (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
-    regulate<NQ>(A, acc, P, bad);
+    regulate<NQ>(A, acc, P, bad, s);
     if (bad) raise_error(A.err, kErrNan, s, A.step);
     put_with_ghosts<NQ>(A, i, j, k, s, acc, P);
 }
@@ -830,7 +837,7 @@ __device__ __forceinline__ void stage_faces_cell(const StageArgs &A, int i, int 
         }
         Prim P = infer<EOS, true>(A.eos, A.t_inf, acc[0] - acc[4], acc[1] - acc[5], acc[2] - acc[6], acc[3] - acc[7],
                                   (NQ == 15) ? acc[14] : 0.0, ePrev, bad);
-        regulate<NQ>(A, acc, P, bad);
+        regulate<NQ>(A, acc, P, bad, s);
         put_with_ghosts<NQ>(A, i, j, k, s, acc, P);
     }
     if (bad) raise_error(A.err, kErrNan, s, A.step);

@@ -537,6 +537,8 @@ void run(void *latticeParams, void *initCondParams, void *hydroParams, const cha
     /* thermal vorticity after the initial condition and after every step
      * (THERMAL_VORTICITY is on in the reference, HydroPlugin.cpp:197-199, :302-305) */
     die_on(vh_event_vorticity(ev, 1), "vh_event_vorticity");
+    /* the regulation factors the reference dumps (regFacShear, regFacBulk) */
+    die_on(vh_event_keep_regulation(ev, 1), "vh_event_keep_regulation");
 
     SurfaceWriter surf(std::string(outputDir) + "/surface.dat");
     const int ncx = nx + 4, ncy = ny + 4, ncz = nz + 4;
@@ -561,7 +563,11 @@ void run(void *latticeParams, void *initCondParams, void *hydroParams, const cha
             dump_field(ev, 8, "pixx", t, outputDir, L);
             dump_field(ev, 9, "pixy", t, outputDir, L);
             dump_field(ev, 13, "pinn", t, outputDir, L);
-            if (cfg.bulk) dump_field(ev, 14, "Pi", t, outputDir, L);
+            dump_field(ev, VH_F_REGFAC, "regFacShear", t, outputDir, L);
+            if (cfg.bulk) {
+                dump_field(ev, 14, "Pi", t, outputDir, L);
+                dump_field(ev, VH_F_REGFAC + 1, "regFacBulk", t, outputDir, L);
+            }
             dump_field(ev, VH_F_W + 3, "wxy", t, outputDir, L);
             dump_field(ev, VH_F_BETA + 1, "beta_x", t, outputDir, L);
             dump_field(ev, VH_F_BETA + 2, "beta_y", t, outputDir, L);

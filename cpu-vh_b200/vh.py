@@ -37,7 +37,7 @@ VH_EOS_CONFORMAL, VH_EOS_TABLE = 0, 1
 VH_ZETA_REFERENCE, VH_ZETA_GAUSSIAN = 0, 1
 VH_PREC_FP64, VH_PREC_MIXED = 0, 1
 VH_F_UT, VH_F_UPT, VH_F_E, VH_F_P = 100, 110, 200, 201
-VH_F_W, VH_F_BETA = 300, 310
+VH_F_W, VH_F_BETA, VH_F_REGFAC = 300, 310, 400
 VH_FO_COLUMNS = 20
 PHASES = ("source", "flux_x", "flux_y", "flux_eta", "final", "fused")
 HBARC = 0.197326938
@@ -101,6 +101,7 @@ _sig("vh_event_kernel_launches", C.c_int, [_evp, C.POINTER(C.c_int)])
 _sig("vh_event_phase_timing", C.c_int, [_evp, C.c_int])
 _sig("vh_event_vorticity", C.c_int, [_evp, C.c_int])
 _sig("vh_event_set_sources", C.c_int, [_evp] + [C.c_void_p] * 4)
+_sig("vh_event_keep_regulation", C.c_int, [_evp, C.c_int])
 _sig("vh_event_init_glauber", C.c_int, [_evp] + [C.c_double] * 7)
 _sig("vh_event_init_hotspots", C.c_int, [_evp, C.c_ulonglong] + [C.c_double] * 6)
 _sig("vh_event_phase_times", C.c_int, [_evp, C.POINTER(C.c_double), C.POINTER(C.c_longlong)])
@@ -326,6 +327,10 @@ class Event:
             return
         self._src = np.ascontiguousarray(src, dtype=np.float64)
         check(lib.vh_event_set_sources(self.h, *[_ptr(self._src[c]) for c in range(4)]), "vh_event_set_sources")
+
+    def keep_regulation(self, enable: bool = True) -> None:
+        """keep the regulation factors of the last stage (fields VH_F_REGFAC, +1)"""
+        check(lib.vh_event_keep_regulation(self.h, 1 if enable else 0), "vh_event_keep_regulation")
 
     def vorticity(self, enable: bool = True) -> None:
         """thermal vorticity now and after every step (fields VH_F_W.., VH_F_BETA..)"""

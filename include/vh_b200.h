@@ -61,6 +61,7 @@ extern "C" {
 #define VH_F_P           201
 #define VH_F_W           300   /* 300..305: thermal vorticity w_tx w_ty w_tn w_xy w_xn w_yn (vh_event_vorticity) */
 #define VH_F_BETA        310   /* 310..313: thermal velocity beta_t beta_x beta_y beta_n = u_mu / T */
+#define VH_F_REGFAC      400   /* 400, 401: regulation factors regFacShear, regFacBulk (vh_event_keep_regulation) */
 
 /* columns of one freezeout element, the 20 columns of surface.dat
  * (FreezeOut.cpp:265-270): tau x y eta  ds0 ds1 ds2 ds3  ux uy un  e T P
@@ -183,6 +184,13 @@ int vh_event_init_hotspots(vh_event *ev, unsigned long long seed, double mean_sp
  * replaced; st == NULL removes them.  A batch picks up a member's sources at
  * its next vh_batch_step. */
 int vh_event_set_sources(vh_event *ev, const double *st, const double *sx, const double *sy, const double *sn);
+
+/* Keep the regulation factors (regFacShear, regFacBulk of
+ * regulateDissipativeCurrents, FullyDiscreteKurganovTadmorScheme.cpp:835-855:
+ * 1 where e > e_reg, tanh(rho)/rho below) of the last RK stage in the fields
+ * VH_F_REGFAC, VH_F_REGFAC + 1 (0 before the first step, as the reference's
+ * calloc'd arrays).  Off by default: it costs one plane write per stage. */
+int vh_event_keep_regulation(vh_event *ev, int enable);
 
 /* Thermal vorticity (calculateThermalVorticity, Vorticity.cpp:6-171, which
  * the reference runs after the initial condition and after every step,

@@ -419,6 +419,8 @@ int vhref_get(int which, double *out)
     else if (which == 311) src = beta_mu->beta_x;
     else if (which == 312) src = beta_mu->beta_y;
     else if (which == 313) src = beta_mu->beta_n;
+    else if (which == 400) src = regFacShear;
+    else if (which == 401) src = regFacBulk;
     if (!src) return -1;
     memcpy(out, src, sizeof(double) * (size_t)len);
     return 0;

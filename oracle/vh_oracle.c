@@ -51,6 +51,8 @@ typedef struct {
     double *w[6], *beta[4];
     /* dynamical sources (vho_set_sources): t, x, y, eta components, padded; NULL when none */
     double *src[4];
+    /* regulation factors of the last stage (regFacShear, regFacBulk), allocated by the first step */
+    double *regfac[2];
 } vho_t;
 
 /* ------------------------------------------------------------------ EoS */
@@ -527,6 +529,11 @@ static void set_inferred(vho_t *h, double **qq, double **uu, double t)
 /* FullyDiscreteKurganovTadmorScheme.cpp:690-859 (REG_SCHEME_1) */
 static void regulate(vho_t *h, double t, double **qq, double **uu)
 {
+    if (!h->regfac[0]) {
+        size_t len = (size_t)h->ncx * h->ncy * h->ncz;
+        h->regfac[0] = (double *)calloc(len, 8);
+        h->regfac[1] = (double *)calloc(len, 8);
+    }
     for (int k = 2; k < h->ncz - 2; ++k)
         for (int j = 2; j < h->ncy - 2; ++j)
             for (int i = 2; i < h->ncx - 2; ++i) {
@@ -560,8 +567,9 @@ static void regulate(vho_t *h, double t, double **qq, double **uu)
                 if (fabs(rhoBulk) < 1.e-7) facBulk = 1.0;
                 if (h->e[s] > h->e_reg) { facShear = 1.0; facBulk = 1.0; }
                 for (int n = 4; n < 14; ++n) qq[n][s] *= facShear;
+                h->regfac[0][s] = facShear;
                 if (isnan(facShear)) h->nan_flag = 1;
-                if (h->bulk) { qq[14][s] *= facBulk; if (isnan(facBulk)) h->nan_flag = 1; }
+                if (h->bulk) { qq[14][s] *= facBulk; h->regfac[1][s] = facBulk; if (isnan(facBulk)) h->nan_flag = 1; }
             }
 }
 
@@ -781,6 +789,10 @@ int vho_get(vho_t *h, int which, double *out)
     else if (which == 201) src = h->p;
     else if (which >= 300 && which < 306) src = h->w[which - 300];
     else if (which >= 310 && which < 314) src = h->beta[which - 310];
+    else if (which == 400 || which == 401) {
+        if (!h->regfac[0]) { memset(out, 0, 8 * len); return 0; }   /* before the first step */
+        src = h->regfac[which - 400];
+    }
     if (!src) return -1;
     memcpy(out, src, 8 * len);
     return 0;
@@ -797,6 +809,7 @@ void vho_destroy(vho_t *h)
     for (int s = 0; s < 2; ++s) free(h->slab[s]);
     for (int c = 0; c < 6; ++c) free(h->w[c]);
     for (int c = 0; c < 4; ++c) free(h->src[c]);
+    free(h->regfac[0]); free(h->regfac[1]);
     for (int c = 0; c < 4; ++c) free(h->beta[c]);
     free(h->p_tb); free(h->T_tb);
     free(h);

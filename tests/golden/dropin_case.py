@@ -6,7 +6,9 @@ vector, HydroWrapper.cpp:20-23).  The vector is a Gaussian blob,
 
 Run as a script where the reference build (oracle/_ref) exists to regenerate
 tests/golden/dropin_surface.json: row count and SHA-256 of the reference's
-surface.dat for this case (the text itself is ~600 kB and not committed)."""
+surface.dat for this case (the text itself is ~600 kB and not committed), and
+the SHA-256 of every field dump the reference's run() writes
+(outputDynamicalQuantities, HydroPlugin.cpp:40-71)."""
 import ctypes as C
 import hashlib
 import json
@@ -41,9 +43,15 @@ def main():
     lib.vhref_run_vector(out.encode(), e.ctypes.data, len(e))
     with open(os.path.join(out, "surface.dat"), "rb") as f:
         d = f.read()
+    dumps = {}
+    for name in sorted(os.listdir(out)):
+        if name != "surface.dat":
+            with open(os.path.join(out, name), "rb") as f:
+                dumps[name] = hashlib.sha256(f.read()).hexdigest()
     shutil.rmtree(out)
     with open(GOLDEN, "w") as f:
         json.dump({"rows": d.count(b"\n"), "sha256": hashlib.sha256(d).hexdigest(), "bytes": len(d),
+                   "dumps": dumps,
                    "source": "reference run(), stock macros, tests/golden/dropin_conf, IC type 13 "
                              "(tests/golden/dropin_case.py)"}, f, indent=1)
     print("wrote", GOLDEN)

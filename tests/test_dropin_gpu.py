@@ -3,9 +3,10 @@
 A reference maintainer's embedding code -- HYDRO::initialize_from_vector and
 run_hydro_no_cli, reading rhic-conf/ and writing cpu-vh_output/surface.dat
 (HydroWrapper.cpp:20-136, HydroPlugin.cpp:74-321) -- is compiled against this
-repository's header and run.  Its surface.dat must be byte-identical to the
-one the reference's own run() writes for the same case (golden hash from
-tests/golden/dropin_case.py): same rows, same order, same six-digit text."""
+repository's header and run.  Its surface.dat and its field dumps must be
+byte-identical to the ones the reference's own run() writes for the same case
+(golden hashes from tests/golden/dropin_case.py): same rows, same order, same
+text."""
 import hashlib
 import json
 import os
@@ -45,6 +46,11 @@ def test_dropin_surface_matches_reference(tmp_path):
         gold = json.load(f)
     assert data.count(b"\n") == gold["rows"]
     assert hashlib.sha256(data).hexdigest() == gold["sha256"]
+    # the field dumps of outputDynamicalQuantities (HydroPlugin.cpp:40-71), byte for byte
+    out = os.path.join(tmp, "cpu-vh_output")
+    mine = {n: hashlib.sha256(open(os.path.join(out, n), "rb").read()).hexdigest()
+            for n in os.listdir(out) if n != "surface.dat"}
+    assert mine == gold["dumps"]
 
 
 def test_cpu_vh_executable_runs_ideal_gubser(tmp_path):

@@ -183,3 +183,30 @@ def test_dynamical_sources_bitexact(case):
     b.step(3)
     mem.sync()
     assert not _compare(cfg, mem, orc, fields)
+
+
+@pytest.mark.parametrize("case", ["gubser", "glauber", "glauber-split"])
+def test_regulation_factors_bitexact(case):
+    """the kept regulation factors equal the oracle's (itself equal to the
+    reference's regFacShear / regFacBulk), fused and split forms"""
+    if case == "gubser":
+        cfg, rows = vh.gubser_config(41, 37), None
+        st = vh.gubser_ic(cfg)
+    else:
+        cfg = vh.glauber_config(27, 25, 9) if case == "glauber" else vh.glauber_config(41, 39, 21)
+        cfg.dx = cfg.dy = 0.5
+        cfg.dz = 0.4
+        cfg.dt = 0.05
+        rows = vh.synthetic_eos_table()
+        st = vh.glauber_ic(cfg, rows)
+    gpu, orc = vh.Event(cfg, rows), OracleEvent(cfg, rows)
+    gpu.set_initial(st)
+    orc.set_initial(st)
+    gpu.keep_regulation(True)
+    gpu.step(3)
+    assert orc.step(3) == 0
+    gpu.sync()
+    for f in ((400, 401) if cfg.bulk else (400,)):
+        a, b = vh.interior(cfg, gpu.field(f)), vh.interior(cfg, orc.field(f))
+        assert np.count_nonzero(np.ascontiguousarray(a).view(np.uint64) !=
+                                np.ascontiguousarray(b).view(np.uint64)) == 0, (case, f)

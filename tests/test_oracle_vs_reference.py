@@ -180,3 +180,20 @@ def test_dynamical_sources_bitexact_vs_reference(case, variant):
     assert orc.step(4) == 0
     for f in FIELDS(orc.nq):
         assert _same(cfg, ref.field(f), orc.field(f)) == 0, (case, f)
+
+
+@pytest.mark.parametrize("case,variant", [("gubser", "conf"), ("glauber", "table")])
+def test_regulation_factors_bitexact_vs_reference(case, variant):
+    """regFacShear / regFacBulk after steps (FullyDiscreteKurganovTadmorScheme.cpp:835-855)"""
+    if not O.ref_available(variant):
+        pytest.skip("reference build not present")
+    cfg, rows, st = CASES[case]()
+    ref = O.RefEvent(variant, cfg, rows, threads=1)
+    orc = O.OracleEvent(cfg, rows)
+    ref.set_initial(st)
+    orc.set_initial(st)
+    ref.step(3)
+    assert orc.step(3) == 0
+    for f in ((400, 401) if cfg.bulk else (400,)):
+        a, b = vh.interior(cfg, ref.field(f)), vh.interior(cfg, orc.field(f))
+        assert np.count_nonzero(a.view(np.uint64) != b.view(np.uint64)) == 0, (case, f)
