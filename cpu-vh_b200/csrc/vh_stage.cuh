@@ -722,10 +722,24 @@ __device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int 
     double H[NQ];
     if (face_ok) {
         face_H_m<NQ, EOS>(A, s - st, st, DIR, __ldg(A.ein + s), H, bad);
+        if constexpr (DIR != 1) {
 #pragma unroll
-        for (int n = 0; n < NQ; ++n) sm[n * (TX * TY) + tid] = H[n];
+            for (int n = 0; n < NQ; ++n) sm[n * (TX * TY) + tid] = H[n];
+        }
+    } else {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) H[n] = 0.0;
     }
-    __syncthreads();
+    /* along x a row of faces is one warp: the next face comes by shuffle, no
+     * block barrier; along y and eta it comes through shared memory */
+    double Hn[NQ];
+    if constexpr (DIR == 1) {
+        static_assert(TX == 32, "a row of x faces is one warp");
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) Hn[n] = __shfl_down_sync(0xffffffffu, H[n], 1);
+    } else {
+        __syncthreads();
+    }
     const bool last = (DIR == 1) ? (tx == TX - 1) : (ty == TY - 1);
     if (face_ok && !last && along <= n_along + 1) {
         const int nxt = (DIR == 1) ? tid + 1 : tid + TX;
@@ -740,7 +754,7 @@ __device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int 
             for (int n = 0; n < NQ; ++n) r[n] = H[n] - F[n];
         } else {
 #pragma unroll
-            for (int n = 0; n < NQ; ++n) r[n] = H[n] - sm[n * (TX * TY) + nxt];
+            for (int n = 0; n < NQ; ++n) r[n] = H[n] - ((DIR == 1) ? Hn[n] : sm[n * (TX * TY) + nxt]);
         }
         double S[4];
         dir_sources<NQ>(A, s, st, d, DIR, S);
@@ -752,7 +766,7 @@ __device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int 
         for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] += r[n];
     }
     if (bad) raise_error(A.err, kErrNan, s, A.step);
-    __syncthreads();
+    if constexpr (DIR != 1) __syncthreads();
 }
 
 /* ---------------------------------------------------------------------
