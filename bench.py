@@ -62,7 +62,7 @@ def phase_words(nq):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
 # ncu captures kept in profiles/kt_stage_kernels_glauber_131x131x61.md and
 # profiles/kt_flux_face_kernel_glauber_131x131x61_mixed.md
-NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 385.30e6, ("glauber_3p1d", "fp64", "source"): 336.17e6,
+NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 387.00e6, ("glauber_3p1d", "fp64", "source"): 336.17e6,
                ("glauber_3p1d", "mixed", "flux"): 388.30e6, ("glauber_3p1d", "mixed", "source"): 322.01e6}
 
 
@@ -213,6 +213,7 @@ def run_serve(args, rank):
     mixed = args.precision == "mixed"
     prec = vh.VH_PREC_MIXED if mixed else vh.VH_PREC_FP64
     srv = vh.Server(rows, hbm_fraction=0.8, max_steps=args.max_steps)
+    solo_cells = srv.solo_cells
     # warm the server (tuning, modules) on one small event outside the timed stream
     wc = vh.hotspot_config(61).copy(precision=prec)
     srv.submit(wc, vh.hotspot_ic(wc, rows, seed=1), 1 << 40)
@@ -259,7 +260,8 @@ def run_serve(args, rank):
             "steps": None, "warmup": 1, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32/f64 mixed" if mixed else "f64", "data": "synthetic",
             "config": {"workload": desc, "events": len(stream), "max_steps": args.max_steps,
-                       "admission": "80% of free HBM", "precision": args.precision},
+                       "admission": "80% of free HBM", "precision": args.precision,
+                       "solo_cells": solo_cells},
             "latency_s": {"p50": pct(lat, 50), "p95": pct(lat, 95), "p99": pct(lat, 99), "max": max(lat)},
             "cell_updates_per_s": cells / span,
             "server": {k: stats[k] for k in ("steps", "fo_blocks", "batch_builds", "t_admit_s", "t_build_s",

@@ -9,9 +9,12 @@
  *           memory budget (a fraction of the free HBM when the server
  *           started); each becomes a vh_event with its state on the device
  *           until it is done;
- *   batch   every active event advanced together by one vh_batch (rebuilt
- *           when the active set changes; launch configuration tuned once per
- *           kind of batch and reused);
+ *   step    the active events advanced concurrently: events below
+ *           solo_cells interior cells in one vh_batch per kind (precision,
+ *           bulk, EoS; rebuilt when its members change, launch configuration
+ *           tuned once per kind of batch and reused), larger events -- which
+ *           fill the GPU on their own and run faster with the single-event
+ *           kernels -- by vh_event_step on their own streams;
  *   freeze  the freezeout blocks of all events queued first, then collected,
  *           at the reference's cadence (a block before loop index n when
  *           n % coarseProperTimeFOFactor == 0, HydroPlugin.cpp:249-266); the
@@ -103,14 +106,27 @@ struct vh_server {
 
 namespace {
 
-int batch_kind(const std::vector<std::unique_ptr<Job>> &act)
+/* events a vh_batch may hold together (vh_batch_create's requirement) */
+int group_key(const vh_config &c) { return (c.bulk ? 1 : 0) + 2 * c.eos_kind + 4 * c.precision; }
+
+/* the tuning cache key: the group and whether its members are 2+1D, 3+1D or both */
+int batch_kind(const std::vector<Job *> &members)
 {
     bool any3 = false, any2 = false;
-    for (auto &j : act) (j->cfg.nz > 1 ? any3 : any2) = true;
+    for (Job *j : members) (j->cfg.nz > 1 ? any3 : any2) = true;
     const int z = any3 && any2 ? 2 : (any3 ? 1 : 0);
-    const vh_config &c = act.front()->cfg;
-    return z + 3 * (c.bulk ? 1 : 0) + 6 * c.eos_kind + 12 * c.precision;
+    return z + 3 * group_key(members.front()->cfg);
 }
+
+bool is_solo(const vh_server_config &sc, const vh_config &c)
+{
+    return sc.solo_cells > 0 && (long long)c.nx * c.ny * c.nz >= sc.solo_cells;
+}
+
+struct Group {
+    vh_batch *batch = nullptr;
+    std::vector<vh_event *> members;      /* the batch's events, in order */
+};
 
 /* steps until the next freezeout block of member j (the block happens
  * before loop index n = steps + 1 when n % fac == 0) */
@@ -141,8 +157,7 @@ void finish_job(vh_server *S, std::unique_ptr<Job> &j, int status)
 void worker_main(vh_server *S)
 {
     cudaSetDevice(S->device);
-    vh_batch *batch = nullptr;
-    bool membership_changed = false;
+    std::map<int, Group> groups;    /* batches by group_key */
     int held_rounds = 0;        /* rounds an admission waited for alignment */
     /* pinned staging for surface copies (a pageable destination halves the copy rate) */
     double *pin = nullptr;
@@ -212,36 +227,51 @@ void worker_main(vh_server *S)
             std::vector<double>().swap(j->Pi);
             if (rc != VH_OK) { finish_job(S, j, rc); continue; }
             S->active.push_back(std::move(j));
-            membership_changed = true;
         }
         if (!admitted.empty()) add(S->st.t_admit_s, t_adm);
         if (S->active.empty()) continue;
 
-        /* ---- batch (rebuilt when members changed) */
+        /* ---- batches of the small events, one per kind (rebuilt when their
+         * members changed), and the solo events */
         const auto t_bld = tick();
-        if (membership_changed || !batch) {
-            if (batch) vh_batch_destroy(batch);
-            batch = nullptr;
+        std::map<int, std::vector<Job *>> want;
+        std::vector<Job *> solo;
+        for (auto &j : S->active) {
+            if (is_solo(S->cfg, j->cfg)) solo.push_back(j.get());
+            else want[group_key(j->cfg)].push_back(j.get());
+        }
+        for (auto it = groups.begin(); it != groups.end();) {
+            if (want.count(it->first)) { ++it; continue; }
+            vh_batch_destroy(it->second.batch);
+            it = groups.erase(it);
+        }
+        int brc = VH_OK;
+        const char *bwhere = "";
+        bool built = false;
+        for (auto &kv : want) {
             std::vector<vh_event *> evs;
-            for (auto &j : S->active) evs.push_back(j->ev);
-            int rc = vh_batch_create(evs.data(), (int)evs.size(), &batch);
-            if (rc != VH_OK) { set_fatal(rc, "vh_batch_create"); break; }
-            const int kind = batch_kind(S->active);
+            for (Job *j : kv.second) evs.push_back(j->ev);
+            Group &g = groups[kv.first];
+            if (g.batch && g.members == evs) continue;
+            if (g.batch) vh_batch_destroy(g.batch);
+            g.batch = nullptr;
+            g.members = evs;
+            built = true;
+            if ((brc = vh_batch_create(evs.data(), (int)evs.size(), &g.batch)) != VH_OK) { bwhere = "vh_batch_create"; break; }
+            const int kind = batch_kind(kv.second);
             auto it = S->tunings.find(kind);
-            if (it != S->tunings.end()) rc = vh_batch_set_tuning(batch, &it->second);
+            if (it != S->tunings.end()) brc = vh_batch_set_tuning(g.batch, &it->second);
             else {
                 vh_batch_tuning t;
-                rc = vh_batch_autotune(batch, &t);
-                if (rc == VH_OK) S->tunings[kind] = t;
+                brc = vh_batch_autotune(g.batch, &t);
+                if (brc == VH_OK) S->tunings[kind] = t;
             }
-            if (rc != VH_OK) { set_fatal(rc, "batch tuning"); break; }
-            {
-                std::lock_guard<std::mutex> lk(S->mu);
-                S->st.batch_builds += 1;
-            }
-            membership_changed = false;
-            add(S->st.t_build_s, t_bld);
+            if (brc != VH_OK) { bwhere = "batch tuning"; break; }
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->st.batch_builds += 1;
         }
+        if (brc != VH_OK) { set_fatal(brc, bwhere); break; }
+        if (built) add(S->st.t_build_s, t_bld);
 
         /* ---- steps up to the earliest freezeout block (0: a block is due now) */
         int k = 1 << 30;
@@ -253,12 +283,25 @@ void worker_main(vh_server *S)
         if (S->cfg.max_steps > 0)
             for (auto &j : S->active) k = std::min(k, std::max(0, S->cfg.max_steps - j->steps));
         if (k > 0) {
+            /* everything is queued before anything is waited for: the solo
+             * events and the batches run concurrently on their streams */
             const auto t_st = tick();
-            int rc = vh_batch_step(batch, k);
+            for (Job *j : solo)
+                if (j->status == VH_OK) j->status = vh_event_step(j->ev, k);
+            int rc = VH_OK;
+            for (auto &kv : groups)
+                if ((rc = vh_batch_step(kv.second.batch, k)) != VH_OK) break;
             if (rc != VH_OK) { set_fatal(rc, "vh_batch_step"); break; }
-            void *bs = nullptr;
-            vh_batch_stream(batch, &bs);
-            cudaStreamSynchronize((cudaStream_t)bs);
+            for (auto &kv : groups) {
+                void *bs = nullptr;
+                vh_batch_stream(kv.second.batch, &bs);
+                cudaStreamSynchronize((cudaStream_t)bs);
+            }
+            for (Job *j : solo) {
+                void *es = nullptr;
+                vh_event_stream(j->ev, &es);
+                cudaStreamSynchronize((cudaStream_t)es);
+            }
             add(S->st.t_step_s, t_st);
             for (auto &j : S->active) j->steps += k;
             std::lock_guard<std::mutex> lk(S->mu);
@@ -305,24 +348,25 @@ void worker_main(vh_server *S)
             S->st.fo_blocks += (long long)due.size();
         }
 
-        /* ---- retire */
-        std::vector<std::unique_ptr<Job>> keep;
+        /* ---- retire (a batch goes before the events it holds) */
+        std::vector<std::unique_ptr<Job>> keep, retire;
         for (auto &j : S->active) {
             const bool capped = S->cfg.max_steps > 0 && j->steps >= S->cfg.max_steps;
-            if (j->status != VH_OK || j->zero_blocks >= 3 || capped) {
-                finish_job(S, j, j->status);
-                membership_changed = true;
-            } else {
-                keep.push_back(std::move(j));
+            if (j->status != VH_OK || j->zero_blocks >= 3 || capped) retire.push_back(std::move(j));
+            else keep.push_back(std::move(j));
+        }
+        for (auto &j : retire) {
+            auto it = groups.find(group_key(j->cfg));
+            if (it != groups.end() &&
+                std::find(it->second.members.begin(), it->second.members.end(), j->ev) != it->second.members.end()) {
+                vh_batch_destroy(it->second.batch);
+                groups.erase(it);
             }
         }
+        for (auto &j : retire) finish_job(S, j, j->status);
         S->active.swap(keep);
-        if (membership_changed && batch) {
-            vh_batch_destroy(batch);
-            batch = nullptr;
-        }
     }
-    if (batch) vh_batch_destroy(batch);
+    for (auto &kv : groups) vh_batch_destroy(kv.second.batch);
     if (pin) cudaFreeHost(pin);
     for (auto &j : S->active)
         if (j->ev) vh_event_destroy(j->ev);
@@ -339,6 +383,7 @@ void vh_server_config_default(vh_server_config *c)
     c->hbm_fraction = 0.8;
     c->max_events = 4096;
     c->max_steps = 0;
+    c->solo_cells = 1 << 17;
 }
 
 int vh_server_create(const vh_server_config *cfg, const double *eos_rows, int eos_nrows, vh_server **out)
@@ -349,7 +394,7 @@ int vh_server_create(const vh_server_config *cfg, const double *eos_rows, int eo
     vh_server_config c;
     vh_server_config_default(&c);
     if (cfg) c = *cfg;
-    if (!(c.hbm_fraction > 0 && c.hbm_fraction <= 1) || c.max_events < 1 || c.max_steps < 0)
+    if (!(c.hbm_fraction > 0 && c.hbm_fraction <= 1) || c.max_events < 1 || c.max_steps < 0 || c.solo_cells < 0)
         return vh::set_error(VH_ERR_ARG, "bad server configuration");
     auto *S = new vh_server;
     S->cfg = c;

@@ -436,7 +436,8 @@ class Batch:
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("hbm_fraction", C.c_double), ("max_events", C.c_int), ("max_steps", C.c_int)]
+    _fields_ = [("hbm_fraction", C.c_double), ("max_events", C.c_int), ("max_steps", C.c_int),
+                ("solo_cells", C.c_int)]
 
 
 class ServerDone(C.Structure):
@@ -466,13 +467,18 @@ _sig("vh_server_destroy", C.c_int, [C.c_void_p])
 
 class Server:
     """vh_server_*: submit events at any time; a worker thread admits them by
-    free device memory, advances them as one batch, streams their freezeout
-    surfaces to host memory and retires them."""
+    free device memory, advances them concurrently (small events in one batch
+    per kind, events of at least solo_cells cells alone; None: the library's
+    default), streams their freezeout surfaces to host memory and retires
+    them."""
 
-    def __init__(self, eos_rows=None, hbm_fraction=0.8, max_events=4096, max_steps=0):
+    def __init__(self, eos_rows=None, hbm_fraction=0.8, max_events=4096, max_steps=0, solo_cells=None):
         c = ServerConfig()
         lib.vh_server_config_default(C.byref(c))
         c.hbm_fraction, c.max_events, c.max_steps = hbm_fraction, max_events, max_steps
+        if solo_cells is not None:
+            c.solo_cells = solo_cells
+        self.solo_cells = c.solo_cells
         self._rows = None if eos_rows is None else np.ascontiguousarray(eos_rows, dtype=np.float64)
         h = C.c_void_p()
         check(lib.vh_server_create(C.byref(c), _ptr(self._rows), 0 if self._rows is None else len(self._rows),

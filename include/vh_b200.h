@@ -268,12 +268,13 @@ int vh_batch_stream(vh_batch *b, void **stream);
  * per process): events are submitted with their host initial condition at
  * any time; a worker thread admits them while their estimated device
  * footprint fits hbm_fraction of the free device memory, keeps their state on
- * the device, advances all admitted events as one batch, runs each event's
+ * the device, advances the admitted events concurrently -- the small ones as
+ * batches (one per kind: precision, bulk, EoS), events of at least solo_cells
+ * interior cells alone with the single-event kernels -- runs each event's
  * freezeout blocks at its fo_factor cadence (HydroPlugin.cpp:249-266) and
  * streams the elements to host memory, and retires an event after three
  * blocks with no cell above e_F (HydroPlugin.cpp:267-281), at max_steps, or on
- * a device error.  Events of one server share its EoS rows; precision, bulk
- * and the EoS kind must agree among the events submitted.
+ * a device error.  Events of one server share its EoS rows.
  */
 typedef struct vh_server vh_server;
 
@@ -281,6 +282,8 @@ typedef struct vh_server_config {
     double hbm_fraction;     /* share of the free device memory at creation the events may use */
     int max_events;          /* most events resident at once                                     */
     int max_steps;           /* RK2 steps after which an event is retired (0: no cap)            */
+    int solo_cells;          /* events with at least this many interior cells are stepped alone,
+                                on their own stream, beside the batches (0: every event batched) */
 } vh_server_config;
 
 typedef struct vh_server_done {
@@ -293,13 +296,13 @@ typedef struct vh_server_done {
 
 typedef struct vh_server_stats {
     long long submitted, queued, active, done;
-    long long steps;         /* batch steps run          */
+    long long steps;         /* steps run (each advances every active event) */
     long long fo_blocks;     /* freezeout blocks run     */
     long long batch_builds;  /* batches (re)built        */
     unsigned long long bytes_in_use, budget_bytes;
     double t_admit_s;        /* worker wall time: creating and initialising events */
     double t_build_s;        /*   (re)building and tuning batches                  */
-    double t_step_s;         /*   batch steps, launch to completion                */
+    double t_step_s;         /*   steps of the batches and solo events, launch to completion */
     double t_fo_s;           /*   freezeout blocks and surface copies              */
 } vh_server_stats;
 

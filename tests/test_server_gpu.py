@@ -1,7 +1,7 @@
 """The event server (vh_server_*): events submitted together, admitted by
-memory, advanced as one batch and frozen out at their own cadence must give
-exactly the surfaces and step counts of each event run alone with the same
-cadence (FP64 is bit-exact through batching)."""
+memory, advanced in batches (or alone, above the solo size) and frozen out at
+their own cadence must give exactly the surfaces and step counts of each event
+run alone with the same cadence (FP64 is bit-exact through batching)."""
 import numpy as np
 import pytest
 
@@ -25,11 +25,13 @@ def _events(rows):
     return out
 
 
-@pytest.mark.parametrize("hbm_fraction", [0.5, 1e-9])
-def test_server_matches_single_event_runs(hbm_fraction):
+@pytest.mark.parametrize("hbm_fraction,solo_cells", [(0.5, None), (1e-9, None), (0.5, 1000), (0.5, 1)])
+def test_server_matches_single_event_runs(hbm_fraction, solo_cells):
+    """solo_cells 1000 steps the 33^2 and 41^2 events alone beside a batch of
+    the other three; 1 steps every event alone"""
     rows = vh.synthetic_eos_table()
     evs = _events(rows)
-    srv = vh.Server(rows, hbm_fraction=hbm_fraction, max_steps=60)
+    srv = vh.Server(rows, hbm_fraction=hbm_fraction, max_steps=60, solo_cells=solo_cells)
     for tag, (c, st) in enumerate(evs):
         srv.submit(c, st, tag)
     srv.wait(300)
@@ -39,6 +41,8 @@ def test_server_matches_single_event_runs(hbm_fraction):
     assert stats["done"] == len(evs) and stats["queued"] == 0 and stats["active"] == 0
     if hbm_fraction < 1e-6:
         assert stats["batch_builds"] >= len(evs)      # admitted one at a time
+    if solo_cells == 1:
+        assert stats["batch_builds"] == 0
     for tag, (c, st) in enumerate(evs):
         d = done[tag]
         assert d.t_submit <= d.t_admit <= d.t_done
@@ -51,15 +55,33 @@ def test_server_matches_single_event_runs(hbm_fraction):
     srv.close()
 
 
-def test_server_reports_incompatible_events():
+def test_server_batches_each_kind_apart():
+    """events of different precision and EoS kind are served side by side,
+    one batch per kind; FP64 members equal their single runs bit for bit, the
+    mixed member its single mixed run within the batch-vs-single rounding"""
     rows = vh.synthetic_eos_table()
-    srv = vh.Server(rows, max_steps=20)
     a = vh.hotspot_config(17)
     b = vh.hotspot_config(19).copy(precision=vh.VH_PREC_MIXED)
-    srv.submit(a, vh.hotspot_ic(a, rows, seed=1), 1)
-    srv.submit(b, vh.hotspot_ic(b, rows, seed=2), 2)
-    with pytest.raises(vh.VhError):
-        srv.wait(120)
+    g = vh.gubser_config(15, 15)
+    for c in (a, b, g):
+        c.fo_factor = 4
+    ics = [vh.hotspot_ic(a, rows, seed=1), vh.hotspot_ic(b, rows, seed=2), vh.gubser_ic(g)]
+    srv = vh.Server(rows, max_steps=20)
+    for tag, (c, st) in enumerate(zip((a, b, g), ics)):
+        srv.submit(c, st, tag)
+    srv.wait(120)
+    done = {d.tag: d for d in srv.poll()}
+    assert srv.stats()["batch_builds"] == 3
+    for tag, (c, st) in enumerate(zip((a, b, g), ics)):
+        steps, ref, status = vh.run_like_server(c, rows, st, max_steps=20)
+        surf = srv.take_surface(tag)
+        assert done[tag].status == status == 0 and done[tag].steps == steps
+        assert surf.shape == ref.shape
+        if c.precision == vh.VH_PREC_FP64:
+            assert np.array_equal(surf.view(np.uint64), ref.view(np.uint64))
+        else:
+            scale = np.maximum(np.max(np.abs(ref), axis=0), 1e-300)
+            assert np.max(np.abs(surf - ref) / scale) < 1e-5
     srv.close()
 
 
