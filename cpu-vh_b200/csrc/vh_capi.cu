@@ -6,7 +6,9 @@
  * phase-split kernels; buffer roles rotate by index on the host.
  */
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -535,6 +537,17 @@ int vh_event_freezeout_launch(vh_event *ev)
         CUDA_TRY(cudaMalloc(&ev->fo_scratch, ev->fo_scratch_ints * sizeof(int)));
         CUDA_TRY(cudaMallocHost(&ev->fo_hdr, 2 * sizeof(int)));
         CUDA_TRY(cudaEventCreateWithFlags(&ev->fo_done, cudaEventDisableTiming));
+        /* a first element buffer sized for a surface crossing the lattice
+         * (twice its cross sections in 3+1D, eight times its edges in 2+1D),
+         * so that blocks seldom overflow it; VH_FO_INITIAL_CAP overrides the
+         * size (tests of the overflow path) */
+        if (!ev->fo_elems) {
+            const long long nx = c.nx, ny = c.ny, nz = c.nz;
+            long long cap = (nz > 1 ? 2 * (nx * ny + ny * nz + nx * nz) : 8 * (nx + ny)) + 1024;
+            if (const char *env = getenv("VH_FO_INITIAL_CAP")) cap = std::max(1LL, atoll(env));
+            ev->fo_cap = (int)std::min<long long>(cap, 1LL << 28);
+            CUDA_TRY(cudaMalloc(&ev->fo_elems, (size_t)ev->fo_cap * VH_FO_COLUMNS * sizeof(double)));
+        }
     }
     vh::FoArgs a;
     fo_args(ev, a);
@@ -555,21 +568,17 @@ int vh_event_freezeout_finish(vh_event *ev, int *n_elements, int *n_above)
     CUDA_TRY(cudaEventSynchronize(ev->fo_done));
     int above = ev->fo_hdr[0], total = ev->fo_hdr[1];
     if (total > ev->fo_cap) {
-        /* not enough room: re-run with a larger buffer from the same slabs
-         * (the slab shift is idempotent) */
+        /* not enough room: a buffer with room to grow, and the emit step
+         * again from the offsets the block left in the scratch */
         cudaFree(ev->fo_elems);
         ev->fo_elems = nullptr;
-        ev->fo_cap = total + total / 4 + 1024;
+        ev->fo_cap = total + total / 2 + 1024;
         CUDA_TRY(cudaMalloc(&ev->fo_elems, (size_t)ev->fo_cap * VH_FO_COLUMNS * sizeof(double)));
         vh::FoArgs a;
         fo_args(ev, a);
-        vh::launch_freezeout(a, ev->stream);
+        vh::launch_freezeout_emit(a, ev->stream);
         CUDA_TRY(cudaGetLastError());
-        CUDA_TRY(cudaMemcpyAsync(ev->fo_hdr, ev->fo_scratch + ev->fo_scratch_ints - 2, 2 * sizeof(int),
-                                 cudaMemcpyDeviceToHost, ev->stream));
         CUDA_TRY(cudaStreamSynchronize(ev->stream));
-        above = ev->fo_hdr[0];
-        total = ev->fo_hdr[1];
     }
     ev->fo_prev = 1 - ev->fo_prev;
     ev->fo_count = total;

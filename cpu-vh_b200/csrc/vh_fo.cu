@@ -338,10 +338,18 @@ void launch_freezeout(const FoArgs &a, cudaStream_t st)
     const unsigned gk = (unsigned)((sc.nc + 127) / 128);
     fo_count_kernel<<<gk, 128, 0, st>>>(a, sc);
     exclusive_scan(sc.counts, sc.nc, sc.bsum, sc.hdr + 2, st);
-    if (a.elems && a.cap > 0) {
-        if (a.eos.kind == 1) fo_emit_kernel<1><<<gk, 128, 0, st>>>(a, sc);
-        else fo_emit_kernel<0><<<gk, 128, 0, st>>>(a, sc);
-    }
+    launch_freezeout_emit(a, st);
+}
+
+/* the emit step alone, from the offsets the last launch_freezeout left in the
+ * scratch: the elements of a block that did not fit, into a larger buffer */
+void launch_freezeout_emit(const FoArgs &a, cudaStream_t st)
+{
+    if (!a.elems || a.cap <= 0) return;
+    FoScratch sc = carve(a);
+    const unsigned gk = (unsigned)((sc.nc + 127) / 128);
+    if (a.eos.kind == 1) fo_emit_kernel<1><<<gk, 128, 0, st>>>(a, sc);
+    else fo_emit_kernel<0><<<gk, 128, 0, st>>>(a, sc);
 }
 
 } // namespace vh

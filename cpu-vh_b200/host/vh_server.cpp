@@ -323,6 +323,7 @@ void worker_main(vh_server *S)
             int nel = 0, nab = 0;
             int rc = vh_event_freezeout_finish(j->ev, &nel, &nab);
             if (rc == VH_OK && nel > 0) {
+                const auto t_cp = tick();
                 const size_t need = (size_t)nel * VH_FO_COLUMNS;
                 if (need > pin_cap) {
                     if (pin) cudaFreeHost(pin);
@@ -337,6 +338,9 @@ void worker_main(vh_server *S)
                 } else {
                     rc = vh_event_fetch_surface(j->ev, j->surface.data() + off, nel, &nel);
                 }
+                add(S->st.t_fo_copy_s, t_cp);
+                std::lock_guard<std::mutex> lk(S->mu);
+                S->st.fo_elements += nel;
             }
             if (rc == VH_OK) rc = vh_event_status(j->ev, nullptr, nullptr);
             if (rc != VH_OK) { j->status = rc; continue; }

@@ -449,7 +449,8 @@ class ServerStats(C.Structure):
     _fields_ = [("submitted", C.c_longlong), ("queued", C.c_longlong), ("active", C.c_longlong),
                 ("done", C.c_longlong), ("steps", C.c_longlong), ("fo_blocks", C.c_longlong),
                 ("batch_builds", C.c_longlong), ("bytes_in_use", C.c_ulonglong), ("budget_bytes", C.c_ulonglong),
-                ("t_admit_s", C.c_double), ("t_build_s", C.c_double), ("t_step_s", C.c_double), ("t_fo_s", C.c_double)]
+                ("t_admit_s", C.c_double), ("t_build_s", C.c_double), ("t_step_s", C.c_double), ("t_fo_s", C.c_double),
+                ("t_fo_copy_s", C.c_double), ("fo_elements", C.c_longlong)]
 
 
 _sig("vh_server_config_default", None, [C.POINTER(ServerConfig)])

@@ -304,6 +304,8 @@ typedef struct vh_server_stats {
     double t_build_s;        /*   (re)building and tuning batches                  */
     double t_step_s;         /*   steps of the batches and solo events, launch to completion */
     double t_fo_s;           /*   freezeout blocks and surface copies              */
+    double t_fo_copy_s;      /*     of which surface copies to host memory          */
+    long long fo_elements;   /* freezeout elements collected                         */
 } vh_server_stats;
 
 void vh_server_config_default(vh_server_config *c);

@@ -50,13 +50,24 @@ def _run_blocks(cfg, rows, st, blocks):
     return total
 
 
-def test_freezeout_gubser_2p1d_bitexact():
+# the element buffer's first size: the library's estimate, or one so small
+# that blocks overflow it and are emitted again into a larger buffer
+CAPS = [None, "1", "200"]
+
+
+@pytest.mark.parametrize("initial_cap", CAPS)
+def test_freezeout_gubser_2p1d_bitexact(initial_cap, monkeypatch):
+    if initial_cap:
+        monkeypatch.setenv("VH_FO_INITIAL_CAP", initial_cap)
     cfg = vh.gubser_config(41, 37)
     cfg.T_freezeout_GeV = 0.2
     assert _run_blocks(cfg, None, vh.gubser_ic(cfg), 5) > 0
 
 
-def test_freezeout_glauber_3p1d_bitexact():
+@pytest.mark.parametrize("initial_cap", CAPS)
+def test_freezeout_glauber_3p1d_bitexact(initial_cap, monkeypatch):
+    if initial_cap:
+        monkeypatch.setenv("VH_FO_INITIAL_CAP", initial_cap)
     cfg = vh.glauber_config(21, 19, 7)
     cfg.dx = cfg.dy = 0.6
     cfg.dz = 0.5
