@@ -159,14 +159,49 @@ void worker_main(vh_server *S)
     cudaSetDevice(S->device);
     std::map<int, Group> groups;    /* batches by group_key */
     int held_rounds = 0;        /* rounds an admission waited for alignment */
-    /* pinned staging for surface copies (a pageable destination halves the copy rate) */
-    double *pin = nullptr;
-    size_t pin_cap = 0;
     auto tick = [] { return Clock::now(); };
     auto add = [&](double &acc, Clock::time_point a) {
         const double d = std::chrono::duration<double>(Clock::now() - a).count();
         std::lock_guard<std::mutex> lk(S->mu);
         acc += d;
+        return d;
+    };
+    /* Surfaces come to host memory in two moves: at the block, a device copy
+     * into a pinned staging buffer (a pageable destination halves the copy
+     * rate); in the next round, while the GPU runs its steps, the append to
+     * the event's surface (the host copy and the first touch of its pages
+     * cost as much as the device copy).  Staging buffers are reused. */
+    struct Staging { double *buf = nullptr; size_t cap = 0; };
+    struct Pending { Job *j; Staging s; size_t n; };
+    std::vector<Staging> pool;
+    std::vector<Pending> pending;
+    auto take_staging = [&](size_t need) {
+        int best = -1;
+        for (int i = 0; i < (int)pool.size(); ++i)
+            if (pool[i].cap >= need && (best < 0 || pool[i].cap < pool[best].cap)) best = i;
+        Staging st;
+        if (best >= 0) {
+            st = pool[best];
+            pool.erase(pool.begin() + best);
+            return st;
+        }
+        const size_t cap = std::max(need, (size_t)1 << 15);
+        if (cudaMallocHost(&st.buf, cap * sizeof(double)) == cudaSuccess) st.cap = cap;
+        else st.buf = nullptr;
+        return st;
+    };
+    /* append the staged blocks (of one event, or of all) to their surfaces */
+    auto flush = [&](const Job *only) {
+        if (pending.empty()) return 0.0;
+        const auto t = tick();
+        std::vector<Pending> keep;
+        for (auto &c : pending) {
+            if (only && c.j != only) { keep.push_back(c); continue; }
+            c.j->surface.insert(c.j->surface.end(), c.s.buf, c.s.buf + c.n);
+            pool.push_back(c.s);
+        }
+        pending.swap(keep);
+        return add(S->st.t_fo_copy_s, t);
     };
     bool waiting = false;       /* events queued after this round's admission */
     auto set_fatal = [&](int rc, const char *where) {
@@ -292,6 +327,7 @@ void worker_main(vh_server *S)
             for (auto &kv : groups)
                 if ((rc = vh_batch_step(kv.second.batch, k)) != VH_OK) break;
             if (rc != VH_OK) { set_fatal(rc, "vh_batch_step"); break; }
+            const double copy_s = flush(nullptr);
             for (auto &kv : groups) {
                 void *bs = nullptr;
                 vh_batch_stream(kv.second.batch, &bs);
@@ -302,10 +338,16 @@ void worker_main(vh_server *S)
                 vh_event_stream(j->ev, &es);
                 cudaStreamSynchronize((cudaStream_t)es);
             }
-            add(S->st.t_step_s, t_st);
+            {
+                const double d = std::chrono::duration<double>(Clock::now() - t_st).count() - copy_s;
+                std::lock_guard<std::mutex> lk(S->mu);
+                S->st.t_step_s += d;
+            }
             for (auto &j : S->active) j->steps += k;
             std::lock_guard<std::mutex> lk(S->mu);
             S->st.steps += k;
+        } else {
+            flush(nullptr);
         }
 
         /* ---- freezeout blocks that are due: queue all, then collect */
@@ -325,17 +367,14 @@ void worker_main(vh_server *S)
             if (rc == VH_OK && nel > 0) {
                 const auto t_cp = tick();
                 const size_t need = (size_t)nel * VH_FO_COLUMNS;
-                if (need > pin_cap) {
-                    if (pin) cudaFreeHost(pin);
-                    pin_cap = std::max(need, 2 * pin_cap);
-                    if (cudaMallocHost(&pin, pin_cap * sizeof(double)) != cudaSuccess) { pin = nullptr; pin_cap = 0; }
-                }
-                const size_t off = j->surface.size();
-                j->surface.resize(off + need);
-                if (pin) {
-                    rc = vh_event_fetch_surface(j->ev, pin, nel, &nel);
-                    if (rc == VH_OK) std::copy(pin, pin + need, j->surface.data() + off);
-                } else {
+                Staging st = take_staging(need);
+                if (st.buf) {
+                    rc = vh_event_fetch_surface(j->ev, st.buf, nel, &nel);
+                    if (rc == VH_OK) pending.push_back({j, st, need});
+                    else pool.push_back(st);
+                } else {                                 /* no pinned memory: straight to the surface */
+                    const size_t off = j->surface.size();
+                    j->surface.resize(off + need);
                     rc = vh_event_fetch_surface(j->ev, j->surface.data() + off, nel, &nel);
                 }
                 add(S->st.t_fo_copy_s, t_cp);
@@ -367,11 +406,15 @@ void worker_main(vh_server *S)
                 groups.erase(it);
             }
         }
-        for (auto &j : retire) finish_job(S, j, j->status);
+        for (auto &j : retire) {
+            flush(j.get());
+            finish_job(S, j, j->status);
+        }
         S->active.swap(keep);
     }
     for (auto &kv : groups) vh_batch_destroy(kv.second.batch);
-    if (pin) cudaFreeHost(pin);
+    for (auto &c : pending) pool.push_back(c.s);
+    for (auto &b : pool) cudaFreeHost(b.buf);
     for (auto &j : S->active)
         if (j->ev) vh_event_destroy(j->ev);
 }
