@@ -559,7 +559,8 @@ def run_batch(args, torch, world, rank, barrier, max_over_ranks):
                                               "CUDA events per event"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": None,
-                             "kernel": "kt_batch_kernel " + dom, "launches": dom_n,
+                             "kernel": ("kt_batch_face_kernel " if mixed and dom == "flux" else "kt_batch_kernel ") + dom,
+                             "launches": dom_n,
                              "launch_us": launch_s * 1e6, "algorithmic_bytes": alg_bytes,
                              "share": dom_ms / sum(t for t, _ in kern.values()),
                              "note": f"peak: {peak_kind} HBM copy bandwidth; FP64-issue bound"},

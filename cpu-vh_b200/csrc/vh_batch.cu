@@ -148,6 +148,8 @@ struct vh_batch {
     std::vector<TimeTable> ttabs;
     std::vector<int> mem_ttab;
     std::map<int, Tiles> tiles;      /* key: tile_x */
+    int4 *ftiles[3] = {};            /* mixed precision: face tiles per axis */
+    int n_ftiles[3] = {};
     bool tuned = false;
     vh_batch_tuning tune{};
     cudaGraph_t graph = nullptr;
@@ -194,6 +196,35 @@ int build_tiles(vh_batch *b, int tx)
         BTRY(cudaMemcpy(T.z, z.data(), z.size() * sizeof(int4), cudaMemcpyHostToDevice));
     }
     b->tiles[tx] = T;
+    return VH_OK;
+}
+
+/* mixed precision: the face tiles of kt_batch_face_kernel, per axis (x
+ * tiles cover 31 cells of 8 rows, y tiles 32 cells of 7 rows, eta tiles 32
+ * cells of 7 planes of one row, of the 3+1D members) */
+int build_face_tiles(vh_batch *b)
+{
+    constexpr int TX = vh::kBatchFaceTX, TY = vh::kBatchFaceTY;
+    std::vector<int4> f[3];
+    for (size_t m = 0; m < b->mem.size(); ++m) {
+        const vh_config &c = b->mem[m]->cfg;
+        for (int k = 0; k < c.nz; ++k) {
+            for (int j0 = 0; j0 < c.ny; j0 += TY)
+                for (int i0 = 0; i0 < c.nx; i0 += TX - 1) f[0].push_back(make_int4((int)m, i0, j0, k));
+            for (int j0 = 0; j0 < c.ny; j0 += TY - 1)
+                for (int i0 = 0; i0 < c.nx; i0 += TX) f[1].push_back(make_int4((int)m, i0, j0, k));
+        }
+        if (c.nz > 1)
+            for (int j = 0; j < c.ny; ++j)
+                for (int k0 = 0; k0 < c.nz; k0 += TY - 1)
+                    for (int i0 = 0; i0 < c.nx; i0 += TX) f[2].push_back(make_int4((int)m, i0, j, k0));
+    }
+    for (int d = 0; d < 3; ++d) {
+        b->n_ftiles[d] = (int)f[d].size();
+        if (f[d].empty()) continue;
+        BTRY(cudaMalloc(&b->ftiles[d], f[d].size() * sizeof(int4)));
+        BTRY(cudaMemcpy(b->ftiles[d], f[d].data(), f[d].size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
     return VH_OK;
 }
 
@@ -275,11 +306,27 @@ void launch_phase(vh_batch *b, int stage, int phase, int tx, int persistent)
     k<<<grid, block, 0, b->stream>>>(B);
 }
 
+/* mixed precision: one axis of the face-once flux over the face tiles */
+void launch_face(vh_batch *b, int stage, int dir)
+{
+    vh::BatchLaunch B;
+    B.args = b->d_args + (size_t)stage * b->mem.size();
+    B.tiles = b->ftiles[dir - 1];
+    B.ntiles = b->n_ftiles[dir - 1];
+    if (B.ntiles == 0) return;
+    vh::BatchKernel k = vh::batch_face_kernel_mixed(b->nq, b->eos_kind, dir);
+    k<<<B.ntiles, dim3(vh::kBatchFaceTX, vh::kBatchFaceTY, 1), 0, b->stream>>>(B);
+}
+
 void launch_stage(vh_batch *b, int stage, const vh_batch_tuning &t, vh::StageMarks *m)
 {
     if (m) { m->n = 0; cudaEventRecord(m->ev[0], b->stream); }
     auto run = [&](int phase) {
-        launch_phase(b, stage, phase, t.tile_x[phase], t.persistent[phase]);
+        /* the split stage's flux is face-once in mixed precision, as on
+         * single events (the tile shape of these phases is then unused) */
+        const bool face = b->mixed && phase >= VH_PHASE_FLUX_X && phase <= VH_PHASE_FLUX_ETA;
+        if (face) launch_face(b, stage, phase - VH_PHASE_FLUX_X + 1);
+        else launch_phase(b, stage, phase, t.tile_x[phase], t.persistent[phase]);
         if (m) { m->phase[m->n] = phase; cudaEventRecord(m->ev[++m->n], b->stream); }
     };
     if (t.fused) { run(VH_PHASE_FUSED); return; }
@@ -416,6 +463,8 @@ int preload(vh_batch *b)
             BTRY(cudaFuncGetAttributes(&attr, k));
             vh::resident_blocks(k);
         }
+    if (b->mixed)
+        for (int d = 1; d <= 3; ++d) BTRY(cudaFuncGetAttributes(&attr, vh::batch_face_kernel_mixed(b->nq, b->eos_kind, d)));
     return VH_OK;
 }
 
@@ -510,6 +559,7 @@ int vh_batch_create(vh_event *const *events, int n_events, vh_batch **out)
     CTRY(cudaMemset(b->d_nstep, 0, nm * sizeof(int)));
 #undef CTRY
     rc = ensure_times(b, 1024);
+    if (rc == VH_OK && b->mixed) rc = build_face_tiles(b);
     if (rc != VH_OK) { vh_batch_destroy(b); return rc; }
     *out = b;
     return VH_OK;
@@ -521,6 +571,7 @@ int vh_batch_destroy(vh_batch *b)
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graph(b);
     for (auto &kv : b->tiles) { cudaFree(kv.second.all); cudaFree(kv.second.z); }
+    for (int4 *f : b->ftiles) cudaFree(f);
     for (auto &T : b->ttabs) cudaFree(T.d);
     for (auto &m : b->marks)
         for (cudaEvent_t e : m.ev) cudaEventDestroy(e);

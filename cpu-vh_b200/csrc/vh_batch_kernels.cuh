@@ -51,6 +51,35 @@ __global__ void __launch_bounds__(128, 4) kt_batch_kernel(const __grid_constant_
     }
 }
 
+/* Mixed precision: the face-once flux of one axis over the batch, one block
+ * of 32 x 8 faces per tile (member, i0, j0, k0) -- flux_faces_tile, as the
+ * single-event kt_flux_face_kernel runs it, so a member's fluxes equal its
+ * single-event ones.  Tiles step by 31 cells along x for DIR 1 and by 7 along
+ * y (DIR 2) or eta (DIR 3): the last face of a tile row only feeds the cell
+ * below it. */
+constexpr int kBatchFaceTX = 32, kBatchFaceTY = 8;
+
+template <int NQ, int EOS, int DIR>
+__global__ void __launch_bounds__(kBatchFaceTX * kBatchFaceTY, 2) kt_batch_face_kernel(const __grid_constant__ BatchLaunch B)
+{
+    __shared__ __align__(16) StageArgs sA;
+    __shared__ double sm[NQ * kBatchFaceTX * kBatchFaceTY];
+    const int tid = threadIdx.x + kBatchFaceTX * threadIdx.y;
+    int cur = -1;
+    for (int t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
+        const int4 tile = __ldg(B.tiles + t);
+        if (tile.x != cur) {           /* uniform over the block */
+            __syncthreads();
+            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(B.args + tile.x);
+            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sA);
+            for (int w = tid; w < (int)(sizeof(StageArgs) / 8); w += kBatchFaceTX * kBatchFaceTY) dst[w] = src[w];
+            __syncthreads();
+            cur = tile.x;
+        }
+        flux_faces_tile<NQ, EOS, DIR, kBatchFaceTX, kBatchFaceTY>(sA, tile.y, tile.z, tile.w, sm);
+    }
+}
+
 template <int NQ, int EOS, int PHASE, bool MIXED>
 static BatchKernel batch_kernel_z(bool st2, int zm)
 {

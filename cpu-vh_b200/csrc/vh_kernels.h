@@ -107,6 +107,9 @@ using BatchKernel = void (*)(BatchLaunch);
 /* phase: VH_PHASE_*; zm: 0 all members 2+1D, 1 all 3+1D, 2 mixed */
 BatchKernel batch_kernel(int nq, int eos_kind, int phase, bool st2, int zm, bool mixed);
 BatchKernel batch_kernel_mixed(int nq, int eos_kind, int phase, bool st2, int zm);
+/* mixed precision: the face-once flux along dir (1-3) over face tiles of
+ * 32 x 8 faces (block 32 x 8) */
+BatchKernel batch_face_kernel_mixed(int nq, int eos_kind, int dir);
 
 /* ---- freezeout ---- */
 struct FoArgs {

@@ -33,4 +33,17 @@ BatchKernel batch_kernel_mixed(int nq, int eos_kind, int phase, bool st2, int zm
     return batch_kernel_of<true>(nq, eos_kind, phase, st2, zm);
 }
 
+template <int NQ, int EOS>
+static BatchKernel batch_face_t(int dir)
+{
+    return dir == 1 ? kt_batch_face_kernel<NQ, EOS, 1> : dir == 2 ? kt_batch_face_kernel<NQ, EOS, 2>
+                                                                   : kt_batch_face_kernel<NQ, EOS, 3>;
+}
+
+BatchKernel batch_face_kernel_mixed(int nq, int eos_kind, int dir)
+{
+    if (nq == 15) return eos_kind == 1 ? batch_face_t<15, 1>(dir) : batch_face_t<15, 0>(dir);
+    return eos_kind == 1 ? batch_face_t<14, 1>(dir) : batch_face_t<14, 0>(dir);
+}
+
 } // namespace vh
