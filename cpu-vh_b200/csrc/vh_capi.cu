@@ -374,11 +374,24 @@ static const double *field_ptr(const vh_event *ev, int field)
     return nullptr;
 }
 
+/* A 2+1D event's state planes carry no eta ghost copies while it evolves
+ * (put_with_ghosts); a read writes them first, so every read sees the
+ * reference's padded layout. */
+static void fill_eta_ghosts(vh_event *ev, int field, const double *plane)
+{
+    if (ev->cfg.nz != 1) return;
+    const bool state = (field >= 0 && field < ev->nq) || (field >= VH_F_UT && field < VH_F_UT + 4) ||
+                       (field >= VH_F_UPT && field < VH_F_UPT + 4) || field == VH_F_E || field == VH_F_P;
+    if (state)
+        vh::launch_eta_ghost_fill(const_cast<double *>(plane), ev->cfg.nx, ev->cfg.ny, ev->ncx, ev->ncy, ev->stream);
+}
+
 int vh_event_get_field(vh_event *ev, int field, double *host_out)
 {
     if (!ev || !host_out) return fail(VH_ERR_ARG, "null argument");
     const double *src = field_ptr(ev, field);
     if (!src) return fail(VH_ERR_ARG, "unknown field id");
+    fill_eta_ghosts(ev, field, src);
     size_t len = (size_t)ev->ncx * ev->ncy * ev->ncz;
     CUDA_TRY(cudaMemcpyAsync(host_out, src, len * sizeof(double), cudaMemcpyDeviceToHost, ev->stream));
     CUDA_TRY(cudaStreamSynchronize(ev->stream));
@@ -390,6 +403,8 @@ int vh_event_device_field(vh_event *ev, int field, double **d_ptr)
     if (!ev || !d_ptr) return fail(VH_ERR_ARG, "null argument");
     const double *src = field_ptr(ev, field);
     if (!src) return fail(VH_ERR_ARG, "unknown field id");
+    fill_eta_ghosts(ev, field, src);
+    CUDA_TRY(cudaGetLastError());
     *d_ptr = const_cast<double *>(src);
     return VH_OK;
 }

@@ -138,6 +138,8 @@ struct FoArgs {
 /* Runs the whole freezeout block; returns the number of elements through
  * *a.n_total (device) and leaves elements in a.elems. */
 void launch_freezeout(const FoArgs &a, cudaStream_t s);
+/* nz = 1: write the eta ghost planes of one padded field plane (ncz = 5) */
+void launch_eta_ghost_fill(double *plane, int nx, int ny, int ncx, int ncy, cudaStream_t s);
 void launch_freezeout_emit(const FoArgs &a, cudaStream_t s);
 void launch_cornelius_batch(int dim, const double *cubes, int n, double v0, const double *dx,
                             double *slots, int *counts, int *err, cudaStream_t st);

@@ -83,7 +83,8 @@ __global__ void vorticity_kernel(const __grid_constant__ VortArgs A)
     const long long s = i + (long long)A.ncx * j + sxy * k;
     const double T = eos_T<EOS>(A.eos, __ldg(A.e + s));
     const double yT = 1.0 / T;
-    const long long nb[6] = {s - 1, s + 1, s - A.ncx, s + A.ncx, s - sxy, s + sxy};
+    const long long sz = (A.nz > 1) ? sxy : 0;      /* nz = 1: no eta ghost planes are kept */
+    const long long nb[6] = {s - 1, s + 1, s - A.ncx, s + A.ncx, s - sz, s + sz};
     double b[4], ddt[4], dd[3][4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -112,6 +113,28 @@ __global__ void vorticity_kernel(const __grid_constant__ VortArgs A)
     w[5 * L + s] = (-1.0 / 2.0) * (dd[1][3] - dd[2][2]);
 #pragma unroll
     for (int c = 0; c < 4; ++c) w[(6 + c) * L + s] = b[c];
+}
+
+/* the four eta ghost planes of one field plane of a 2+1D event, copied from
+ * its interior plane (what DynamicalVariables.cpp:220-378 leaves there) */
+__global__ void eta_ghost_fill_kernel(double *plane, int nx, int ny, int ncx, long long sxy)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x + 2;
+    const int j = blockIdx.y * blockDim.y + threadIdx.y + 2;
+    if (i >= nx + 2 || j >= ny + 2) return;
+    const long long s = i + (long long)ncx * j + 2 * sxy;
+    const double v = plane[s];
+    plane[s - sxy] = v;
+    plane[s - 2 * sxy] = v;
+    plane[s + sxy] = v;
+    plane[s + 2 * sxy] = v;
+}
+
+void launch_eta_ghost_fill(double *plane, int nx, int ny, int ncx, int ncy, cudaStream_t s)
+{
+    dim3 block(32, 4, 1);
+    dim3 grid((nx + 31) / 32, (ny + 3) / 4, 1);
+    eta_ghost_fill_kernel<<<grid, block, 0, s>>>(plane, nx, ny, ncx, (long long)ncx * ncy);
 }
 
 void launch_vorticity(const VortArgs &a, cudaStream_t s)

@@ -291,7 +291,8 @@ __device__ __forceinline__ void source_update(const StageArgs &A, long long s, d
 {
     const long long L = A.L;
     const double th = A.theta;
-    const long long sx = 1, sy = A.ncx, sz = (long long)A.ncx * A.ncy;
+    /* nz = 1: the eta neighbours are the cell itself (see put_with_ghosts) */
+    const long long sx = 1, sy = A.ncx, sz = (A.nz > 1) ? (long long)A.ncx * A.ncy : 0;
     double Qv[NQ];
 #pragma unroll
     for (int n = 0; n < NQ; ++n) Qv[n] = __ldg(A.qin + n * L + s);
@@ -406,7 +407,13 @@ __device__ __forceinline__ void put_cell(const StageArgs &A, long long d, const 
     A.uout[3 * L + d] = P.un;
 }
 
-/* the cell and its zero-gradient ghost copies (DynamicalVariables.cpp:220-378) */
+/* the cell and its zero-gradient ghost copies (DynamicalVariables.cpp:220-378).
+ * A 2+1D event (nz = 1) keeps no eta ghost planes while it evolves: nothing
+ * in the step reads them (the eta pass is skipped, and the eta differences of
+ * the source terms and of the vorticity take the cell itself, which is what
+ * the ghost copies hold), so the four copies of every cell -- 4/5 of the
+ * phase's stores -- are left out and written only when a field is read
+ * (launch_eta_ghost_fill). */
 template <int NQ>
 __device__ __forceinline__ void put_with_ghosts(const StageArgs &A, int i, int j, int k, long long s,
                                                 const double *__restrict__ acc, const Prim &P)
@@ -417,8 +424,10 @@ __device__ __forceinline__ void put_with_ghosts(const StageArgs &A, int i, int j
     if (i == A.nx + 1) { put_cell<NQ>(A, s + 1, acc, P); put_cell<NQ>(A, s + 2, acc, P); }
     if (j == 2) { put_cell<NQ>(A, s - A.ncx, acc, P); put_cell<NQ>(A, s - 2 * A.ncx, acc, P); }
     if (j == A.ny + 1) { put_cell<NQ>(A, s + A.ncx, acc, P); put_cell<NQ>(A, s + 2 * A.ncx, acc, P); }
-    if (k == 2) { put_cell<NQ>(A, s - sxy, acc, P); put_cell<NQ>(A, s - 2 * sxy, acc, P); }
-    if (k == A.nz + 1) { put_cell<NQ>(A, s + sxy, acc, P); put_cell<NQ>(A, s + 2 * sxy, acc, P); }
+    if (A.nz > 1) {
+        if (k == 2) { put_cell<NQ>(A, s - sxy, acc, P); put_cell<NQ>(A, s - 2 * sxy, acc, P); }
+        if (k == A.nz + 1) { put_cell<NQ>(A, s + sxy, acc, P); put_cell<NQ>(A, s + 2 * sxy, acc, P); }
+    }
 }
 
 /* One whole stage for cell (i, j, k) at padded index s. */
@@ -574,7 +583,8 @@ __device__ __forceinline__ void source_update_m(const StageArgs &A, long long s,
 {
     const long long L = A.L;
     const float th = (float)A.theta;
-    const long long sx = 1, sy = A.ncx, sz = (long long)A.ncx * A.ncy;
+    /* nz = 1: the eta neighbours are the cell itself (see put_with_ghosts) */
+    const long long sx = 1, sy = A.ncx, sz = (A.nz > 1) ? (long long)A.ncx * A.ncy : 0;
     double Qv[NQ];
 #pragma unroll
     for (int n = 0; n < NQ; ++n) Qv[n] = __ldg(A.qin + n * L + s);

@@ -331,7 +331,10 @@ int vh_server_wait(vh_server *s, double timeout_s);
 int vh_server_stats_get(vh_server *s, vh_server_stats *out);
 int vh_server_destroy(vh_server *s);
 
-/* Device pointer of a padded field (for zero-copy inspection / timing). */
+/* Device pointer of a padded field (for zero-copy inspection / timing).  A
+ * 2+1D event keeps no eta ghost planes while it steps; for its state fields
+ * this call writes them on the event's stream first, so read the plane in
+ * that stream's order. */
 int vh_event_device_field(vh_event *ev, int field, double **d_ptr);
 
 /* Energy density [fm^-4] for temperature T [fm^-1] with the event's EoS
