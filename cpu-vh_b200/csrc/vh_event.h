@@ -14,6 +14,8 @@
 #define VH_EVENT_H
 
 #include <cuda_runtime.h>
+#include <cmath>
+#include <cstdlib>
 #include <vector>
 #include "vh_b200.h"
 #include "vh_internal.h"
@@ -83,6 +85,15 @@ struct vh_event {
     size_t marks_used = 0;
 };
 
+/* an environment switch set to 0 (read on every call; tests of the forms) */
+static inline bool vh_env_off(const char *name)
+{
+    const char *e = getenv(name);
+    return e && e[0] == '0';
+}
+
+/* VH_CS2_SHORTCUT=0 makes the device evaluate the table sound speed
+ * everywhere (the results are the same) */
 static inline vh::DevEos dev_eos(const vh_event *ev)
 {
     vh::DevEos E;
@@ -94,6 +105,7 @@ static inline vh::DevEos dev_eos(const vh_event *ev)
     E.e_min = ev->heos.e_min;
     E.e_spacing = ev->heos.e_spacing;
     E.inv_spacing = 1.0 / ev->heos.e_spacing;
+    E.cs2_third_hi = (ev->cfg.eos_kind == VH_EOS_TABLE && !vh_env_off("VH_CS2_SHORTCUT")) ? ev->heos.cs2_third_hi : -INFINITY;
     E.pq.keys = ev->powf.keys;
     E.pq.vals = ev->powf.vals;
     E.pq.bucket = ev->powf.bucket;

@@ -25,6 +25,7 @@ struct DevEos {
     int e_length;
     double e_min, e_spacing;
     double inv_spacing;       /* RN(1/e_spacing), for div_rcp */
+    double cs2_third_hi;      /* eos_cs2 is exactly 1/3 for e <= this (HostEos::cs2_third_bound) */
     PowfTab pq;               /* host-exact powf(x, 0.25) */
 };
 
@@ -83,6 +84,7 @@ __device__ __forceinline__ double eos_cs2(const DevEos &E, double ed)        /* 
 {
     if (EOS == 1) {
         const double v_min = 0.01, v_max = 1. / 3.;
+        if (ed <= E.cs2_third_hi) return v_max;    /* the clamp's value, proven for this table */
         double pp = eos_p<1>(E, ed);
         double p_r = eos_p<1>(E, ed + E.e_spacing);
         double v = E.e_spacing / (p_r - pp);

@@ -34,7 +34,46 @@ void HostEos::init(const vh_config &cfg, const double *rows, int nrows)
             p_tb[ii] = rows[4 * ii + 1] / kHbarc;
             T_tb[ii] = rows[4 * ii + 3] / kHbarc;
         }
+        cs2_third_hi = cs2_third_bound();
     }
+}
+
+/* The table sound speed of the reference, e_spacing / (p(e + e_spacing) -
+ * p(e)) clamped to [0.01, 1/3] (EquationOfState.cpp:109-160), is exactly the
+ * clamp's 1/3 wherever the computed pressure step dp = p(e + de) - p(e) lies
+ * in [0, 3 de): the quotient is then above 1/3 or +inf.  If the pressure
+ * column rises with every segment slope in (0, 2.9], the exact step of the
+ * interpolation (the last segment extrapolated above the table, the first
+ * one below it, both floored at 1e-15, which is monotone) lies in
+ * [0, 2.9 de], and the computed one differs from it by the rounding of the
+ * interpolation, which grows with e.  This returns the largest e (four table
+ * lengths, or the table's end) at which that rounding stays below 1 % of the
+ * smallest exact step, or -inf when the table lacks these properties; up to
+ * that e the device takes 1/3 without evaluating the expression, with
+ * identical results, and evaluates it beyond. */
+double HostEos::cs2_third_bound() const
+{
+    const int N = e_length;
+    if (N < 2 || !(e_spacing > 0) || !(p_tb[0] >= 0)) return -INFINITY;
+    double smin = INFINITY, smax = -INFINITY, pmax = 0;
+    for (int i = 0; i + 1 < N; ++i) {
+        const double sl = (p_tb[i + 1] - p_tb[i]) / e_spacing;
+        smin = std::min(smin, sl);
+        smax = std::max(smax, sl);
+    }
+    for (int i = 0; i < N; ++i) pmax = std::max(pmax, std::fabs(p_tb[i]));
+    if (!(smin > 0) || !(smax <= 2.9) || !std::isfinite(pmax)) return -INFINITY;
+    auto ulp = [](double x) { x = std::fabs(x); return std::nextafter(x, INFINITY) - x; };
+    for (double lengths : {4.0, 1.0}) {
+        const double hi = e_min + lengths * (N - 1) * e_spacing;
+        /* |frac| + 1 bounds the interpolation weights for e in [e_min, hi + de];
+         * below e_min the pressure is floored long before the weights grow */
+        const double w = (hi + e_spacing - e_min) / e_spacing + 2;
+        const double M = pmax * 2 * w;                        /* largest product and sum */
+        const double err = 2 * (4 * ulp(M) + smax * 2 * ulp(hi + e_spacing)) + ulp(smax * e_spacing);
+        if (err <= 0.01 * smin * e_spacing) return hi;
+    }
+    return -INFINITY;
 }
 
 /* EquationOfState.cpp:329-360 */
@@ -120,6 +159,7 @@ double vh_eos_eval(const vh_config *cfg, const double *rows, int nrows, int what
     case 0: return eos.pressure(x);
     case 1: return eos.cs2(x);
     case 2: return eos.temperature(x);
+    case 4: return eos.kind == VH_EOS_TABLE ? eos.cs2_third_hi : -INFINITY;
     default: return eos.energy_of_T(x);
     }
 }

@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <string>
+#include <cmath>
 #include <vector>
 #include "vh_b200.h"
 
@@ -25,11 +26,15 @@ struct HostEos {
     int e_length = 0;
     double e_min = 0, e_max = 0, e_spacing = 1;
     std::vector<double> p_tb, T_tb;
+    /* the table sound speed is exactly 1/3 for every e <= cs2_third_hi
+     * (-inf: no such bound is known for this table); see cs2_third_bound */
+    double cs2_third_hi = -INFINITY;
 
     void init(const vh_config &cfg, const double *rows, int nrows);
     double interp(double ed, const std::vector<double> &tb) const;
     double pressure(double ed) const;
     double cs2(double ed) const;
+    double cs2_third_bound() const;
     double temperature(double ed) const;
     double energy_of_T(double T) const;
 };

@@ -392,7 +392,9 @@ int vh_eos_synthetic_table(int nrows, double T_lo_GeV, double e_max_GeV, double 
                            double dip, double Tc_GeV, double w_GeV, double *rows);
 
 /* Host copy of the reference EoS functions for a given configuration and
- * table (EquationOfState.cpp:44-290). what: 0 p(e), 1 cs2(e), 2 T(e), 3 e(T). */
+ * table (EquationOfState.cpp:44-290). what: 0 p(e), 1 cs2(e), 2 T(e), 3 e(T);
+ * 4: the energy density up to which the table's cs2 is exactly 1/3, so that
+ * the kernels skip its evaluation there (-inf: no such bound; x unused). */
 double vh_eos_eval(const vh_config *cfg, const double *eos_rows, int eos_nrows, int what, double x);
 
 /* Viscous Gubser flow at proper time t0 (2+1D, nz = 1): e, p [fm^-4],

@@ -132,3 +132,35 @@ def test_initial_conditions():
     h2 = vh.hotspot_ic(vh.gubser_config(61, 61), None, seed=7)
     h3 = vh.hotspot_ic(vh.gubser_config(61, 61), None, seed=8)
     assert np.array_equal(h1.e, h2.e) and not np.array_equal(h1.e, h3.e)
+
+
+def test_table_sound_speed_is_one_third_up_to_the_bound():
+    """the kernels take the table sound speed as 1/3 without evaluating it up
+    to the bound the library proves for the table (vh_eos_eval what = 4): the
+    oracle's full evaluation of the reference's expression gives exactly 1/3
+    on a dense sample up to that bound -- at the table's nodes, between them,
+    below the table where the pressure is floored and above it where the last
+    segment is extrapolated -- and tables without the properties the proof
+    needs (rising pressure, slopes in (0, 2.9]) get no bound"""
+    rows = vh.synthetic_eos_table()
+    cfg = vh.glauber_config(9, 9, 3)
+    hi = vh.eos_eval(cfg, rows, 4, 0.0)
+    e = rows[:, 0] / 0.197326938
+    d = e[1] - e[0]
+    assert hi >= e[-1]
+    orc = O.OracleEvent(cfg, rows)
+    rng = np.random.default_rng(7)
+    xs = np.concatenate([rng.uniform(-1e3, hi, 100000), np.geomspace(1e-12, hi, 5000), e, e + d / 2,
+                         e + d * (1 - 1e-12), e[-1] + d * np.arange(1, 200), [hi, -1e6, 0.0, 1e-300]])
+    cs = np.array([orc.L.vho_eos_cs2(orc.h, float(x)) for x in xs])
+    assert np.count_nonzero(cs != 1.0 / 3.0) == 0
+    for bad in ("flat", "falling", "steep"):
+        r = rows.copy()
+        if bad == "flat":
+            r[700, 1] = r[699, 1]
+        elif bad == "falling":
+            r[700, 1] = r[699, 1] * 0.999
+        else:
+            r[:, 1] *= 10.0
+        assert vh.eos_eval(cfg, r, 4, 0.0) == -np.inf, bad
+    assert vh.eos_eval(vh.gubser_config(9, 9), None, 4, 0.0) == -np.inf

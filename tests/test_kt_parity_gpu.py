@@ -210,3 +210,42 @@ def test_regulation_factors_bitexact(case):
         a, b = vh.interior(cfg, gpu.field(f)), vh.interior(cfg, orc.field(f))
         assert np.count_nonzero(np.ascontiguousarray(a).view(np.uint64) !=
                                 np.ascontiguousarray(b).view(np.uint64)) == 0, (case, f)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_table_sound_speed_shortcut_is_exact(precision, monkeypatch):
+    """the kernels take the table sound speed as 1/3 up to the bound the
+    library proves for the table; with the shortcut off (VH_CS2_SHORTCUT=0,
+    read when a step is issued) the source terms and root solves evaluate the
+    reference's expression everywhere, and every value is the same bit for bit
+    -- single events (split stage) and batch members"""
+    cfg = vh.glauber_config(41, 37, 23)
+    cfg.dx = cfg.dy = 0.5
+    cfg.dz = 0.4
+    cfg.dt = 0.05
+    if precision == "mixed":
+        cfg = cfg.copy(precision=vh.VH_PREC_MIXED)
+    rows = vh.synthetic_eos_table()
+    st = vh.glauber_ic(cfg, rows, b=4.0)
+    h = vh.hotspot_config(27).copy(precision=cfg.precision)
+    hst = vh.hotspot_ic(h, rows, seed=3)
+
+    def run():
+        ev = vh.Event(cfg, rows)
+        ev.set_initial(st)
+        ev.step(8)
+        ev.sync()
+        m = vh.Event(h, rows)
+        m.set_initial(hst)
+        b = vh.Batch([m])
+        b.step(6)
+        m.sync()
+        b.close()
+        return ev, m
+
+    a, am = run()
+    monkeypatch.setenv("VH_CS2_SHORTCUT", "0")
+    b, bm = run()
+    assert a.launches_per_step() == 10
+    assert not {f: n for f in FIELDS_15 if (n := _bitdiff(cfg, a.field(f), b.field(f)))}
+    assert not {f: n for f in FIELDS_15 if (n := _bitdiff(h, am.field(f), bm.field(f)))}
