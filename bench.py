@@ -62,7 +62,7 @@ def phase_words(nq):
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
 # ncu captures kept in profiles/kt_stage_kernels_glauber_131x131x61.md and
 # profiles/kt_flux_face_kernel_glauber_131x131x61_mixed.md
-NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 387.00e6, ("glauber_3p1d", "fp64", "source"): 336.17e6,
+NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 387.84e6, ("glauber_3p1d", "fp64", "source"): 336.17e6,
                ("glauber_3p1d", "mixed", "flux"): 388.30e6, ("glauber_3p1d", "mixed", "source"): 322.01e6}
 
 
