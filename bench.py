@@ -265,7 +265,7 @@ def run_serve(args, rank):
             "latency_s": {"p50": pct(lat, 50), "p95": pct(lat, 95), "p99": pct(lat, 99), "max": max(lat)},
             "cell_updates_per_s": cells / span,
             "server": {k: stats[k] for k in ("steps", "fo_blocks", "batch_builds", "t_admit_s", "t_build_s",
-                                             "t_step_s", "t_fo_s", "t_fo_copy_s", "fo_elements")} | {"events_with_device_error": bad},
+                                             "t_step_s", "t_fo_s", "t_fo_copy_s", "fo_elements", "t_retire_s", "t_wait_s")} | {"events_with_device_error": bad},
             "serial_plain_fp64": {"events_per_s": len(stream) / serial_span,
                                   "latency_s": {"p50": pct(slat, 50), "p95": pct(slat, 95), "p99": pct(slat, 99)},
                                   "events_with_device_error": serial_bad,

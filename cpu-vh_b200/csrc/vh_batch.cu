@@ -415,14 +415,14 @@ int autotune(vh_batch *b)
                 t.fused = 0;
                 launch_stage(b, 0, t, &mk[used++]);
                 t.fused = 1;
-                launch_stage(b, 0, t, &mk[used++]);
+                if (!b->mixed) launch_stage(b, 0, t, &mk[used++]);
             }
         BTRY(cudaGetLastError());
         BTRY(cudaStreamSynchronize(b->stream));
         /* best[phase] over candidates: min over rounds */
         size_t k = first;
         for (int cnd = 0; cnd < ncand; ++cnd)
-            for (int f = 0; f < 2; ++f) {
+            for (int f = 0; f < (b->mixed ? 1 : 2); ++f) {
                 const vh::StageMarks &m = mk[k++];
                 for (int n = 0; n < m.n; ++n) {
                     float ms = 0;
@@ -430,14 +430,19 @@ int autotune(vh_batch *b)
                     if (ms < best[m.phase[n]]) { best[m.phase[n]] = ms; best_c[m.phase[n]] = cnd; }
                 }
             }
-        if (best[VH_PHASE_FUSED] > 2.0) break;
+        const double split_ms = best[VH_PHASE_SOURCE] + best[VH_PHASE_FLUX_X] + best[VH_PHASE_FLUX_Y] +
+                                best[VH_PHASE_FINAL] + (b->any_z ? best[VH_PHASE_FLUX_ETA] : 0.0);
+        if (std::min(best[VH_PHASE_FUSED], split_ms) > 2.0) break;
     }
     for (auto &m : mk)
         for (cudaEvent_t e : m.ev) cudaEventDestroy(e);
     double split = best[VH_PHASE_SOURCE] + best[VH_PHASE_FLUX_X] + best[VH_PHASE_FLUX_Y] + best[VH_PHASE_FINAL] +
                    (b->any_z ? best[VH_PHASE_FLUX_ETA] : 0.0);
     vh_batch_tuning t{};
-    t.fused = best[VH_PHASE_FUSED] < split ? 1 : 0;
+    /* a mixed batch keeps the split stage: its face-once flux and the fused
+     * stage's per-cell flux round differently, and a batch's results must not
+     * depend on which of two close timings won */
+    t.fused = (!b->mixed && best[VH_PHASE_FUSED] < split) ? 1 : 0;
     for (int ph = 0; ph < VH_NPHASES; ++ph) {
         const int c = best_c[ph];
         t.tile_x[ph] = kShapes[c / 2][0];

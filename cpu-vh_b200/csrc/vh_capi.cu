@@ -68,6 +68,59 @@ int device_powf(int dev, vh::DevPowf *out)
     return VH_OK;
 }
 
+/* Device memory of events comes from a stream-ordered pool per device that
+ * keeps freed memory mapped: events that come and go (the server retires
+ * and admits them continually) reuse it, without cudaFree's unmapping and
+ * device-wide synchronisation.  The pool is trimmed when the last event on
+ * the device is destroyed, so an idle process holds nothing. */
+struct EventPool {
+    cudaMemPool_t pool = nullptr;
+    int live = 0;
+};
+std::mutex g_pool_mu;
+std::map<int, EventPool> g_pools;
+
+cudaError_t pool_of(int dev, cudaMemPool_t *out)
+{
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    EventPool &P = g_pools[dev];
+    if (!P.pool) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaError_t e = cudaMemPoolCreate(&P.pool, &props);
+        if (e != cudaSuccess) { P.pool = nullptr; return e; }
+        unsigned long long keep = ~0ULL;
+        e = cudaMemPoolSetAttribute(P.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        if (e != cudaSuccess) return e;
+    }
+    *out = P.pool;
+    return cudaSuccess;
+}
+
+void pool_live(int dev, int delta)
+{
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    EventPool &P = g_pools[dev];
+    P.live += delta;
+    if (P.live == 0 && P.pool) cudaMemPoolTrimTo(P.pool, 0);
+}
+
+/* an event buffer, ordered on the event's stream */
+cudaError_t ev_alloc(vh_event *ev, void *ptr, size_t bytes)
+{
+    cudaMemPool_t pool = nullptr;
+    cudaError_t e = pool_of(ev->device, &pool);
+    if (e != cudaSuccess) return e;
+    return cudaMallocFromPoolAsync(reinterpret_cast<void **>(ptr), bytes, pool, ev->stream);
+}
+
+void ev_free(vh_event *ev, void *p)
+{
+    if (p) cudaFreeAsync(p, ev->stream);
+}
+
 } // namespace
 
 
@@ -103,24 +156,19 @@ int vh_device_available(void)
 int vh_event_destroy(vh_event *ev)
 {
     if (!ev) return VH_OK;
-    if (ev->stream) cudaStreamSynchronize(ev->stream);
-    cudaFree(ev->slab);
-    cudaFree(ev->tables);
-    cudaFree(ev->err);
-    cudaFree(ev->err_cell);
-    cudaFree(ev->powf_miss);
-    cudaFree(ev->ic);
-    cudaFree(ev->fo_slabs);
-    cudaFree(ev->fo_scratch);
-    cudaFree(ev->fo_elems);
+    if (ev->stream) {
+        for (double *p : {ev->slab, ev->tables, ev->ic, ev->fo_slabs, ev->fo_elems, ev->vort, ev->src, ev->regfac})
+            ev_free(ev, p);
+        for (void *p : {(void *)ev->err, (void *)ev->err_cell, (void *)ev->powf_miss, (void *)ev->fo_scratch})
+            ev_free(ev, p);
+        cudaStreamSynchronize(ev->stream);
+    }
     if (ev->fo_hdr) cudaFreeHost(ev->fo_hdr);
-    cudaFree(ev->vort);
-    cudaFree(ev->src);
-    cudaFree(ev->regfac);
     if (ev->fo_done) cudaEventDestroy(ev->fo_done);
     for (auto &m : ev->marks)
         for (cudaEvent_t e : m.ev) cudaEventDestroy(e);
     if (ev->stream) cudaStreamDestroy(ev->stream);
+    if (ev->pooled) pool_live(ev->device, -1);
     delete ev;
     return VH_OK;
 }
@@ -150,28 +198,30 @@ int vh_event_create(const vh_config *cfg, const double *eos_rows, int eos_nrows,
 #define TRY(x) do { cudaError_t e__ = (x); if (e__ != cudaSuccess) { rc = fail(e__ == cudaErrorMemoryAllocation ? VH_ERR_NOMEM : VH_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e__)); vh_event_destroy(ev); return rc; } } while (0)
     TRY(cudaGetDevice(&ev->device));
     TRY(cudaStreamCreateWithFlags(&ev->stream, cudaStreamNonBlocking));
+    pool_live(ev->device, 1);
+    ev->pooled = true;
     const long long planes = 3LL * ev->nq + 2 * 2 + 3 * 4;
-    TRY(cudaMalloc(&ev->slab, (size_t)(planes * ev->L) * sizeof(double)));
+    TRY(ev_alloc(ev, &ev->slab, (size_t)(planes * ev->L) * sizeof(double)));
     TRY(cudaMemsetAsync(ev->slab, 0, (size_t)(planes * ev->L) * sizeof(double), ev->stream));
     double *p = ev->slab;
     for (int b = 0; b < 3; ++b) { ev->q[b] = p; p += ev->nq * ev->L; }
     for (int b = 0; b < 2; ++b) { ev->ep[b] = p; p += 2 * ev->L; }
     for (int b = 0; b < 3; ++b) { ev->u[b] = p; p += 4 * ev->L; }
     if (cfg->eos_kind == VH_EOS_TABLE) {
-        TRY(cudaMalloc(&ev->tables, 2 * (size_t)eos_nrows * sizeof(double)));
+        TRY(ev_alloc(ev, &ev->tables, 2 * (size_t)eos_nrows * sizeof(double)));
         TRY(cudaMemcpyAsync(ev->tables, ev->heos.p_tb.data(), eos_nrows * sizeof(double), cudaMemcpyHostToDevice, ev->stream));
         TRY(cudaMemcpyAsync(ev->tables + eos_nrows, ev->heos.T_tb.data(), eos_nrows * sizeof(double), cudaMemcpyHostToDevice, ev->stream));
     } else {
         rc = device_powf(ev->device, &ev->powf);
         if (rc != VH_OK) { vh_event_destroy(ev); return rc; }
     }
-    TRY(cudaMalloc(&ev->err, 2 * sizeof(int)));
-    TRY(cudaMalloc(&ev->err_cell, sizeof(long long)));
-    TRY(cudaMalloc(&ev->powf_miss, sizeof(unsigned long long)));
+    TRY(ev_alloc(ev, &ev->err, 2 * sizeof(int)));
+    TRY(ev_alloc(ev, &ev->err_cell, sizeof(long long)));
+    TRY(ev_alloc(ev, &ev->powf_miss, sizeof(unsigned long long)));
     TRY(cudaMemsetAsync(ev->err, 0, 2 * sizeof(int), ev->stream));
     TRY(cudaMemsetAsync(ev->err_cell, 0, sizeof(long long), ev->stream));
     TRY(cudaMemsetAsync(ev->powf_miss, 0, sizeof(unsigned long long), ev->stream));
-    TRY(cudaMalloc(&ev->ic, (size_t)(17 * ev->N) * sizeof(double)));
+    TRY(ev_alloc(ev, &ev->ic, (size_t)(17 * ev->N) * sizeof(double)));
     TRY(cudaStreamSynchronize(ev->stream));
 #undef TRY
     *out = ev;
@@ -417,7 +467,7 @@ int vh_event_set_sources(vh_event *ev, const double *st, const double *sx, const
     const size_t N = (size_t)ev->N, B = N * sizeof(double);
     if (!ev->src) {
         const size_t P = (size_t)4 * ev->L * sizeof(double);
-        CUDA_TRY(cudaMalloc(&ev->src, P));
+        CUDA_TRY(ev_alloc(ev, &ev->src, P));
         CUDA_TRY(cudaMemsetAsync(ev->src, 0, P, ev->stream));
     }
     /* through the initial-condition staging planes (free between initial states) */
@@ -438,7 +488,7 @@ int vh_event_keep_regulation(vh_event *ev, int enable)
     ev->regfac_on = enable != 0;
     if (ev->regfac_on && !ev->regfac) {
         const size_t P = (size_t)2 * ev->L * sizeof(double);
-        CUDA_TRY(cudaMalloc(&ev->regfac, P));
+        CUDA_TRY(ev_alloc(ev, &ev->regfac, P));
         CUDA_TRY(cudaMemsetAsync(ev->regfac, 0, P, ev->stream));   /* as calloc'd before the first step */
     }
     return VH_OK;
@@ -452,7 +502,7 @@ int vh_event_vorticity(vh_event *ev, int enable)
     if (!ev->vort_on) return VH_OK;
     if (!ev->vort) {
         const size_t B = (size_t)10 * ev->L * sizeof(double);
-        CUDA_TRY(cudaMalloc(&ev->vort, B));
+        CUDA_TRY(ev_alloc(ev, &ev->vort, B));
         CUDA_TRY(cudaMemsetAsync(ev->vort, 0, B, ev->stream));
     }
     launch_vort(ev);                              /* HydroPlugin.cpp:197-199 */
@@ -546,10 +596,10 @@ int vh_event_freezeout_launch(vh_event *ev)
     const vh_config &c = ev->cfg;
     const size_t N = (size_t)ev->N;
     if (!ev->fo_slabs) {
-        CUDA_TRY(cudaMalloc(&ev->fo_slabs, 2 * 11 * N * sizeof(double)));
+        CUDA_TRY(ev_alloc(ev, &ev->fo_slabs, 2 * 11 * N * sizeof(double)));
         CUDA_TRY(cudaMemsetAsync(ev->fo_slabs, 0, 2 * 11 * N * sizeof(double), ev->stream));
         ev->fo_scratch_ints = vh::freezeout_scratch_ints(c.nx, c.ny, c.nz);
-        CUDA_TRY(cudaMalloc(&ev->fo_scratch, ev->fo_scratch_ints * sizeof(int)));
+        CUDA_TRY(ev_alloc(ev, &ev->fo_scratch, ev->fo_scratch_ints * sizeof(int)));
         CUDA_TRY(cudaMallocHost(&ev->fo_hdr, 2 * sizeof(int)));
         CUDA_TRY(cudaEventCreateWithFlags(&ev->fo_done, cudaEventDisableTiming));
         /* a first element buffer sized for a surface crossing the lattice
@@ -561,7 +611,7 @@ int vh_event_freezeout_launch(vh_event *ev)
             long long cap = (nz > 1 ? 2 * (nx * ny + ny * nz + nx * nz) : 8 * (nx + ny)) + 1024;
             if (const char *env = getenv("VH_FO_INITIAL_CAP")) cap = std::max(1LL, atoll(env));
             ev->fo_cap = (int)std::min<long long>(cap, 1LL << 28);
-            CUDA_TRY(cudaMalloc(&ev->fo_elems, (size_t)ev->fo_cap * VH_FO_COLUMNS * sizeof(double)));
+            CUDA_TRY(ev_alloc(ev, &ev->fo_elems, (size_t)ev->fo_cap * VH_FO_COLUMNS * sizeof(double)));
         }
     }
     vh::FoArgs a;
@@ -585,10 +635,10 @@ int vh_event_freezeout_finish(vh_event *ev, int *n_elements, int *n_above)
     if (total > ev->fo_cap) {
         /* not enough room: a buffer with room to grow, and the emit step
          * again from the offsets the block left in the scratch */
-        cudaFree(ev->fo_elems);
+        ev_free(ev, ev->fo_elems);
         ev->fo_elems = nullptr;
         ev->fo_cap = total + total / 2 + 1024;
-        CUDA_TRY(cudaMalloc(&ev->fo_elems, (size_t)ev->fo_cap * VH_FO_COLUMNS * sizeof(double)));
+        CUDA_TRY(ev_alloc(ev, &ev->fo_elems, (size_t)ev->fo_cap * VH_FO_COLUMNS * sizeof(double)));
         vh::FoArgs a;
         fo_args(ev, a);
         vh::launch_freezeout_emit(a, ev->stream);

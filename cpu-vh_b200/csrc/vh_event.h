@@ -49,6 +49,7 @@ struct vh_event {
     int ec = 0;                           /* e/p buffer holding the current state */
     int uc = 0, up = 1, us = 2;           /* u, up, uS */
     double *tables = nullptr;             /* p_tb then T_tb */
+    bool pooled = false;                  /* counted in the device's event memory pool */
     int *err = nullptr;                   /* [0] code, [1] step */
     long long *err_cell = nullptr;
     unsigned long long *powf_miss = nullptr;

@@ -142,7 +142,6 @@ void finish_job(vh_server *S, std::unique_ptr<Job> &j, int status)
 {
     j->status = status;
     j->t_done = S->now();
-    j->surface.shrink_to_fit();
     if (j->ev) vh_event_destroy(j->ev);
     j->ev = nullptr;
     std::lock_guard<std::mutex> lk(S->mu);
@@ -215,7 +214,9 @@ void worker_main(vh_server *S)
         std::vector<std::unique_ptr<Job>> admitted;
         {
             std::unique_lock<std::mutex> lk(S->mu);
+            const auto t_w = tick();
             S->cv.wait(lk, [&] { return S->stop || !S->queue.empty() || !S->active.empty(); });
+            S->st.t_wait_s += std::chrono::duration<double>(Clock::now() - t_w).count();
             if (S->stop) break;
             /* admit where every member is fo_factor - 1 steps before its next
              * block, as a new event is: all blocks then fall in one round
@@ -398,6 +399,7 @@ void worker_main(vh_server *S)
             if (j->status != VH_OK || j->zero_blocks >= 3 || capped) retire.push_back(std::move(j));
             else keep.push_back(std::move(j));
         }
+        const auto t_ret = tick();
         for (auto &j : retire) {
             auto it = groups.find(group_key(j->cfg));
             if (it != groups.end() &&
@@ -410,6 +412,7 @@ void worker_main(vh_server *S)
             flush(j.get());
             finish_job(S, j, j->status);
         }
+        if (!retire.empty()) add(S->st.t_retire_s, t_ret);
         S->active.swap(keep);
     }
     for (auto &kv : groups) vh_batch_destroy(kv.second.batch);

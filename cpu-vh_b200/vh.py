@@ -450,7 +450,8 @@ class ServerStats(C.Structure):
                 ("done", C.c_longlong), ("steps", C.c_longlong), ("fo_blocks", C.c_longlong),
                 ("batch_builds", C.c_longlong), ("bytes_in_use", C.c_ulonglong), ("budget_bytes", C.c_ulonglong),
                 ("t_admit_s", C.c_double), ("t_build_s", C.c_double), ("t_step_s", C.c_double), ("t_fo_s", C.c_double),
-                ("t_fo_copy_s", C.c_double), ("fo_elements", C.c_longlong)]
+                ("t_fo_copy_s", C.c_double), ("fo_elements", C.c_longlong), ("t_retire_s", C.c_double),
+                ("t_wait_s", C.c_double)]
 
 
 _sig("vh_server_config_default", None, [C.POINTER(ServerConfig)])

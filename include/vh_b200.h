@@ -306,6 +306,8 @@ typedef struct vh_server_stats {
     double t_fo_s;           /*   freezeout blocks and surface copies              */
     double t_fo_copy_s;      /*     of which surface copies to host memory          */
     long long fo_elements;   /* freezeout elements collected                         */
+    double t_retire_s;       /*   retiring events (freeing their device memory)      */
+    double t_wait_s;         /*   idle, waiting for submissions                      */
 } vh_server_stats;
 
 void vh_server_config_default(vh_server_config *c);
