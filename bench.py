@@ -85,6 +85,8 @@ def parse():
                     help="mixed: FP32 limiter/flux/source arithmetic, FP64 accumulation and root solve")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--fo-blocks", type=int, default=4,
+                    help="freezeout blocks timed after the steps (0: none), one per fo_factor steps")
     return ap.parse_args()
 
 
@@ -363,6 +365,40 @@ def cpu_baseline(cfg, rows, st, variant, steps=2):
                       f"{threads} OpenMP threads" + (" (reference sources, -O3 -ffp-contract=off)" if kind == "reference"
                                                       else " (C restatement, 1 thread)"),
             "seconds": secs}
+
+
+def reference_freezeout(cfg, rows, variant):
+    """One freezeout block of the reference's own code (serial Cornelius scan
+    that writes its surface.dat lines, FreezeOut.cpp:200-361), timed on the
+    host clock after the first block and fo_factor more steps.  Its cost is
+    ~90 us per cell (~100 s for a 10^6-cell lattice), so it runs on a bounded
+    sample: the same event on a lattice of about 6e4 cells covering the same
+    volume, scaled to the full lattice by the cell count."""
+    import tempfile
+    import oracle as O
+    import vh
+    if variant != "table" or not O.ref_available(variant):
+        return None
+    N = cfg.nx * cfg.ny * cfg.nz
+    f = max(1.0, (N / 6e4) ** (1.0 / (3 if cfg.nz > 1 else 2)))
+    sc = cfg.copy(nx=max(8, int(round(cfg.nx / f))), ny=max(8, int(round(cfg.ny / f))),
+                  nz=max(1, int(round(cfg.nz / f))) if cfg.nz > 1 else 1)
+    sc.dx, sc.dy = cfg.dx * cfg.nx / sc.nx, cfg.dy * cfg.ny / sc.ny
+    sc.dz = cfg.dz * cfg.nz / sc.nz
+    ref = O.RefEvent(variant, sc, rows, threads=os.cpu_count() or 1)
+    ref.set_initial(vh.glauber_ic(sc, rows))
+    ref.step(2)
+    path = os.path.join(tempfile.gettempdir(), f"vh_ref_surface_{os.getpid()}.dat")
+    ref.freezeout(path)
+    ref.step(max(1, cfg.fo_factor))
+    t0 = time.perf_counter()
+    ref.freezeout(path)
+    secs = time.perf_counter() - t0
+    os.remove(path)
+    Ns = sc.nx * sc.ny * sc.nz
+    return {"ms_per_block": secs * 1e3 * N / Ns, "cores": 1, "kind": "reference",
+            "sample": f"one block on the same event at {sc.nx}x{sc.ny}x{sc.nz} ({secs:.2f} s), scaled by the "
+                      f"cell count to {cfg.nx}x{cfg.ny}x{cfg.nz}; serial, writes its surface.dat lines"}
 
 
 def run_reference(args):
@@ -653,6 +689,32 @@ def main():
     achieved = alg_bytes / launch_s / 1e9
     traffic = NCU_TRAFFIC.get((args.workload, args.precision, dom))
 
+    # freezeout at the event's cadence (run() calls it every fo_factor steps,
+    # HydroPlugin.cpp:249-266): device time of a block -- slab gather, the
+    # Cornelius cube scan, compaction, element emission and the count read
+    # back -- reported beside the step and combined with it
+    fo = None
+    if args.fo_blocks > 0:
+        fac = max(1, cfg.fo_factor)
+        ev.freezeout()                           # the first block compares against a zero slab: untimed
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fo_ms, fo_el = [], []
+        for _ in range(args.fo_blocks):
+            ev.step(fac)
+            ev.sync()
+            f0.record(stream)
+            ne, _ = ev.freezeout()
+            f1.record(stream)
+            f1.synchronize()
+            fo_ms.append(f0.elapsed_time(f1))
+            fo_el.append(ne)
+        ms_fo = max_over_ranks(sum(fo_ms) / len(fo_ms))
+        fo = {"ms_per_block": ms_fo, "elements_per_block": sum(fo_el) / len(fo_el), "blocks": len(fo_ms),
+              "fo_factor": fac, "cells_scanned_per_s": N * world / (ms_fo / 1e3),
+              "combined_cell_updates_per_s": N * fac * world / ((fac * ms_step + ms_fo) / 1e3),
+              "timer": "CUDA events around vh_event_freezeout on the event's stream (kernels and the "
+                       "element-count read-back); combined = one block per fo_factor steps"}
+
     e2e = None
     if not args.no_e2e:
         # pinned host buffers; one event = upload IC, K steps, download e
@@ -691,6 +753,8 @@ def main():
     base = None
     if rank == 0 and world == 1 and not args.no_baseline:
         base = cpu_baseline(cfg, rows, st, variant)
+        if fo is not None:
+            fo["reference"] = reference_freezeout(cfg, rows, variant)
 
     if rank == 0:
         line = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": world,
@@ -711,6 +775,8 @@ def main():
                 "clocks": clk, "gpu_launches": ev.launches_per_step() * args.steps}
         if prec:
             line["precision_error"] = prec
+        if fo:
+            line["freezeout"] = fo
         if e2e:
             line["e2e"] = e2e
         if base:

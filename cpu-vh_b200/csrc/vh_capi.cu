@@ -157,7 +157,8 @@ int vh_event_destroy(vh_event *ev)
 {
     if (!ev) return VH_OK;
     if (ev->stream) {
-        for (double *p : {ev->slab, ev->tables, ev->ic, ev->fo_slabs, ev->fo_elems, ev->vort, ev->src, ev->regfac})
+        for (double *p : {ev->slab, ev->tables, ev->ic, ev->fo_slabs, ev->fo_elems, ev->fo_slots, ev->vort, ev->src,
+                          ev->regfac})
             ev_free(ev, p);
         for (void *p : {(void *)ev->err, (void *)ev->err_cell, (void *)ev->powf_miss, (void *)ev->fo_scratch})
             ev_free(ev, p);
@@ -586,6 +587,8 @@ static void fo_args(vh_event *ev, vh::FoArgs &a)
     a.n_total = nullptr;
     a.elems = ev->fo_elems;
     a.cap = ev->fo_cap;
+    a.slots = ev->fo_slots;
+    a.slot_cap = ev->fo_slot_cap;
 }
 
 int vh_event_freezeout_launch(vh_event *ev)
@@ -612,6 +615,10 @@ int vh_event_freezeout_launch(vh_event *ev)
             if (const char *env = getenv("VH_FO_INITIAL_CAP")) cap = std::max(1LL, atoll(env));
             ev->fo_cap = (int)std::min<long long>(cap, 1LL << 28);
             CUDA_TRY(ev_alloc(ev, &ev->fo_elems, (size_t)ev->fo_cap * VH_FO_COLUMNS * sizeof(double)));
+            /* element slots for as many crossed cubes as the first buffer has
+             * elements (a cube beyond them runs Cornelius again in the emit step) */
+            ev->fo_slot_cap = ev->fo_cap;
+            CUDA_TRY(ev_alloc(ev, &ev->fo_slots, (size_t)ev->fo_slot_cap * vh::kFoSlotDoubles * sizeof(double)));
         }
     }
     vh::FoArgs a;

@@ -67,6 +67,8 @@ struct vh_event {
     size_t fo_scratch_ints = 0;
     double *fo_elems = nullptr;
     int fo_cap = 0;
+    double *fo_slots = nullptr;           /* element slots of the count step (vh_fo.cu) */
+    int fo_slot_cap = 0;
     int fo_count = 0;
     int *fo_hdr = nullptr;                /* pinned: n_above, n_total of the last block */
     cudaEvent_t fo_done = nullptr;

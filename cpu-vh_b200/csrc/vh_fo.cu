@@ -230,6 +230,15 @@ __device__ int cube_surface(const FoArgs &a, int ix, int iy, int iz, cor::Work &
     return cor::surface_3d(w, cb, a.eF, dx3, cen, nor);
 }
 
+/* element slots: the centroids and normals the count step finds for the
+ * first slot_cap crossed cubes, kept for the emit step (8 doubles per
+ * element, kMaxElements per cube) so that it need not run Cornelius again:
+ * the per-thread Cornelius work area (~13 KB) is what the emit step's DRAM
+ * traffic was made of */
+static_assert(cor::kMaxHedra <= cor::kMaxElements && cor::kMaxElements * 8 == kFoSlotDoubles,
+              "a cube's elements fit its slot");
+constexpr int kSlotDoubles = kFoSlotDoubles;
+
 __global__ void __launch_bounds__(128) fo_count_kernel(const __grid_constant__ FoArgs a, FoScratch sc)
 {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -243,6 +252,11 @@ __global__ void __launch_bounds__(128) fo_count_kernel(const __grid_constant__ F
     int ne = cube_surface(a, ix, iy, iz, w, cen, nor);
     if (ne < 0) { raise_error(a.err, 5, sc.list[i], a.n); ne = 0; }
     sc.counts[i] = ne;
+    if (i < a.slot_cap) {
+        double *o = a.slots + i * kSlotDoubles;
+        for (int k = 0; k < ne; k++)
+            for (int d = 0; d < 4; d++) { o[8 * k + d] = cen[k][d]; o[8 * k + 4 + d] = nor[k][d]; }
+    }
 }
 
 /* FreezeOut.cpp:40-55 */
@@ -268,6 +282,59 @@ __device__ __forceinline__ double interp4(double x0, double x1, double x2, doubl
            ((1 - x0) * (x1) * (x2) * (x3) * c[7]) + ((x0) * (x1) * (x2) * (x3) * c[15]);
 }
 
+/* FreezeOut.cpp:200-361, per element: position, tau-scaled normal, the ten
+ * interpolated fields, T and P */
+template <int EOS>
+__device__ __forceinline__ void emit_element(const FoArgs &a, int ix, int iy, int iz, const double *cen,
+                                             const double *nor, double *__restrict__ o)
+{
+    const bool four = a.nz > 1;
+    const double cell_tau = a.t0 + ((double)a.n) * a.dt;
+    const double cell_x = (double)ix * a.dx - (((double)(a.nx - 1)) / 2.0 * a.dx);
+    const double cell_y = (double)iy * a.dy - (((double)(a.ny - 1)) / 2.0 * a.dy);
+    double f[10];
+    if (four) {
+        const double cell_z = (double)iz * a.dz - (((double)(a.nz - 1)) / 2.0 * a.dz);
+        const double tf = cen[0] / a.dtau_c, xf = cen[1] / a.dx, yf = cen[2] / a.dy, zf = cen[3] / a.dz;
+        for (int v = 0; v < 10; v++) {
+            double c[16];
+            for (int t = 0; t < 2; t++) for (int bx = 0; bx < 2; bx++) for (int by = 0; by < 2; by++) for (int bz = 0; bz < 2; bz++)
+                c[t * 8 + bx * 4 + by * 2 + bz] = slab(a, t, v + 1, ix + bx, iy + by, iz + bz);
+            f[v] = interp4(tf, xf, yf, zf, c);
+        }
+        o[0] = cen[0] + cell_tau; o[1] = cen[1] + cell_x; o[2] = cen[2] + cell_y; o[3] = cen[3] + cell_z;
+        o[4] = a.t * nor[0]; o[5] = a.t * nor[1]; o[6] = a.t * nor[2]; o[7] = a.t * nor[3];
+    } else {
+        const double tf = cen[1] / a.dtau_c, xf = cen[2] / a.dx, yf = cen[3] / a.dy;
+        for (int v = 0; v < 10; v++)
+            f[v] = interp3(tf, xf, yf, slab(a, 0, v + 1, ix, iy, 0), slab(a, 1, v + 1, ix, iy, 0),
+                           slab(a, 0, v + 1, ix + 1, iy, 0), slab(a, 0, v + 1, ix, iy + 1, 0),
+                           slab(a, 1, v + 1, ix + 1, iy, 0), slab(a, 1, v + 1, ix, iy + 1, 0),
+                           slab(a, 0, v + 1, ix + 1, iy + 1, 0), slab(a, 1, v + 1, ix + 1, iy + 1, 0));
+        o[0] = cen[1] + cell_tau; o[1] = cen[2] + cell_x; o[2] = cen[3] + cell_y; o[3] = 0.0;
+        o[4] = a.t * nor[1]; o[5] = a.t * nor[2]; o[6] = a.t * nor[3]; o[7] = 0.0;
+    }
+    o[8] = f[0]; o[9] = f[1]; o[10] = f[2];
+    o[11] = f[3];
+    o[12] = eos_T<EOS>(a.eos, f[3]);
+    o[13] = eos_p<EOS>(a.eos, f[3]);
+    o[14] = f[4]; o[15] = f[5]; o[16] = f[6]; o[17] = f[7]; o[18] = f[8];
+    o[19] = f[9];
+}
+
+/* a crossed cube beyond the slots: Cornelius again, as the count step ran it */
+template <int EOS>
+static __device__ __noinline__ void emit_recompute(const FoArgs &a, int ix, int iy, int iz, long long off)
+{
+    cor::Work w;
+    double cen[cor::kMaxHedra][4], nor[cor::kMaxHedra][4];
+    const int ne = cube_surface(a, ix, iy, iz, w, cen, nor);
+    for (int k = 0; k < ne; k++) {
+        if (off + k >= a.cap) return;
+        emit_element<EOS>(a, ix, iy, iz, cen[k], nor[k], a.elems + (off + k) * VH_FO_COLUMNS);
+    }
+}
+
 template <int EOS>
 __global__ void __launch_bounds__(128) fo_emit_kernel(const __grid_constant__ FoArgs a, FoScratch sc)
 {
@@ -275,46 +342,13 @@ __global__ void __launch_bounds__(128) fo_emit_kernel(const __grid_constant__ Fo
     if (i >= sc.nc || i >= sc.hdr[0]) return;
     int ix, iy, iz;
     cube_coords(a, sc.list[i], ix, iy, iz);
-    cor::Work w;
-    double cen[cor::kMaxHedra][4], nor[cor::kMaxHedra][4];
-    const int ne = cube_surface(a, ix, iy, iz, w, cen, nor);
-    if (ne <= 0) return;
-    const bool four = a.nz > 1;
     const long long off = sc.counts[i];
+    if (i >= a.slot_cap) { emit_recompute<EOS>(a, ix, iy, iz, off); return; }
+    const int ne = sc.counts[i + 1] - sc.counts[i];
+    const double *sl = a.slots + i * kSlotDoubles;
     for (int k = 0; k < ne; k++) {
         if (off + k >= a.cap) return;
-        double *o = a.elems + (off + k) * VH_FO_COLUMNS;
-        const double cell_tau = a.t0 + ((double)a.n) * a.dt;
-        const double cell_x = (double)ix * a.dx - (((double)(a.nx - 1)) / 2.0 * a.dx);
-        const double cell_y = (double)iy * a.dy - (((double)(a.ny - 1)) / 2.0 * a.dy);
-        double f[10];
-        if (four) {
-            const double cell_z = (double)iz * a.dz - (((double)(a.nz - 1)) / 2.0 * a.dz);
-            const double tf = cen[k][0] / a.dtau_c, xf = cen[k][1] / a.dx, yf = cen[k][2] / a.dy, zf = cen[k][3] / a.dz;
-            for (int v = 0; v < 10; v++) {
-                double c[16];
-                for (int t = 0; t < 2; t++) for (int bx = 0; bx < 2; bx++) for (int by = 0; by < 2; by++) for (int bz = 0; bz < 2; bz++)
-                    c[t * 8 + bx * 4 + by * 2 + bz] = slab(a, t, v + 1, ix + bx, iy + by, iz + bz);
-                f[v] = interp4(tf, xf, yf, zf, c);
-            }
-            o[0] = cen[k][0] + cell_tau; o[1] = cen[k][1] + cell_x; o[2] = cen[k][2] + cell_y; o[3] = cen[k][3] + cell_z;
-            o[4] = a.t * nor[k][0]; o[5] = a.t * nor[k][1]; o[6] = a.t * nor[k][2]; o[7] = a.t * nor[k][3];
-        } else {
-            const double tf = cen[k][1] / a.dtau_c, xf = cen[k][2] / a.dx, yf = cen[k][3] / a.dy;
-            for (int v = 0; v < 10; v++)
-                f[v] = interp3(tf, xf, yf, slab(a, 0, v + 1, ix, iy, 0), slab(a, 1, v + 1, ix, iy, 0),
-                               slab(a, 0, v + 1, ix + 1, iy, 0), slab(a, 0, v + 1, ix, iy + 1, 0),
-                               slab(a, 1, v + 1, ix + 1, iy, 0), slab(a, 1, v + 1, ix, iy + 1, 0),
-                               slab(a, 0, v + 1, ix + 1, iy + 1, 0), slab(a, 1, v + 1, ix + 1, iy + 1, 0));
-            o[0] = cen[k][1] + cell_tau; o[1] = cen[k][2] + cell_x; o[2] = cen[k][3] + cell_y; o[3] = 0.0;
-            o[4] = a.t * nor[k][1]; o[5] = a.t * nor[k][2]; o[6] = a.t * nor[k][3]; o[7] = 0.0;
-        }
-        o[8] = f[0]; o[9] = f[1]; o[10] = f[2];
-        o[11] = f[3];
-        o[12] = eos_T<EOS>(a.eos, f[3]);
-        o[13] = eos_p<EOS>(a.eos, f[3]);
-        o[14] = f[4]; o[15] = f[5]; o[16] = f[6]; o[17] = f[7]; o[18] = f[8];
-        o[19] = f[9];
+        emit_element<EOS>(a, ix, iy, iz, sl + 8 * k, sl + 8 * k + 4, a.elems + (off + k) * VH_FO_COLUMNS);
     }
 }
 

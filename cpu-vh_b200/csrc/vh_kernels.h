@@ -132,8 +132,14 @@ struct FoArgs {
     int *n_above;                /* cells above eF */
     double *elems;               /* output, VH_FO_COLUMNS per element */
     int cap;                     /* capacity of elems in elements */
+    double *slots;               /* centroids and normals of the first slot_cap crossed cubes */
+    int slot_cap;
     int *n_total;
 };
+
+/* doubles of one crossed cube's element slot: up to 10 elements (Cornelius
+ * MAX_ELEMENTS), centroid and normal (4 + 4) each */
+constexpr int kFoSlotDoubles = 80;
 
 /* Runs the whole freezeout block; returns the number of elements through
  * *a.n_total (device) and leaves elements in a.elems. */
