@@ -66,6 +66,14 @@ NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 387.84e6, ("glauber_3p1d", "fp6
                ("glauber_3p1d", "mixed", "flux"): 388.30e6, ("glauber_3p1d", "mixed", "source"): 322.01e6}
 
 
+# batched flux launches: DRAM bytes per cell from ncu captures of the same
+# batch cut to its first 64 events (1 312 264 cells), scaled by the cell count
+# (the traffic of a launch is per cell: each member's stencil once), from
+# profiles/kt_batch_kernel_hotspots_64ev_fp64.md and
+# profiles/kt_batch_face_kernel_hotspots_64ev_mixed.md
+NCU_TRAFFIC_PER_CELL = {("fp64", "flux"): 371.7, ("mixed", "flux"): 371.6}
+
+
 KERNEL_NAMES = {"source": "kt_source_kernel", "flux": "kt_flux_staged_kernel (x, y, eta)",
                 "final": "kt_final_kernel", "fused": "kt_stage_kernel"}
 
@@ -594,7 +602,9 @@ def run_batch(args, torch, world, rank, barrier, max_over_ranks):
                                        "how": f"FP64 vh_event_step, one event at a time, {solo_steps} steps each, "
                                               "CUDA events per event"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": None,
+                             "frac": achieved / peak,
+                             "traffic": (NCU_TRAFFIC_PER_CELL[(args.precision, dom)] * Ntot
+                                         if (args.precision, dom) in NCU_TRAFFIC_PER_CELL else None),
                              "kernel": ("kt_batch_face_kernel " if mixed and dom == "flux" else "kt_batch_kernel ") + dom,
                              "launches": dom_n,
                              "launch_us": launch_s * 1e6, "algorithmic_bytes": alg_bytes,
