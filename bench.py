@@ -74,6 +74,13 @@ NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 387.84e6, ("glauber_3p1d", "fp6
 NCU_TRAFFIC_PER_CELL = {("fp64", "flux"): 371.7, ("mixed", "flux"): 371.6}
 
 
+# steps of the mixed-precision error report: the Gubser event to its end
+# (tau = 4 fm/c); the Glauber event to tau = 12.6 fm/c (800 steps) -- at step
+# 909 its FP64 evolution, bit-identical to the reference's, trips the
+# reference's NaN guard (EnergyMomentumTensor.cpp:197-203) in the dilute edge
+PRECISION_STEPS = {"gubser_2p1d": 300, "glauber_3p1d": 800}
+
+
 KERNEL_NAMES = {"source": "kt_source_kernel", "flux": "kt_flux_staged_kernel (x, y, eta)",
                 "final": "kt_final_kernel", "fused": "kt_stage_kernel"}
 
@@ -93,6 +100,8 @@ def parse():
                     help="mixed: FP32 limiter/flux/source arithmetic, FP64 accumulation and root solve")
     ap.add_argument("--no-baseline", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--precision-steps", type=int, default=0,
+                    help="--precision mixed: steps of the error report (0: the workload's whole event)")
     ap.add_argument("--fo-blocks", type=int, default=4,
                     help="freezeout blocks timed after the steps (0: none), one per fo_factor steps")
     return ap.parse_args()
@@ -133,12 +142,15 @@ def batch_workload(n_events):
     return cfgs, rows, ics, desc
 
 
-def precision_report(cfg, rows, st, steps, ev_mixed):
+def precision_report(cfg, rows, st, steps, ev_mixed=None):
     """Error of a mixed-precision event after `steps` steps against the FP64
     path (bit-identical to the oracle), next to the FP64 path's own
     sensitivity: the same FP64 run from an initial energy density scaled by
     (1 + 2^-50).  Relative L-infinity = max|a - b| / max|b|, relative L2 =
-    |a - b|_2 / |b|_2, over the interior cells."""
+    |a - b|_2 / |b|_2, over the interior cells; then the freezeout over the
+    same steps (element count, sums of d sigma_mu) of single events.  ev_mixed:
+    the mixed event to judge (a batch member), else a single mixed event is
+    run."""
     import numpy as np
     import vh
     fields = [("e", vh.VH_F_E), ("ut", vh.VH_F_UT), ("ux", vh.VH_F_UT + 1), ("uy", vh.VH_F_UT + 2),
@@ -146,8 +158,8 @@ def precision_report(cfg, rows, st, steps, ev_mixed):
     if cfg.bulk:
         fields.append(("Pi", 14))
 
-    def run(ic):
-        e = vh.Event(cfg.copy(precision=vh.VH_PREC_FP64), rows)
+    def run(ic, prec=vh.VH_PREC_FP64):
+        e = vh.Event(cfg.copy(precision=prec), rows)
         e.set_initial(ic)
         e.step(steps)
         e.sync()
@@ -166,9 +178,37 @@ def precision_report(cfg, rows, st, steps, ev_mixed):
     ref = run(st)
     bumped = vh.InitialState(st.e * (1 + 2.0 ** -50), st.p, st.u, st.pi, st.Pi)
     floor = run(bumped)
-    rep = {"steps": steps, "mixed_vs_fp64": errs(ev_mixed, ref), "fp64_sensitivity": errs(floor, ref)}
-    ref.close()
-    floor.close()
+    own = ev_mixed is None
+    if own:
+        ev_mixed = run(st, vh.VH_PREC_MIXED)
+    rep = {"steps": steps, "tau_fm": cfg.t0 + steps * cfg.dt, "mixed_vs_fp64": errs(ev_mixed, ref),
+           "fp64_sensitivity": errs(floor, ref)}
+    for e in (ref, floor) + ((ev_mixed,) if own else ()):
+        e.close()
+
+    # freezeout over the same steps, a block every fo_factor steps as run()
+    # does: element count and the sums of d sigma_mu over all elements
+    def surf(ic, prec):
+        e = vh.Event(cfg.copy(precision=prec), rows)
+        e.set_initial(ic)
+        fac = max(1, cfg.fo_factor)
+        n, ds = 0, np.zeros(4)
+        for _ in range(max(1, steps // fac)):
+            e.step(fac)
+            ne, _ = e.freezeout()
+            if ne:
+                n += ne
+                ds += e.surface()[:, 4:8].sum(axis=0)
+        e.close()
+        return n, ds
+
+    n64, s64 = surf(st, vh.VH_PREC_FP64)
+    fo = {"blocks": max(1, steps // max(1, cfg.fo_factor)), "elements_fp64": n64}
+    for key, (ic, prec) in (("mixed_vs_fp64", (st, vh.VH_PREC_MIXED)), ("fp64_sensitivity", (bumped, vh.VH_PREC_FP64))):
+        n, sm = surf(ic, prec)
+        fo[key] = {"elements": n, "count_rel": abs(n - n64) / max(n64, 1),
+                   "dsigma_sum_rel_linf": float(np.max(np.abs(sm - s64)) / max(np.max(np.abs(s64)), 1e-300))}
+    rep["freezeout"] = fo
     return rep
 
 
@@ -758,7 +798,8 @@ def main():
 
     prec = None
     if mixed and rank == 0:
-        prec = precision_report(cfg, rows, st, ev.progress()[0], ev)
+        psteps = args.precision_steps or PRECISION_STEPS.get(args.workload, args.steps)
+        prec = precision_report(cfg, rows, st, psteps)
 
     base = None
     if rank == 0 and world == 1 and not args.no_baseline:

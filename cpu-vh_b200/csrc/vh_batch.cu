@@ -386,8 +386,9 @@ void drop_graph(vh_batch *b)
 }
 
 /* Time stage 1 of the current step for every (tile shape, grid form), fused
- * and split; stage 1 writes only the scratch planes (qS, e/p[1], uS), which
- * the real step rewrites, so the members' state is untouched. */
+ * and split (split only for a mixed batch, whose forms round differently);
+ * stage 1 writes only the scratch planes (qS, e/p[1], uS), which the real
+ * step rewrites, so the members' state is untouched. */
 int autotune(vh_batch *b)
 {
     for (int s = 0; s < kNumShapes; ++s) {

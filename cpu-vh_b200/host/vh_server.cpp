@@ -64,7 +64,15 @@ struct Job {
     int zero_blocks = 0;            /* blocks with no cell above e_F (accumulator2) */
     double t_done = 0;
     int status = VH_OK;
-    std::vector<double> surface;    /* VH_FO_COLUMNS per element */
+    /* VH_FO_COLUMNS per element, one chunk per freezeout block: appending a
+     * block copies it once (no regrowth of one large vector) */
+    std::vector<std::vector<double>> surface;
+    size_t surface_doubles = 0;
+    void append(const double *p, size_t n)
+    {
+        surface.emplace_back(p, p + n);
+        surface_doubles += n;
+    }
 };
 
 size_t estimate_bytes(const vh_config &c)
@@ -196,7 +204,7 @@ void worker_main(vh_server *S)
         std::vector<Pending> keep;
         for (auto &c : pending) {
             if (only && c.j != only) { keep.push_back(c); continue; }
-            c.j->surface.insert(c.j->surface.end(), c.s.buf, c.s.buf + c.n);
+            c.j->append(c.s.buf, c.n);
             pool.push_back(c.s);
         }
         pending.swap(keep);
@@ -374,9 +382,9 @@ void worker_main(vh_server *S)
                     if (rc == VH_OK) pending.push_back({j, st, need});
                     else pool.push_back(st);
                 } else {                                 /* no pinned memory: straight to the surface */
-                    const size_t off = j->surface.size();
-                    j->surface.resize(off + need);
-                    rc = vh_event_fetch_surface(j->ev, j->surface.data() + off, nel, &nel);
+                    std::vector<double> blk(need);
+                    rc = vh_event_fetch_surface(j->ev, blk.data(), nel, &nel);
+                    if (rc == VH_OK) { j->surface_doubles += need; j->surface.push_back(std::move(blk)); }
                 }
                 add(S->st.t_fo_copy_s, t_cp);
                 std::lock_guard<std::mutex> lk(S->mu);
@@ -541,7 +549,7 @@ int vh_server_poll(vh_server *S, vh_server_done *out, int max, int *n)
         d.tag = j->tag;
         d.status = j->status;
         d.steps = j->steps;
-        d.n_elements = (long long)(j->surface.size() / VH_FO_COLUMNS);
+        d.n_elements = (long long)(j->surface_doubles / VH_FO_COLUMNS);
         d.t_submit = j->t_submit;
         d.t_admit = j->t_admit;
         d.t_done = j->t_done;
@@ -558,12 +566,16 @@ int vh_server_take_surface(vh_server *S, unsigned long long tag, double *out, lo
     std::lock_guard<std::mutex> lk(S->mu);
     auto it = S->fetched.find(tag);
     if (it == S->fetched.end()) return vh::set_error(VH_ERR_ARG, "no polled event with this tag");
-    const long long m = (long long)(it->second->surface.size() / VH_FO_COLUMNS);
+    const Job &j = *it->second;
+    const long long m = (long long)(j.surface_doubles / VH_FO_COLUMNS);
     *n = m;
     if (m > cap_elements) return vh::set_error(VH_ERR_CAPACITY, "surface buffer too small");
     if (m > 0) {
         if (!out) return vh::set_error(VH_ERR_ARG, "null output");
-        std::memcpy(out, it->second->surface.data(), it->second->surface.size() * sizeof(double));
+        for (const auto &blk : j.surface) {
+            std::memcpy(out, blk.data(), blk.size() * sizeof(double));
+            out += blk.size();
+        }
     }
     S->fetched.erase(it);
     return VH_OK;

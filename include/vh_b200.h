@@ -225,9 +225,13 @@ int vh_event_stream(vh_event *ev, void **stream);
  * refers to existing events (it owns none of their memory): one launch per
  * RK phase covers every member, a CUDA graph of one whole RK2 step is
  * replayed, and the tile shape, grid form and fused/split choice come from
- * timing the batch's own members.  Each member's results are bit-identical
- * to vh_event_step on it alone.  Members must share the EoS kind, bulk on/off
- * and the device, must have an initial state, and must outlive the batch.
+ * timing the batch's own members.  In FP64 each member's results are
+ * bit-identical to vh_event_step on it alone, whatever the tuning.  A mixed-
+ * precision batch evaluates each face once in its flux phases (as single
+ * events of 2^15 cells and more do) and its tuner keeps the phase kernels, so
+ * its results do not depend on timing.  Members must share the EoS kind, bulk
+ * on/off, the precision and the device, must have an initial state, and must
+ * outlive the batch.
  * Between batch steps every single-event call (freezeout, fields, status,
  * even vh_event_step) may be used on a member; its stream is ordered after
  * the batch's work and the batch after its stream.
