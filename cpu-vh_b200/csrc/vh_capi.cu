@@ -107,13 +107,21 @@ void pool_live(int dev, int delta)
     if (P.live == 0 && P.pool) cudaMemPoolTrimTo(P.pool, 0);
 }
 
-/* an event buffer, ordered on the event's stream */
+/* an event buffer, ordered on the event's stream.  VH_POISON_ALLOC=1 fills
+ * every new buffer with all-ones bytes (a NaN in every double) before the
+ * library's own initialisation, so that a value read before any kernel
+ * wrote it shows up in the parity tests (a diagnostic, off by default). */
 cudaError_t ev_alloc(vh_event *ev, void *ptr, size_t bytes)
 {
     cudaMemPool_t pool = nullptr;
     cudaError_t e = pool_of(ev->device, &pool);
     if (e != cudaSuccess) return e;
-    return cudaMallocFromPoolAsync(reinterpret_cast<void **>(ptr), bytes, pool, ev->stream);
+    e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(ptr), bytes, pool, ev->stream);
+    if (e == cudaSuccess) {
+        const char *p = getenv("VH_POISON_ALLOC");
+        if (p && p[0] == '1') e = cudaMemsetAsync(*reinterpret_cast<void **>(ptr), 0xFF, bytes, ev->stream);
+    }
+    return e;
 }
 
 void ev_free(vh_event *ev, void *p)
