@@ -72,10 +72,12 @@ int device_powf(int dev, vh::DevPowf *out)
  * keeps freed memory mapped: events that come and go (the server retires
  * and admits them continually) reuse it, without cudaFree's unmapping and
  * device-wide synchronisation.  The pool is trimmed when the last event on
- * the device is destroyed, so an idle process holds nothing. */
+ * the device is destroyed and no server holds it (a server keeps the memory
+ * through its idle gaps), so an idle process holds nothing. */
 struct EventPool {
     cudaMemPool_t pool = nullptr;
     int live = 0;
+    int holds = 0;
 };
 std::mutex g_pool_mu;
 std::map<int, EventPool> g_pools;
@@ -104,7 +106,7 @@ void pool_live(int dev, int delta)
     std::lock_guard<std::mutex> lk(g_pool_mu);
     EventPool &P = g_pools[dev];
     P.live += delta;
-    if (P.live == 0 && P.pool) cudaMemPoolTrimTo(P.pool, 0);
+    if (P.live == 0 && P.holds == 0 && P.pool) cudaMemPoolTrimTo(P.pool, 0);
 }
 
 /* an event buffer, ordered on the event's stream.  VH_POISON_ALLOC=1 fills
@@ -132,6 +134,14 @@ void ev_free(vh_event *ev, void *p)
 } // namespace
 
 
+
+void vh::event_pool_hold(int dev, int delta)
+{
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    EventPool &P = g_pools[dev];
+    P.holds += delta;
+    if (P.live == 0 && P.holds == 0 && P.pool) cudaMemPoolTrimTo(P.pool, 0);
+}
 
 vh::StageArgs vh::stage_args_base(const vh_event *ev)
 {

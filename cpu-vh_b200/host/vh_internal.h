@@ -57,6 +57,10 @@ int set_error(int code, const std::string &msg);
 void draw_hotspots(uint64_t seed, double mean_spots, double k_gamma, double amp_mean_GeV, double R, double a,
                    std::vector<double> &cx, std::vector<double> &cy, std::vector<double> &amp);
 
+/* keep (delta +1) or release (-1) the device's event memory pool through
+ * times without events (vh_capi.cu) */
+void event_pool_hold(int dev, int delta);
+
 } // namespace vh
 
 #endif

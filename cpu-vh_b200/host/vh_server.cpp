@@ -463,6 +463,7 @@ int vh_server_create(const vh_server_config *cfg, const double *eos_rows, int eo
     S->budget = (size_t)(c.hbm_fraction * (double)fr);
     S->st.budget_bytes = S->budget;
     S->t0 = Clock::now();
+    vh::event_pool_hold(S->device, 1);      /* keep event memory through idle gaps */
     S->worker = std::thread(worker_main, S);
     *out = S;
     return VH_OK;
@@ -609,6 +610,7 @@ int vh_server_destroy(vh_server *S)
         S->cv.notify_all();
     }
     if (S->worker.joinable()) S->worker.join();
+    vh::event_pool_hold(S->device, -1);
     delete S;
     return VH_OK;
 }
