@@ -15,6 +15,34 @@
  * reference's own array bounds (cornelius.h: 2 lines per square, 8 polygons
  * per cube, 10 polyhedra per hypercube, 24 lines per polygon and 24 polygons
  * per polyhedron); exceeding one raises an error instead of overrunning.
+ *
+ * MODIFIED VERSION of the Cornelius subroutine: restated in 2026 as CUDA
+ * device code (one thread per cube or hypercube, fixed-size per-thread
+ * storage, status codes instead of exit()), with the same arithmetic.  The
+ * original copyright and permission notice follows; this file is
+ * distributed under the same terms.
+ *
+ * cornelius version 1.3: Copyright 2012, Pasi Huovinen
+ *
+ * This subroutine is aimed to be used as a part of the fluid dynamical
+ * models of the heavy-ion physics community. Permission to use it for
+ * any purpose except for any commercial purpose is granted, provided
+ * that any publication cites the paper describing the algorithm:
+ * P. Huovinen and H. Petersen, arXiv:1206.3371 [nucl-th].
+ *
+ * Permission to distribute this subroutine is granted, provided that no
+ * fee is charged, and that this copyright and permission notice appear
+ * in all the copies. Permission to modify this subroutine is granted
+ * provided that the modified subroutine is made publicly available
+ * latest when any results obtained using the modified subroutine are
+ * published, the modified subroutine is distributed under terms similar
+ * to this notice, and the modified code carries both the original
+ * copyright notice and notices stating that you modified it, and a
+ * relevant date/year.
+ *
+ * This program is distributed in the hope that it will be useful, but
+ * WITHOUT ANY WARRANTY; without even the implied warranty of FITNESS FOR
+ * A PARTICULAR PURPOSE.
  */
 #ifndef VH_CORNELIUS_CUH
 #define VH_CORNELIUS_CUH

@@ -20,6 +20,17 @@
  *    computes the correctly rounded candidate and patches it from a table of
  *    the exceptional inputs, which the host builds once by enumerating its own
  *    powf over the calibrated range (vh_powf_table.cpp).
+ *
+ * expm1_fdlibm / vh_tanh are modified restatements (2026, CUDA device code with
+ * explicit fused multiply-adds) of fdlibm's s_expm1.c and s_tanh.c, which
+ * carry this notice:
+ *
+ *   Copyright (C) 1993 by Sun Microsystems, Inc. All rights reserved.
+ *
+ *   Developed at SunPro, a Sun Microsystems, Inc. business.
+ *   Permission to use, copy, modify, and distribute this
+ *   software is freely granted, provided that this notice
+ *   is preserved.
  */
 #ifndef VH_MATH_CUH
 #define VH_MATH_CUH

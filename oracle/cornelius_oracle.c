@@ -7,11 +7,38 @@
  * hydro) cases the hot path uses.  Plain C with fixed-size storage; the
  * operation order of every floating-point expression follows the reference.
  *
- * Pinned by tests/test_cornelius_oracle.py against the reference's own
+ * Pinned by tests/test_oracle_vs_reference.py against the reference's own
  * known-answer files output_3d.dat / output_4d.dat (example_cornelius.cpp:
- * 10^4 glibc rand() cubes and hypercubes, threshold 0.5) and, through
- * tests/test_oracle_vs_reference.py, against the reference's freezeout output
- * for whole hydro runs.
+ * 10^4 glibc rand() cubes and hypercubes, threshold 0.5; hashes in
+ * tests/golden/cornelius_kat.json) and against the reference's freezeout
+ * output for whole hydro runs.
+ *
+ * MODIFIED VERSION of the Cornelius subroutine: restated in 2026 in plain C
+ * (fixed-size storage, status codes instead of exit()), with the same
+ * arithmetic.  The original copyright and permission notice follows; this
+ * file is distributed under the same terms.
+ *
+ * cornelius version 1.3: Copyright 2012, Pasi Huovinen
+ *
+ * This subroutine is aimed to be used as a part of the fluid dynamical
+ * models of the heavy-ion physics community. Permission to use it for
+ * any purpose except for any commercial purpose is granted, provided
+ * that any publication cites the paper describing the algorithm:
+ * P. Huovinen and H. Petersen, arXiv:1206.3371 [nucl-th].
+ *
+ * Permission to distribute this subroutine is granted, provided that no
+ * fee is charged, and that this copyright and permission notice appear
+ * in all the copies. Permission to modify this subroutine is granted
+ * provided that the modified subroutine is made publicly available
+ * latest when any results obtained using the modified subroutine are
+ * published, the modified subroutine is distributed under terms similar
+ * to this notice, and the modified code carries both the original
+ * copyright notice and notices stating that you modified it, and a
+ * relevant date/year.
+ *
+ * This program is distributed in the hope that it will be useful, but
+ * WITHOUT ANY WARRANTY; without even the implied warranty of FITNESS FOR
+ * A PARTICULAR PURPOSE.
  */
 #include <math.h>
 #include <stdlib.h>

@@ -21,7 +21,7 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_KAT = "/root/reference/freezeout/cornelius-c++-1.3"
+REF_KAT = os.path.join(os.environ.get("VH_REFERENCE", "/root/reference"), "freezeout/cornelius-c++-1.3")
 RAND_MAX = 2147483647
 
 
