@@ -107,39 +107,58 @@ def parse():
     return ap.parse_args()
 
 
+DESC_GUBSER = ("gubser_2p1d: 101x101x1, dx=0.1 fm, tau0=1.0, dtau=0.01, conformal a=15.6269, eta/s=0.2, "
+               "theta=1.8, T0=0.3 GeV, pi at Navier-Stokes")
+DESC_GLAUBER = ("glauber_3p1d: 131x131x61, dx=dy=0.15 fm, deta=0.2, tau0=0.6, dtau=0.015, Au+Au optical Glauber "
+                "b=7 fm, peak 30 GeV/fm^3, 2000-row synthetic crossover EoS, eta/s=0.08, Gaussian zeta/s (bulk on), "
+                "FP64")
+
+
+def desc_batch(n_events):
+    return (f"batch_hotspots_2p1d: {n_events} events, n x n x 1 with n uniform in {{81..201 step 20}} (seed 2024), "
+            "dx=0.1 fm, tau0=0.6, dtau=0.01, Poisson(200) hotspots of width 0.4 fm, Gamma(1.6) amplitudes, "
+            "mean peak 20 GeV/fm^3, centres in the b=0 Woods-Saxon overlap, 2000-row synthetic EoS, eta/s=0.08, "
+            "Gaussian zeta/s (bulk on), FP64")
+
+
+def single_config(desc, nx, ny, nz, nq, world):
+    """the config record of a single-event line (both arms print the same)"""
+    state_mb = (3 * nq + 16) * (nx + 4) * (ny + 4) * (nz + 4) * 8 / 1e6   # q x3, e/p x2, u x3 planes
+    l2 = (f"state {state_mb:.0f} MB > 126 MB L2, no flush" if state_mb > 126 else
+          f"state {state_mb:.0f} MB fits in the 126 MB L2 (not flushed; latency-bound small lattice)")
+    return {"workload": desc, "cells": nx * ny * nz, "parallelism": f"replicas x{world}", "l2": l2}
+
+
 def workload(name):
     import vh
     if name == "gubser_2p1d":
         cfg = vh.gubser_config()
-        return cfg, None, vh.gubser_ic(cfg), "conf", (
-            "gubser_2p1d: 101x101x1, dx=0.1 fm, tau0=1.0, dtau=0.01, conformal a=15.6269, eta/s=0.2, "
-            "theta=1.8, T0=0.3 GeV, pi at Navier-Stokes")
+        return cfg, None, vh.gubser_ic(cfg), "conf", DESC_GUBSER
     cfg = vh.glauber_config()
     rows = vh.synthetic_eos_table()
-    return cfg, rows, vh.glauber_ic(cfg, rows), "table", (
-        "glauber_3p1d: 131x131x61, dx=dy=0.15 fm, deta=0.2, tau0=0.6, dtau=0.015, Au+Au optical Glauber b=7 fm, "
-        "peak 30 GeV/fm^3, 2000-row synthetic crossover EoS, eta/s=0.08, Gaussian zeta/s (bulk on), FP64")
+    return cfg, rows, vh.glauber_ic(cfg, rows), "table", DESC_GLAUBER
 
 
 BATCH_SIZES = (81, 101, 121, 141, 161, 181, 201)
 EVENT_STEPS = 300      # RK2 steps of one event for events/s (the Gubser event's step count)
 
 
+def batch_sizes(n_events):
+    """n of each n x n event of the batched workload, drawn uniformly from
+    BATCH_SIZES (seed 2024)"""
+    import numpy as np
+    rng = np.random.default_rng(2024)
+    return [int(x) for x in rng.choice(BATCH_SIZES, size=n_events)]
+
+
 def batch_workload(n_events):
     """Lumpy 2+1D events, n x n with n drawn uniformly from BATCH_SIZES
     (seed 2024), hotspot initial conditions seeded with the event index."""
-    import numpy as np
     import vh
-    rng = np.random.default_rng(2024)
-    sizes = [int(x) for x in rng.choice(BATCH_SIZES, size=n_events)]
     rows = vh.synthetic_eos_table()
-    cfgs = [vh.hotspot_config(n) for n in sizes]
+    cfgs = [vh.hotspot_config(n) for n in batch_sizes(n_events)]
     ics = [vh.hotspot_ic(c, rows, seed=i) for i, c in enumerate(cfgs)]
-    desc = (f"batch_hotspots_2p1d: {n_events} events, n x n x 1 with n uniform in {{81..201 step 20}} (seed 2024), "
-            "dx=0.1 fm, tau0=0.6, dtau=0.01, Poisson(200) hotspots of width 0.4 fm, Gamma(1.6) amplitudes, "
-            "mean peak 20 GeV/fm^3, centres in the b=0 Woods-Saxon overlap, 2000-row synthetic EoS, eta/s=0.08, "
-            "Gaussian zeta/s (bulk on), FP64")
-    return cfgs, rows, ics, desc
+    return cfgs, rows, ics, desc_batch(n_events)
 
 
 def precision_report(cfg, rows, st, steps, ev_mixed=None):
@@ -449,54 +468,117 @@ def reference_freezeout(cfg, rows, variant):
                       f"cell count to {cfg.nx}x{cfg.ny}x{cfg.nz}; serial, writes its surface.dat lines"}
 
 
+def _ref_steps_timed(refs, args, budget_s):
+    """warm-up then K timed steps of every reference event, K bounded so the
+    timed part stays within about budget_s seconds"""
+    def step_all(k):
+        for r in refs:
+            r.step(k)
+    t0 = time.perf_counter()
+    step_all(1)
+    est = time.perf_counter() - t0
+    warm = max(0, min(args.warmup, int(budget_s / 5 / max(est, 1e-3))) - 1)
+    if warm:
+        step_all(warm)
+    k = max(1, min(args.steps, int(budget_s / max(est, 1e-3))))
+    t0 = time.perf_counter()
+    step_all(k)
+    return k, time.perf_counter() - t0
+
+
 def run_reference(args):
+    """The reference's own CPU implementation (its sources compiled in place
+    by oracle/ref.mk into oracle/_ref) on the same workload and config.  The
+    inputs come from the copy of the workload generators linked into those
+    libraries (oracle/workload_gen.c) and the reference's own EoS, so this
+    process loads no library of this repository but oracle/_ref."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     import oracle as O
-    if args.workload == "batch_hotspots_2p1d":
-        cfgs, rows, ics, desc = batch_workload(args.events)
-        items, variant = list(zip(cfgs, ics))[:8], "table"
-        sample = "the first 8 events of the batch, one after another"
-    else:
-        cfg, rows, st, variant, desc = workload(args.workload)
-        items, sample = [(cfg, st)], "the event"
     threads = os.cpu_count() or 1
-    refs = []
-    for cfg, st in items:
-        if O.ref_available(variant):
-            ref, kind = O.RefEvent(variant, cfg, rows, threads=threads), "reference"
-        else:
-            ref, kind, threads = O.OracleEvent(cfg, rows), "port", 1
-        ref.set_initial(st)
-        refs.append(ref)
-    N = sum(c.nx * c.ny * c.nz for c, _ in items)
+    batch = args.workload == "batch_hotspots_2p1d"
+    if batch:
+        variant = "table"
+        sizes = batch_sizes(args.events)[:8]
+        cfgs = [O.hotspot_workload(n) for n in sizes]
+        desc, sample = desc_batch(args.events), "the first 8 events of the batch, one after another"
+    elif args.workload == "gubser_2p1d":
+        variant, cfgs, desc, sample = "conf", [O.gubser_workload()], DESC_GUBSER, "the event"
+    else:
+        variant, cfgs, desc, sample = "table", [O.glauber_workload()], DESC_GLAUBER, "the event"
+    if not O.ref_available(variant):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference's sources were not compiled "
+                          "(oracle/_ref missing: build() needs the reference tree)"}), flush=True)
+        return 0
+    lib = O.ref_lib_path(variant)
+    rows = O.synthetic_eos_rows(O.load_gen_lib(lib)) if variant == "table" else None
 
-    def step_all(k):
-        for r in refs:
-            r.step(k)
+    def make_refs(var, nthreads):
+        out = []
+        for i, c in enumerate(cfgs):
+            r = O.RefEvent(var, c, rows, threads=nthreads)
+            gl = O.load_gen_lib(O.ref_lib_path(var))
+            if batch:
+                st = O.hotspot_state(c, r.pressure, seed=i, lib=gl)
+            elif var.startswith("conf"):
+                st = O.gubser_state(c, lib=gl)
+            else:
+                st = O.glauber_state(c, r.pressure, lib=gl)
+            r.set_initial(st)
+            out.append(r)
+        return out
 
-    # bounded sample: at most ~150 s of timed CPU work
-    t0 = time.perf_counter()
-    step_all(1)
-    est = time.perf_counter() - t0
-    warm = max(0, min(args.warmup, int(30.0 / max(est, 1e-3))) - 1)
-    if warm:
-        step_all(warm)
-    k = max(1, min(args.steps, int(150.0 / max(est, 1e-3))))
-    t0 = time.perf_counter()
-    step_all(k)
-    secs = time.perf_counter() - t0
-    v = N * k / secs
+    N = sum(c.nx * c.ny * c.nz for c in cfgs)
+    # the reference keeps its state in process globals: one event per library
+    # at a time, so a batch sample runs its events one after another
+    if batch:
+        cells, secs = 0, 0.0
+        gl = O.load_gen_lib(lib)
+        for i, c in enumerate(cfgs):
+            ev = O.RefEvent(variant, c, rows, threads=threads)
+            ev.set_initial(O.hotspot_state(c, ev.pressure, seed=i, lib=gl))
+            k, sc = _ref_steps_timed([ev], args, 150.0 / len(cfgs))
+            cells += k * c.nx * c.ny
+            secs += sc
+        v, k, ms_step = cells / secs, None, None
+    else:
+        refs = make_refs(variant, threads)
+        k, secs = _ref_steps_timed(refs, args, 120.0)
+        v = N * k / secs
+        ms_step = secs / k * 1e3
     line = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs / k * 1e3,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "impl": "reference",
-            "config": {"workload": desc, "cells": N, "timed_steps": k},
-            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": kind,
-                             "sample": f"{k} RK2 steps of {sample}, timed of {args.steps} requested "
-                                       f"(bounded to ~150 s), {threads} OpenMP threads"},
+            "config": ({"workload": desc, "events": args.events, "parallelism": f"replicas x{args.gpus}"} if batch
+                       else single_config(desc, cfgs[0].nx, cfgs[0].ny, cfgs[0].nz, 15 if cfgs[0].bulk else 14,
+                                          args.gpus)),
+            "timed_steps": k,
+            "ghost_cells": "race-fixed restatement of setGhostCells (private loop indices; the shipped loops "
+                           "share them across OpenMP threads, DynamicalVariables.cpp:290-291, :324-325, :358-359)",
+            "build": "the reference's sources, g++ -O3 -fopenmp -std=c++11 -march=x86-64-v3 -ffp-contract=off",
+            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "reference",
+                             "sample": (f"{k} RK2 steps of {sample}" if k else f"RK2 steps of {sample}") +
+                                       f", of {args.steps} requested (bounded to ~150 s), {threads} OpenMP threads"},
             "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not batch:
+        # the same code on one thread, and as the shipped CMake flags build it
+        # (-march=native, the compiler's own multiply-add contraction), on a
+        # bounded sample of the same event
+        del refs
+        one = make_refs(variant, 1)
+        k1, s1 = _ref_steps_timed(one, argparse.Namespace(steps=2, warmup=1), 25.0)
+        line["one_thread"] = {"value": N * k1 / s1, "unit": "cell-updates/s", "cores": 1,
+                              "sample": f"{k1} RK2 steps of the event after 1 warm-up step"}
+        del one
+        shipped = variant + "_shipped"
+        if O.ref_available(shipped):
+            sh = make_refs(shipped, threads)
+            k2, s2 = _ref_steps_timed(sh, args, 30.0)
+            line["shipped_flags"] = {"value": N * k2 / s2, "unit": "cell-updates/s", "cores": threads,
+                                     "build": O.shipped_build_flags(),
+                                     "sample": f"{k2} RK2 steps of the event, {threads} OpenMP threads"}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -18,6 +18,8 @@ import os
 import subprocess
 import sys
 
+from dataclasses import dataclass
+
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -46,7 +48,8 @@ def _stdout_to_stderr():
 
 
 def build_oracle(force: bool = False) -> str:
-    srcs = [os.path.join(HERE, f) for f in ("vh_oracle.c", "cornelius_oracle.c") if os.path.exists(os.path.join(HERE, f))]
+    srcs = [os.path.join(HERE, f) for f in ("vh_oracle.c", "cornelius_oracle.c", "workload_gen.c")
+            if os.path.exists(os.path.join(HERE, f))]
     newest = max(os.path.getmtime(s) for s in srcs)
     if force or not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < newest:
         subprocess.run(["make", "-s", "-C", HERE, "liboracle_vh.so", "CC_HOST=gcc"], check=True)
@@ -151,8 +154,134 @@ class OracleEvent:
         self.close()
 
 
+# --------------------------------------------------------------- workloads
+# The benchmark's workloads described without the CUDA library: a plain
+# configuration record (the fields of vh_config that the oracles read) and
+# the seeded generators of workload_gen.c, which both liboracle_vh.so and the
+# oracle/_ref libraries export, so the reference can be given its inputs
+# while only its own library is loaded.
+
+@dataclass
+class WorkloadConfig:
+    nx: int
+    ny: int
+    nz: int
+    dx: float
+    dy: float
+    dz: float
+    dt: float
+    t0: float
+    etabar: float
+    theta: float = 1.8
+    bulk: int = 0
+    eos_kind: int = 0                 # 0 conformal, 1 table
+    eos_factor: float = 15.6269
+    T_reg_GeV: float = 0.1
+    T_freezeout_GeV: float = 0.15
+    fo_factor: int = 2
+    zeta_law: int = 0                 # 0 the reference's law, 1 Gaussian in T [GeV]
+    zeta_norm: float = 0.0
+    zeta_T0_GeV: float = 0.0
+    zeta_width_GeV: float = 0.0
+
+
+def gubser_workload(nx=101, ny=101) -> WorkloadConfig:
+    """Config "plain 2+1D Gubser": 101^2, dx = 0.1 fm, tau0 = 1, dtau = 0.01,
+    eta/s = 0.2, conformal a = 15.6269, theta = 1.8, T_F = 0.15 GeV"""
+    return WorkloadConfig(nx, ny, 1, 0.1, 0.1, 0.1, 0.01, 1.0, 0.2)
+
+
+def glauber_workload(nx=131, ny=131, nz=61) -> WorkloadConfig:
+    """Config "plain 3+1D Glauber": 131^2 x 61, dx = dy = 0.15, deta = 0.2,
+    tau0 = 0.6, dtau = 0.015, eta/s = 0.08, table EoS, Gaussian zeta/s"""
+    return WorkloadConfig(nx, ny, nz, 0.15, 0.15, 0.2, 0.015, 0.6, 0.08, bulk=1, eos_kind=1,
+                          zeta_law=1, zeta_norm=0.05, zeta_T0_GeV=0.17, zeta_width_GeV=0.02)
+
+
+def hotspot_workload(n=101) -> WorkloadConfig:
+    """a 2+1D lumpy event of the batched workload: n x n, dx = 0.1 fm,
+    tau0 = 0.6, dtau = 0.01, otherwise as the Glauber event"""
+    c = glauber_workload(n, n, 1)
+    c.dx = c.dy = c.dz = 0.1
+    c.t0, c.dt = 0.6, 0.01
+    return c
+
+
+@dataclass
+class WorkloadState:
+    e: np.ndarray
+    p: np.ndarray
+    u: np.ndarray          # (4, N)
+    pi: np.ndarray | None  # (10, N)
+    Pi: np.ndarray | None  # (N,)
+
+
+def _gen_sigs(L):
+    if getattr(L, "_vhg_ready", False):
+        return L
+    L.vhg_eos_synthetic_table.argtypes = [C.c_int] + [C.c_double] * 6 + [_dp]
+    L.vhg_ic_glauber.argtypes = [C.c_int] * 3 + [C.c_double] * 10 + [_dp, _dp]
+    L.vhg_ic_hotspots.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_uint64] + [C.c_double] * 6 + [_dp, _dp]
+    L.vhg_ic_gubser.argtypes = [C.c_int, C.c_int] + [C.c_double] * 7 + [_dp, _dp, _dp, C.c_void_p]
+    L._vhg_ready = True
+    return L
+
+
+def synthetic_eos_rows(lib=None, nrows=2000, T_lo=0.05, e_max=60.0, a=15.6269, dip=0.2, Tc=0.16, w=0.04):
+    """the 2000-row crossover EoS table (rows e, P, s, T)"""
+    L = _gen_sigs(lib or oracle_lib())
+    rows = np.zeros((nrows, 4))
+    assert L.vhg_eos_synthetic_table(nrows, T_lo, e_max, a, dip, Tc, w, rows) == 0
+    return rows
+
+
+def glauber_state(cfg, pressure, lib=None, R=6.38, a=0.535, sigma_nn=4.2, b=7.0, e0=30.0, eta_flat=3.0,
+                  eta_sigma=1.3) -> WorkloadState:
+    """optical-Glauber initial state; pressure(e) -> p is the EoS of the
+    caller's library"""
+    L = _gen_sigs(lib or oracle_lib())
+    N = cfg.nx * cfg.ny * cfg.nz
+    e, u = np.zeros(N), np.zeros(4 * N)
+    assert L.vhg_ic_glauber(cfg.nx, cfg.ny, cfg.nz, cfg.dx, cfg.dy, cfg.dz, R, a, sigma_nn, b, e0, eta_flat,
+                            eta_sigma, e, u) == 0
+    return WorkloadState(e, pressure(e), u.reshape(4, N), None, np.zeros(N) if cfg.bulk else None)
+
+
+def hotspot_state(cfg, pressure, seed, lib=None, mean_spots=200.0, w=0.4, k_gamma=1.6, amp=20.0, R=6.38,
+                  a=0.535) -> WorkloadState:
+    L = _gen_sigs(lib or oracle_lib())
+    N = cfg.nx * cfg.ny
+    e, u = np.zeros(N), np.zeros(4 * N)
+    assert L.vhg_ic_hotspots(cfg.nx, cfg.ny, cfg.dx, cfg.dy, seed, mean_spots, w, k_gamma, amp, R, a, e, u) == 0
+    return WorkloadState(e, pressure(e), u.reshape(4, N), None, np.zeros(N) if cfg.bulk else None)
+
+
+def gubser_state(cfg, lib=None, q=1.0, T0_GeV=0.3) -> WorkloadState:
+    L = _gen_sigs(lib or oracle_lib())
+    N = cfg.nx * cfg.ny
+    e, p, u, pi = np.zeros(N), np.zeros(N), np.zeros(4 * N), np.zeros(10 * N)
+    assert L.vhg_ic_gubser(cfg.nx, cfg.ny, cfg.dx, cfg.dy, cfg.t0, cfg.eos_factor, cfg.etabar, q, T0_GeV, e, p, u,
+                           pi.ctypes.data_as(C.c_void_p)) == 0
+    return WorkloadState(e, p, u.reshape(4, N), pi.reshape(10, N), None)
+
+
+def ref_lib_path(variant: str) -> str:
+    return os.path.join(REF_DIR, f"libvhref_{variant}.so")
+
+
 def ref_available(variant: str) -> bool:
-    return os.path.exists(os.path.join(REF_DIR, f"libvhref_{variant}.so"))
+    return os.path.exists(ref_lib_path(variant))
+
+
+def load_gen_lib(path: str):
+    """a library exporting the workload generators (oracle/_ref or the oracle)"""
+    return _gen_sigs(C.CDLL(path))
+
+
+def shipped_build_flags() -> str:
+    """how the *_shipped reference libraries were compiled (oracle/ref.mk)"""
+    p = os.path.join(REF_DIR, "shipped_flags.txt")
+    return open(p).read().strip() if os.path.exists(p) else "unknown"
 
 
 class RefEvent:
@@ -187,6 +316,14 @@ class RefEvent:
         for f in ("vhref_eos_pressure", "vhref_eos_temperature", "vhref_eos_cs2", "vhref_eos_energy"):
             getattr(L, f).argtypes = [C.c_double]
             getattr(L, f).restype = C.c_double
+        L.vhref_eos_pressure_n.argtypes = [_dp, _dp, C.c_long]
+
+    def pressure(self, e):
+        """the reference's equilibrium pressure of the energy densities e"""
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        p = np.zeros_like(e)
+        self.L.vhref_eos_pressure_n(e, p, len(e))
+        return p
 
     def set_initial(self, st):
         N = self.cfg.nx * self.cfg.ny * self.cfg.nz

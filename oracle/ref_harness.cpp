@@ -319,6 +319,11 @@ int vhref_load_eos_table(const double *rows, int nrows)
 }
 
 double vhref_eos_pressure(double ed) { return eqnOfState.equilibriumPressure(ed); }
+/* the reference's equilibrium pressure of n energy densities (initial states) */
+void vhref_eos_pressure_n(const double *ed, double *p_out, long n)
+{
+    for (long i = 0; i < n; ++i) p_out[i] = eqnOfState.equilibriumPressure(ed[i]);
+}
 double vhref_eos_temperature(double ed) { return eqnOfState.effectiveTemperature(ed); }
 double vhref_eos_cs2(double ed) { return eqnOfState.speedOfSoundSquared(ed); }
 double vhref_eos_energy(double T) { return eqnOfState.equilibriumEnergyDensity(T); }

@@ -164,3 +164,45 @@ def test_table_sound_speed_is_one_third_up_to_the_bound():
             r[:, 1] *= 10.0
         assert vh.eos_eval(cfg, r, 4, 0.0) == -np.inf, bad
     assert vh.eos_eval(vh.gubser_config(9, 9), None, 4, 0.0) == -np.inf
+
+
+def _same_bits(a, b):
+    a, b = np.ascontiguousarray(a, dtype=np.float64), np.ascontiguousarray(b, dtype=np.float64)
+    return a.shape == b.shape and np.array_equal(a.view(np.uint64), b.view(np.uint64))
+
+
+def test_oracle_workload_generators_equal_the_library_bit_for_bit():
+    """the CPU side (oracle/workload_gen.c, which the reference's own libraries
+    link) makes the benchmark's inputs bit for bit as the library does, so the
+    reference arm runs on the same inputs without loading the CUDA library"""
+    rows = O.synthetic_eos_rows()
+    assert _same_bits(rows, vh.synthetic_eos_table())
+    g = vh.glauber_config(23, 21, 9)
+    og = O.glauber_workload(23, 21, 9)
+    for k in ("nx", "ny", "nz", "dx", "dy", "dz", "dt", "t0", "etabar", "bulk", "eos_kind", "theta"):
+        assert getattr(g, k) == getattr(og, k), k
+
+    def press(e, cfg=g):
+        return np.array([vh.eos_eval(cfg, rows, 0, x) for x in e])
+
+    a, b = vh.glauber_ic(g, rows), O.glauber_state(og, press)
+    assert _same_bits(a.e, b.e) and _same_bits(a.p, b.p) and _same_bits(a.u, b.u)
+    h, oh = vh.hotspot_config(41), O.hotspot_workload(41)
+    for seed in (0, 7):
+        a, b = vh.hotspot_ic(h, rows, seed=seed), O.hotspot_state(oh, lambda e: press(e, h), seed)
+        assert _same_bits(a.e, b.e) and _same_bits(a.p, b.p) and _same_bits(a.u, b.u)
+    gu, ogu = vh.gubser_config(31, 27), O.gubser_workload(31, 27)
+    a, b = vh.gubser_ic(gu), O.gubser_state(ogu)
+    assert _same_bits(a.e, b.e) and _same_bits(a.p, b.p) and _same_bits(a.u, b.u) and _same_bits(a.pi, b.pi)
+
+
+@pytest.mark.skipif(not O.ref_available("table"), reason="the reference's own sources were not built here")
+def test_reference_pressure_of_the_initial_state_equals_the_library():
+    """the reference arm gives the reference its initial state with the
+    reference's own EoS pressure; it equals the library's host EoS"""
+    rows = O.synthetic_eos_rows()
+    cfg = O.glauber_workload(15, 13, 5)
+    ref = O.RefEvent("table", cfg, rows)
+    st = O.glauber_state(cfg, ref.pressure)
+    g = vh.glauber_config(15, 13, 5)
+    assert _same_bits(st.p, vh.glauber_ic(g, rows).p)
