@@ -101,11 +101,17 @@ __device__ __forceinline__ double eos_T(const DevEos &E, double ed)          /* 
 }
 
 /* --------------------------------------------------------- limiter */
-/* FluxLimiter.cpp:14-32, generalised minmod with sign(0) = +1 */
+/* FluxLimiter.cpp:14-32, generalised minmod with sign(0) = +1:
+ * (sign(x) + sign(y)) * min(|x|, |y|) / 2, evaluated without the integer
+ * sum and its conversion.  The factor is +-2 or 0, and 2m / 2 = m exactly
+ * for m = min(|x|, |y|) below 2^1023 (no overflow in 2m), so the result is
+ * +-m when the signs agree and 0 * m (+0, or NaN for m = inf) when they
+ * differ -- the same value, sign of zero and NaN cases included. */
 __device__ __forceinline__ double minmod(double x, double y)
 {
-    int sx = (x < 0) ? -1 : 1, sy = (y < 0) ? -1 : 1;
-    return (sx + sy) * fmin(fabs(x), fabs(y)) / 2.0;
+    const bool nx = x < 0, ny = y < 0;
+    const double m = fmin(fabs(x), fabs(y));
+    return (nx == ny) ? (nx ? -m : m) : 0.0 * m;
 }
 __device__ __forceinline__ double approx_deriv(double th, double x, double y, double z)
 {
@@ -116,29 +122,11 @@ __device__ __forceinline__ double approx_deriv(double th, double x, double y, do
 }
 
 /* -------------------------------------------------------- inversion */
-/* EnergyMomentumTensor.cpp:22-111, the tabulated-EoS root solve: Newton from
- * ePrev, bisection if Newton does not converge.  Kept out of line: it is
- * called thirteen times per cell and stage, and inlining the loop that often
- * overflows the instruction cache. */
-__device__ __forceinline__ double e_newton_table_body(const DevEos &E, double ePrev, double M0, double M, double Pi, bool &bad)
+/* EnergyMomentumTensor.cpp:48-111: the bisection the tabulated-EoS root solve
+ * falls back to when Newton has not converged in 10^4 iterations.  Out of
+ * line: no workload here reaches it, and every caller shares one copy. */
+static __device__ __noinline__ double e_bisect_table(const DevEos &E, double ePrev, double M0, double M, double Pi)
 {
-    double e0 = ePrev;
-    for (int j = 0; j < 10000; ++j) {                              /* MAX_ITERS_NR */
-        double pp = eos_p<1>(E, e0);
-        double cs2 = eos_cs2<1>(E, e0);
-        double cst2 = pp / e0;
-        double A = M0 * (1.0 - cst2) + Pi;
-        double B = M0 * (M0 + Pi) - M;
-        double H = (double)sqrtf(fabsf(__double2float_rn(A * A + 4 * cst2 * B)));
-        double D = (A - H) / (2 * cst2);
-        double f = e0 + D;
-        double fp = 1.0 - ((cs2 - cst2) * (B + D * H - ((cs2 - cst2) * cst2 * D * M0) / e0)) / (cst2 * e0 * H);
-        if (isnan(f / fp)) { bad = true; return ePrev; }
-        double e = e0 - f / fp;
-        if ((double)fabsf(__double2float_rn(e - e0)) <= 1.0e-3 * (double)fabsf(__double2float_rn(e))) return e;
-        e0 = e;
-    }
-    /* bisection fallback, EnergyMomentumTensor.cpp:48-111 */
     double e_lo = 0.0, e_mid = ePrev, e_hi = 2.0 * (ePrev + 1.0);
     for (int j = 0; j < 1000000; ++j) {                            /* MAX_ITERS_BI */
         double p_lo = eos_p<1>(E, e_lo), p_mid = eos_p<1>(E, e_mid), p_hi = eos_p<1>(E, e_hi);
@@ -156,6 +144,43 @@ __device__ __forceinline__ double e_newton_table_body(const DevEos &E, double eP
         else if (f_mid * f_hi < 0.0) { e_lo = e_mid; e_mid = (e_lo + e_hi) / 2.0; }
     }
     return ePrev;
+}
+
+/* One Newton iteration of EnergyMomentumTensor.cpp:22-44 from e0: the next
+ * iterate, whether f/f' is NaN, and whether the float-truncated convergence
+ * test (:41) passes. */
+__device__ __forceinline__ double e_newton_iter(const DevEos &E, double e0, double M0, double M, double Pi,
+                                                bool &nan_step, bool &conv)
+{
+    double pp = eos_p<1>(E, e0);
+    double cs2 = eos_cs2<1>(E, e0);
+    double cst2 = pp / e0;
+    double A = M0 * (1.0 - cst2) + Pi;
+    double B = M0 * (M0 + Pi) - M;
+    double H = (double)sqrtf(fabsf(__double2float_rn(A * A + 4 * cst2 * B)));
+    double D = (A - H) / (2 * cst2);
+    double f = e0 + D;
+    double fp = 1.0 - ((cs2 - cst2) * (B + D * H - ((cs2 - cst2) * cst2 * D * M0) / e0)) / (cst2 * e0 * H);
+    double q = f / fp;
+    double e = e0 - q;
+    nan_step = isnan(q);
+    conv = (double)fabsf(__double2float_rn(e - e0)) <= 1.0e-3 * (double)fabsf(__double2float_rn(e));
+    return e;
+}
+
+/* EnergyMomentumTensor.cpp:22-111, the tabulated-EoS root solve: Newton from
+ * ePrev, bisection if Newton does not converge. */
+__device__ __forceinline__ double e_newton_table_body(const DevEos &E, double ePrev, double M0, double M, double Pi, bool &bad)
+{
+    double e0 = ePrev;
+    for (int j = 0; j < 10000; ++j) {                              /* MAX_ITERS_NR */
+        bool nan_step, conv;
+        double e = e_newton_iter(E, e0, M0, M, Pi, nan_step, conv);
+        if (nan_step) { bad = true; return ePrev; }
+        if (conv) return e;
+        e0 = e;
+    }
+    return e_bisect_table(E, ePrev, M0, M, Pi);
 }
 
 /* The root solve as a call (one copy of the loop for a long kernel whose

@@ -257,6 +257,120 @@ __device__ __forceinline__ void flux_staged_tile(const StageArgs &A, int i0, int
     if (bad) raise_error(A.err, kErrNan, s, A.step);
 }
 
+/* Geometry of the flux tile along DIR: TX x TY cells, their values with a
+ * 2-cell halo along DIR (BX x BY per component) and the half slopes of
+ * HalfSiteExtrapolation.cpp:12-26 at every position one cell in from the
+ * halo's ends (HX x HY per component). */
+template <int DIR, int TX, int TY>
+struct FluxTile {
+    static constexpr int BX = TX + (DIR == 1 ? 4 : 0), BY = TY + (DIR == 1 ? 0 : 4), P = BX * BY;
+    static constexpr int HX = TX + (DIR == 1 ? 2 : 0), HY = TY + (DIR == 1 ? 0 : 2), H = HX * HY;
+    static constexpr int kDoubles(int nq) { return nq * (P + H); }
+};
+
+/* The staged flux along DIR with each half slope computed once per tile.
+ * A face's half-site states are qR = q(b+1) - d(b+1)/2 and qL = q(b) + d(b)/2
+ * with d the minmod-limited slope at a cell (approx_deriv); the reference
+ * evaluates every slope at a cell for each of the four faces around its two
+ * neighbours along the axis, with identical arguments and so an identical
+ * value.  Here the block computes the half slope d/2 of every tile position
+ * once into shared memory; each thread then forms its cell's four states
+ * (two faces, two sides), runs their root solves (one inlined copy of infer,
+ * in a rolled loop) and updates q* one component at a time.  Every value is
+ * the reference's arithmetic on the same operands, so the results are
+ * bit-identical to flux_staged_tile.  sm: FluxTile::kDoubles(NQ) doubles. */
+template <int NQ, int EOS, int DIR, int TX, int TY>
+__device__ __forceinline__ void flux_slopes_tile(const StageArgs &A, int i0, int j0, int k0, double *__restrict__ sm)
+{
+    using G = FluxTile<DIR, TX, TY>;
+    constexpr int BX = G::BX, P = G::P, HX = G::HX, H = G::H;
+    double *__restrict__ hs = sm + NQ * P;
+    const int tid = threadIdx.x + TX * threadIdx.y;
+    const long long sxy = (long long)A.ncx * A.ncy;
+    const int bx0 = i0 + 2 - (DIR == 1 ? 2 : 0);
+    const int b2lim = (DIR == 3) ? A.nz + 4 : A.ny + 4;
+    const int by_first = (DIR == 1) ? j0 + 2 : (DIR == 3) ? k0 : j0;
+    for (int e = tid; e < NQ * P; e += TX * TY) {
+        const int n = e / P, rr = e - n * P, bxi = rr % BX, byi = rr / BX;
+        const int x = bx0 + bxi, yk = by_first + byi;
+        if (x < A.ncx && yk < b2lim) {
+            const long long g = (DIR == 3) ? x + (long long)A.ncx * (j0 + 2) + sxy * yk
+                                           : x + (long long)A.ncx * yk + sxy * (k0 + 2);
+            cp_async8(sm + e, A.qin + n * A.L + g);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const double th = A.theta;
+    constexpr int tst = (DIR == 1) ? 1 : BX;
+    for (int e = tid; e < NQ * H; e += TX * TY) {
+        const int n = e / H, rr = e - n * H, hx = rr % HX, hy = rr / HX;
+        const int tp = (hx + (DIR == 1 ? 1 : 0)) + BX * (hy + (DIR == 1 ? 0 : 1));
+        const double *q = sm + n * P + tp;
+        hs[e] = approx_deriv(th, q[-tst], q[0], q[tst]) / 2;
+    }
+    __syncthreads();
+    const int i = i0 + threadIdx.x + 2;
+    const int j = (DIR == 3) ? j0 + 2 : j0 + threadIdx.y + 2;
+    const int k = (DIR == 3) ? k0 + threadIdx.y + 2 : k0 + 2;
+    if (i >= A.nx + 2 || j >= A.ny + 2 || k >= A.nz + 2) return;
+    const long long s = i + (long long)A.ncx * j + sxy * k;
+    const int ts = (threadIdx.x + (DIR == 1 ? 2 : 0)) + BX * (threadIdx.y + (DIR == 1 ? 0 : 2));
+    const int hp = (threadIdx.x + (DIR == 1 ? 1 : 0)) + HX * (threadIdx.y + (DIR == 1 ? 0 : 1));
+    constexpr int hst = (DIR == 1) ? 1 : HX;
+    const QTile qt{sm, P};
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    /* states m = 0..3: forward face R, L; backward face R, L */
+    double ut0 = 0, ut1 = 0, ut2 = 0, ut3 = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0;
+#pragma unroll 1
+    for (int m = 0; m < 4; ++m) {
+        const int vo = (m == 0) ? ts + tst : (m == 3) ? ts - tst : ts;
+        const int ho = (m == 0) ? hp + hst : (m == 3) ? hp - hst : hp;
+        const bool minus = (m & 1) == 0;        /* R states subtract the half slope */
+        double st[9];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const int n = (c < 8) ? c : 14;
+            if (n >= NQ) { st[c] = 0; continue; }
+            const double qv = sm[n * P + vo], hv = hs[n * H + ho];
+            st[c] = minus ? qv - hv : qv + hv;
+        }
+        const Prim Pm = infer<EOS, true>(A.eos, A.t, st[0] - st[4], st[1] - st[5], st[2] - st[6], st[3] - st[7],
+                                         st[8], ePrev, bad);
+        const double vm = (DIR == 1) ? Pm.ux : (DIR == 2) ? Pm.uy : Pm.un;
+        if (m == 0) { ut0 = Pm.ut; v0 = vm; }
+        else if (m == 1) { ut1 = Pm.ut; v1 = vm; }
+        else if (m == 2) { ut2 = Pm.ut; v2 = vm; }
+        else { ut3 = Pm.ut; v3 = vm; }
+    }
+    const double y0 = 1.0 / ut0, y1 = 1.0 / ut1, y2 = 1.0 / ut2, y3 = 1.0 / ut3;
+    /* spectral radius of each face, max(|vL / utL|, |vR / utR|) */
+    const double af = fmax(fabs(div_rcp(v1, ut1, y1)), fabs(div_rcp(v0, ut0, y0)));
+    const double ab = fmax(fabs(div_rcp(v3, ut3, y3)), fabs(div_rcp(v2, ut2, y2)));
+    const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
+    const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
+    double S[4];
+    dir_sources_t<NQ>(A, qt, ts, tst, s, d, DIR, S);
+    /* H(s-1/2) - H(s+1/2) component by component, added to q* */
+#pragma unroll 1
+    for (int n = 0; n < NQ; ++n) {
+        const double *q = sm + n * P + ts, *h = hs + n * H + hp;
+        const double Rf = q[tst] - h[hst], Lf = q[0] + h[0], Rb = q[0] - h[0], Lb = q[-tst] + h[-hst];
+        double rf = div_rcp(v0 * Rf, ut0, y0) + div_rcp(v1 * Lf, ut1, y1) - af * (Rf - Lf);
+        rf /= 2;
+        double rb = div_rcp(v2 * Rb, ut2, y2) + div_rcp(v3 * Lb, ut3, y3) - ab * (Rb - Lb);
+        rb /= 2;
+        double r = -rf;
+        r = r + rb;
+        r = div_rcp(r, d, yd);
+        if (n < 4) r += (n == 0) ? S[0] : (n == 1) ? S[1] : (n == 2) ? S[2] : S[3];
+        r *= A.dt;
+        A.qout[n * A.L + s] += r;
+    }
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+}
+
 /* eulerStepKernelX/Y/Z (FullyDiscreteKurganovTadmorScheme.cpp:300-634), the
  * axes in the reference's order x, y, eta. */
 template <int NQ, int EOS, bool HAS_Z>

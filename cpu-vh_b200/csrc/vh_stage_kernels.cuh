@@ -97,6 +97,45 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_staged_kerne
     flux_staged_tile<NQ, EOS, DIR, TX, TY>(A, i0, j0, k0, sm);
 }
 
+/* the same tile with every half slope computed once (flux_slopes_tile);
+ * dynamic shared memory: FluxTile::kDoubles(NQ) doubles, up to 53.8 KB */
+template <int NQ, int EOS, int DIR>
+__global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_slopes_kernel(const __grid_constant__ StageArgs A)
+{
+    constexpr int TX = 32, TY = 4;
+    extern __shared__ double smd[];
+    const int i0 = blockIdx.x * TX;
+    int j0, k0;
+    if (DIR == 3) { j0 = blockIdx.y; k0 = blockIdx.z * TY; } else { j0 = blockIdx.y * TY; k0 = blockIdx.z; }
+    flux_slopes_tile<NQ, EOS, DIR, TX, TY>(A, i0, j0, k0, smd);
+}
+
+template <int NQ, int EOS, int DIR>
+static void launch_flux_slopes(const StageArgs &a, dim3 grid, dim3 block, cudaStream_t s)
+{
+    constexpr size_t bytes = sizeof(double) * FluxTile<DIR, 32, 4>::kDoubles(NQ);
+    static const bool attr = [] {
+        cudaFuncSetAttribute(kt_flux_slopes_kernel<NQ, EOS, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bytes);
+        cudaFuncSetAttribute(kt_flux_slopes_kernel<NQ, EOS, DIR>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             100);
+        return true;
+    }();
+    (void)attr;
+    kt_flux_slopes_kernel<NQ, EOS, DIR><<<grid, block, bytes, s>>>(a);
+}
+
+/* FP64 flux form of the phase-split stage: VH_FLUX_FORM=slopes (default) or
+ * staged (every cell computing its own slopes, flux_staged_tile) */
+static inline int flux_form()
+{
+    static int f = [] {
+        const char *e = getenv("VH_FLUX_FORM");
+        return (e && e[0] == 's' && e[1] == 't') ? 0 : 1;
+    }();
+    return f;
+}
+
 /* staged flux on (default) or off: VH_FLUX_STAGED=0 selects the kernel that
  * reads the stencil straight from device memory */
 static inline bool flux_staged()
@@ -194,6 +233,13 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
         kt_flux_face_kernel<NQ, EOS, 2><<<face_grid<2>(a), fb, 0, s>>>(a);
         mark(2);
         if (z) { kt_flux_face_kernel<NQ, EOS, 3><<<face_grid<3>(a), fb, 0, s>>>(a); mark(3); }
+    } else if (flux_staged() && flux_form() != 0) {
+        const dim3 g3((a.nx + 31) / 32, a.ny, (a.nz + 3) / 4);
+        launch_flux_slopes<NQ, EOS, 1>(a, grid, block, s);
+        mark(1);
+        launch_flux_slopes<NQ, EOS, 2>(a, grid, block, s);
+        mark(2);
+        if (z) { launch_flux_slopes<NQ, EOS, 3>(a, g3, block, s); mark(3); }
     } else if (flux_staged()) {
         const dim3 g3((a.nx + 31) / 32, a.ny, (a.nz + 3) / 4);
         kt_flux_staged_kernel<NQ, EOS, 1><<<grid, block, 0, s>>>(a);

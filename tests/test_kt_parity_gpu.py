@@ -96,14 +96,15 @@ print("LAUNCHES", gpu.launches_per_step(), "BAD", bad)
 """
 
 
-@pytest.mark.parametrize("env", [{}, {"VH_FLUX_STAGED": "0"}, {"VH_STAGE_MODE": "fused"},
+@pytest.mark.parametrize("env", [{}, {"VH_FLUX_FORM": "staged"}, {"VH_FLUX_STAGED": "0"}, {"VH_STAGE_MODE": "fused"},
                                  {"VH_STAGE_MODE": "fused", "VH_STAGE_FACES": "0"}],
-                         ids=["split-staged", "split-global", "fused-faces", "fused-one-thread"])
+                         ids=["split-slopes", "split-staged", "split-global", "fused-faces", "fused-one-thread"])
 def test_large_lattice_forms_bitexact(env):
     """above 2^15 cells the stage runs phase-split, its flux reading a
-    shared-memory tile by default; below, fused with one thread per face; every
-    form must equal the oracle bit for bit on the same lattice (run in a child
-    process: the form is chosen once per process)"""
+    shared-memory tile with the half slopes computed once per tile by default
+    (or each cell computing its own: staged); below, fused with one thread per
+    face; every form must equal the oracle bit for bit on the same lattice (run
+    in a child process: the form is chosen once per process)"""
     import os
     import subprocess
     import sys
