@@ -17,7 +17,12 @@
  * Host code must not use the array's name as an address (on the host it is a
  * stand-in symbol); the device address is looked up once per device with
  * cudaGetSymbolAddress, with that device current, on the first call made on
- * it.  That first call should therefore come before any stream capture.
+ * it (and again if that device's context was destroyed and re-created since).
+ * That first call should therefore come before any stream capture.
+ *
+ * If the elements do not fit in cap_elements, the first cap_elements of them
+ * (in cube order) are written and *d_n_elements still receives the full total,
+ * so a caller detects truncation by comparing it with cap_elements.
  * Every call on a device shares the one array and leaves its contents behind;
  * each call re-zeroes what must start at zero, and calls whose work overlaps
  * on the GPU (different streams, no ordering between them) race on it.
@@ -97,19 +102,44 @@ __global__ void noalloc_finish_kernel(int *n_elements)
     *n_elements = hdr[1] ? -1 : hdr[0];
 }
 
-/* device address of g_noalloc_scratch, looked up once per device */
+/* device address of g_noalloc_scratch, looked up once per device and
+ * context: a context that is torn down and created again (cudaDeviceReset,
+ * or a primary context released by its last user) may load the module at
+ * another address, so the cached address is tied to the context it was
+ * looked up in.  The current context comes from the driver's
+ * cuCtxGetCurrent, reached through the runtime so that the library does not
+ * link the driver library. */
+typedef int (*CtxGetCurrentFn)(void **);
 static std::mutex g_sym_mu;
 static int *g_sym_addr[64];
+static void *g_sym_ctx[64];
+
+static void *current_context()
+{
+    static CtxGetCurrentFn fn = [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return (CtxGetCurrentFn)p;
+    }();
+    void *ctx = nullptr;
+    if (fn && fn(&ctx) != 0) ctx = nullptr;
+    return ctx;
+}
 
 static cudaError_t scratch_address(int dev, int **out)
 {
     std::lock_guard<std::mutex> lk(g_sym_mu);
     if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
-    if (!g_sym_addr[dev]) {
+    void *ctx = current_context();
+    if (!g_sym_addr[dev] || g_sym_ctx[dev] != ctx) {
         int *p = nullptr;
         cudaError_t rc = cudaGetSymbolAddress((void **)&p, g_noalloc_scratch);
         if (rc != cudaSuccess) return rc;
         g_sym_addr[dev] = p;
+        g_sym_ctx[dev] = current_context();   /* the lookup made the primary context current if none was */
     }
     *out = g_sym_addr[dev];
     return cudaSuccess;
@@ -121,7 +151,7 @@ extern "C" int vh_cornelius_surfaces_noalloc(int dim, const double *d_cubes, int
                                              const double *dx, double *d_elements, int cap_elements,
                                              int *d_counts, int *d_n_elements, void *stream)
 {
-    if ((dim != 3 && dim != 4) || n_cubes < 0 || !d_cubes || !dx || !d_counts || !d_n_elements ||
+    if ((dim != 3 && dim != 4) || n_cubes < 0 || (n_cubes > 0 && (!d_cubes || !d_counts)) || !dx || !d_n_elements ||
         (cap_elements > 0 && !d_elements) || cap_elements < 0)
         return vh::set_error(VH_ERR_ARG, "vh_cornelius_surfaces_noalloc: bad argument");
     if (n_cubes > VH_NOALLOC_MAX_CUBES)

@@ -366,6 +366,10 @@ int vh_cornelius_surfaces(int dim, const double *cubes, int n_cubes, double valu
  * layout as above), d_elements (cap_elements x 2*dim doubles, compacted in cube
  * order), d_counts (n_cubes ints) and d_n_elements (one int: the total, or -1
  * after a Cornelius construction error); dx is a host array of dim spacings.
+ * When the total exceeds cap_elements, only the first cap_elements elements
+ * are written and *d_n_elements still holds the total: the output is then
+ * truncated, which the caller detects by comparing the two (the allocating
+ * entry point returns VH_ERR_CAPACITY instead).
  * Work is queued on `stream` (a cudaStream_t, 0 for the legacy stream) and the
  * call returns without waiting; read the outputs after synchronising.
  * The library's working memory is a fixed device array of about 1 MiB held by

@@ -59,6 +59,33 @@ def test_noalloc_matches_allocating_entry_point_twice_in_a_row():
         np.testing.assert_array_equal(el.view(np.uint64), ref_el.view(np.uint64))
 
 
+def test_noalloc_truncates_to_cap_and_reports_the_total():
+    """cap below the total: the first cap elements (cube order) are written and
+    the total still comes back, so the caller sees the truncation"""
+    cubes = K.random_cubes(3, 2000)
+    ref_el, ref_counts = vh.cornelius_surfaces(3, cubes, 0.5, np.ones(3))
+    cap = len(ref_el) // 3
+    el, counts, n = _noalloc(3, cubes, cap=cap)
+    assert n == len(ref_el) > cap
+    np.testing.assert_array_equal(counts, ref_counts)
+    np.testing.assert_array_equal(el[:cap].view(np.uint64), ref_el[:cap].view(np.uint64))
+
+
+def test_noalloc_header_reset_between_calls():
+    """no cubes gives zero elements; a call with fewer cubes after a larger one
+    reports only its own elements (the shared header and counts start again)"""
+    big = K.random_cubes(4, 3000)
+    _noalloc(4, big, cap=1)
+    el, counts, n = _noalloc(4, big[:0], cap=0)
+    assert n == 0 and len(counts) == 0
+    small = big[:200]
+    ref_el, ref_counts = vh.cornelius_surfaces(4, small, 0.5, np.ones(4))
+    el, counts, n = _noalloc(4, small, cap=len(ref_el) + 4)
+    assert n == len(ref_el)
+    np.testing.assert_array_equal(counts, ref_counts)
+    np.testing.assert_array_equal(el.view(np.uint64), ref_el.view(np.uint64))
+
+
 def test_noalloc_rejects_batches_over_the_limit():
     dummy = C.c_void_p(1)
     dx = np.ones(3)
