@@ -400,7 +400,19 @@ int autotune(vh_batch *b)
      * noise to matter (under 2 ms); large batches are timed once */
     const int max_rounds = 2;
     const int ncand = kNumShapes * 2;
-    std::vector<vh::StageMarks> mk((size_t)max_rounds * ncand * 2);
+    /* the timing events, destroyed on every return (value-initialised, so an
+     * event that was never created is null) */
+    struct Marks {
+        std::vector<vh::StageMarks> v;
+        explicit Marks(size_t n) : v(n) {}
+        ~Marks()
+        {
+            for (auto &m : v)
+                for (cudaEvent_t e : m.ev)
+                    if (e) cudaEventDestroy(e);
+        }
+    } marks((size_t)max_rounds * ncand * 2);
+    std::vector<vh::StageMarks> &mk = marks.v;
     for (auto &m : mk)
         for (cudaEvent_t &e : m.ev) BTRY(cudaEventCreate(&e));
     double best[VH_NPHASES];
@@ -435,8 +447,6 @@ int autotune(vh_batch *b)
                                 best[VH_PHASE_FINAL] + (b->any_z ? best[VH_PHASE_FLUX_ETA] : 0.0);
         if (std::min(best[VH_PHASE_FUSED], split_ms) > 2.0) break;
     }
-    for (auto &m : mk)
-        for (cudaEvent_t e : m.ev) cudaEventDestroy(e);
     double split = best[VH_PHASE_SOURCE] + best[VH_PHASE_FLUX_X] + best[VH_PHASE_FLUX_Y] + best[VH_PHASE_FINAL] +
                    (b->any_z ? best[VH_PHASE_FLUX_ETA] : 0.0);
     vh_batch_tuning t{};
