@@ -573,7 +573,7 @@ def run_reference(args):
                               "sample": f"{k1} RK2 steps of the event after 1 warm-up step"}
         del one
         shipped = variant + "_shipped"
-        if O.ref_available(shipped):
+        if O.ref_available(shipped) and O.shipped_runs_here():
             sh = make_refs(shipped, threads)
             k2, s2 = _ref_steps_timed(sh, args, 30.0)
             line["shipped_flags"] = {"value": N * k2 / s2, "unit": "cell-updates/s", "cores": threads,

@@ -278,6 +278,16 @@ def load_gen_lib(path: str):
     return _gen_sigs(C.CDLL(path))
 
 
+def shipped_runs_here() -> bool:
+    """the *_shipped libraries are built for Sapphire Rapids class x86-64
+    (AVX-512 incl. FP16, AMX): only load them on a host that has those"""
+    try:
+        flags = set(open("/proc/cpuinfo").read().split())
+    except OSError:
+        return False
+    return {"avx512f", "avx512bw", "avx512vl", "avx512_fp16", "amx_tile"} <= flags
+
+
 def shipped_build_flags() -> str:
     """how the *_shipped reference libraries were compiled (oracle/ref.mk)"""
     p = os.path.join(REF_DIR, "shipped_flags.txt")

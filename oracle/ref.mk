@@ -41,9 +41,11 @@ DEFS_stock = -DVH_THETA=1.1 -DVH_EOS_FACTOR=13.8997
 # (CMakeLists.txt:14: -O3 -fopenmp -std=c++11 -march=native, with GCC's own
 # multiply-add contraction), for the benchmark's timing only: its arithmetic
 # is then compiler-dependent, so no parity test uses it.  -march names the
-# GPU hosts' processor family (native to the build host would not run on
-# every host the library travels to).
-SHIPPED_MARCH ?= x86-64-v3
+# GPU hosts' processor family (native to the build host might not run on
+# every host the library travels to): the GPU hosts' Xeons (Sapphire and
+# Emerald Rapids) run sapphirerapids code; bench.py checks the host's flags
+# before it loads this library.
+SHIPPED_MARCH ?= sapphirerapids
 CXXFLAGS_SHIPPED = -O3 -fopenmp -std=c++11 -march=$(SHIPPED_MARCH) -fPIC -w \
                    -I$(REF)/rhic/include -I$(REF)/freezeout -include oracle/ref_shim.h
 

@@ -13,6 +13,9 @@
  *
  * Lattice layout: padded SoA arrays of ncx*ncy*ncz doubles, index
  * i + ncx*(j + ncy*k) (DynamicalVariables.cpp:35-41), two ghost cells a side.
+ *
+ * The per-cell loops run under OpenMP (each cell writes only itself, so the
+ * results do not depend on the thread count); error flags are reduced.
  */
 #include <math.h>
 #include <stdio.h>
@@ -461,6 +464,7 @@ static int IDX(const vho_t *h, int i, int j, int k) { return i + h->ncx * (j + h
 /* FullyDiscreteKurganovTadmorScheme.cpp:155-298 */
 static void euler_source(vho_t *h, double t, double **cur, double **upd, double **uu, double **upv)
 {
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = 2; k < h->ncz - 2; ++k)
         for (int j = 2; j < h->ncy - 2; ++j)
             for (int i = 2; i < h->ncx - 2; ++i) {
@@ -477,6 +481,8 @@ static void euler_dir(vho_t *h, double t, double **cur, double **upd, double **u
 {
     int stride = (dir == 1) ? 1 : (dir == 2) ? h->ncx : h->ncx * h->ncy;
     double d = (dir == 1) ? h->dx : (dir == 2) ? h->dy : h->dz;
+    int bad = 0;
+#pragma omp parallel for collapse(2) schedule(static) reduction(| : bad)
     for (int k = 2; k < h->ncz - 2; ++k)
         for (int j = 2; j < h->ncy - 2; ++j)
             for (int i = 2; i < h->ncx - 2; ++i) {
@@ -489,20 +495,22 @@ static void euler_dir(vho_t *h, double t, double **cur, double **upd, double **u
                     I[5 * n + 3] = cur[n][s + stride];
                     I[5 * n + 4] = cur[n][s + 2 * stride];
                 }
-                flux(h, I, H, 1, dir, t, h->e[s], &h->nan_flag);
+                flux(h, I, H, 1, dir, t, h->e[s], &bad);
                 for (int n = 0; n < h->nq; ++n) result[n] = -H[n];
-                flux(h, I, H, 0, dir, t, h->e[s], &h->nan_flag);
+                flux(h, I, H, 0, dir, t, h->e[s], &bad);
                 for (int n = 0; n < h->nq; ++n) { result[n] += H[n]; result[n] /= d; }
                 sources_dir(h, I, H, uu, s, t, d, dir);
                 for (int n = 0; n < 4; ++n) { result[n] += H[n]; result[n] *= h->dt; }
                 for (int n = 4; n < h->nq; ++n) result[n] *= h->dt;
                 for (int n = 0; n < h->nq; ++n) upd[n][s] += result[n];
             }
+    if (bad) h->nan_flag = 1;
 }
 
 /* FullyDiscreteKurganovTadmorScheme.cpp:638-686 */
 static void convex(vho_t *h, double **qq, double **QQ)
 {
+#pragma omp parallel for collapse(2) schedule(static)
     for (int k = 2; k < h->ncz - 2; ++k)
         for (int j = 2; j < h->ncy - 2; ++j)
             for (int i = 2; i < h->ncx - 2; ++i) {
@@ -514,16 +522,19 @@ static void convex(vho_t *h, double **qq, double **QQ)
 /* EnergyMomentumTensor.cpp:235-287 */
 static void set_inferred(vho_t *h, double **qq, double **uu, double t)
 {
+    int bad = 0;
+#pragma omp parallel for collapse(2) schedule(static) reduction(| : bad)
     for (int k = 2; k < h->ncz - 2; ++k)
         for (int j = 2; j < h->ncy - 2; ++j)
             for (int i = 2; i < h->ncx - 2; ++i) {
                 int s = IDX(h, i, j, k);
                 double qs[MAXQ], e_, p_, ut, ux, uy, un;
                 for (int n = 0; n < h->nq; ++n) qs[n] = qq[n][s];
-                inferred(h, t, qs, h->e[s], &e_, &p_, &ut, &ux, &uy, &un, &h->nan_flag);
+                inferred(h, t, qs, h->e[s], &e_, &p_, &ut, &ux, &uy, &un, &bad);
                 h->e[s] = e_; h->p[s] = p_;
                 uu[0][s] = ut; uu[1][s] = ux; uu[2][s] = uy; uu[3][s] = un;
             }
+    if (bad) h->nan_flag = 1;
 }
 
 /* FullyDiscreteKurganovTadmorScheme.cpp:690-859 (REG_SCHEME_1) */
@@ -534,6 +545,8 @@ static void regulate(vho_t *h, double t, double **qq, double **uu)
         h->regfac[0] = (double *)calloc(len, 8);
         h->regfac[1] = (double *)calloc(len, 8);
     }
+    int bad = 0;
+#pragma omp parallel for collapse(2) schedule(static) reduction(| : bad)
     for (int k = 2; k < h->ncz - 2; ++k)
         for (int j = 2; j < h->ncy - 2; ++j)
             for (int i = 2; i < h->ncx - 2; ++i) {
@@ -568,9 +581,10 @@ static void regulate(vho_t *h, double t, double **qq, double **uu)
                 if (h->e[s] > h->e_reg) { facShear = 1.0; facBulk = 1.0; }
                 for (int n = 4; n < 14; ++n) qq[n][s] *= facShear;
                 h->regfac[0][s] = facShear;
-                if (isnan(facShear)) h->nan_flag = 1;
-                if (h->bulk) { qq[14][s] *= facBulk; h->regfac[1][s] = facBulk; if (isnan(facBulk)) h->nan_flag = 1; }
+                if (isnan(facShear)) bad = 1;
+                if (h->bulk) { qq[14][s] *= facBulk; h->regfac[1][s] = facBulk; if (isnan(facBulk)) bad = 1; }
             }
+    if (bad) h->nan_flag = 1;
 }
 
 /* DynamicalVariables.cpp:220-378, the face ghosts only: corner and edge ghost
