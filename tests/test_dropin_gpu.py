@@ -31,18 +31,22 @@ def _driver(tmp):
     return exe
 
 
-def test_dropin_surface_matches_reference(tmp_path):
+@pytest.mark.parametrize("case", ["2p1d", "3p1d"])
+def test_dropin_surface_matches_reference(case, tmp_path):
+    """2+1D (callFOFinder2p1D) and 3+1D (callFOFinder3p1D, FreezeOut.cpp:200-280)
+    runs to the reference's stop rule"""
     tmp = str(tmp_path)
     exe = _driver(tmp)
-    shutil.copytree(dropin_case.CONF, os.path.join(tmp, "rhic-conf"))
+    c = dropin_case.CASES[case]
+    shutil.copytree(c["conf"], os.path.join(tmp, "rhic-conf"))
     os.makedirs(os.path.join(tmp, "cpu-vh_output"))
-    dropin_case.e_vector().tofile(os.path.join(tmp, "e.bin"))
+    dropin_case.e_vector(case).tofile(os.path.join(tmp, "e.bin"))
     r = subprocess.run([exe, "e.bin"], cwd=tmp, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert "All cells have dropped below freezeout energy density" in r.stdout
     with open(os.path.join(tmp, "cpu-vh_output", "surface.dat"), "rb") as f:
         data = f.read()
-    with open(dropin_case.GOLDEN) as f:
+    with open(c["golden"]) as f:
         gold = json.load(f)
     assert data.count(b"\n") == gold["rows"]
     assert hashlib.sha256(data).hexdigest() == gold["sha256"]

@@ -197,3 +197,67 @@ def test_regulation_factors_bitexact_vs_reference(case, variant):
     for f in ((400, 401) if cfg.bulk else (400,)):
         a, b = vh.interior(cfg, ref.field(f)), vh.interior(cfg, orc.field(f))
         assert np.count_nonzero(a.view(np.uint64) != b.view(np.uint64)) == 0, (case, f)
+
+
+# ------------------------------------------------- the shipped HotQCD EoS
+import hotqcd_eos_prefix as HQ  # noqa: E402
+
+
+def hotqcd_glauber():
+    """a small 3+1D Glauber event (bulk on) on the reference's shipped EoS"""
+    cfg = vh.glauber_config(19, 17, 7)
+    cfg.dx = cfg.dy = 0.7
+    cfg.dz = 0.5
+    cfg.dt = 0.05
+    return cfg
+
+
+@pytest.mark.skipif(not os.path.exists(HQ.full_table_path()), reason="the reference's EoS file is not here")
+def test_hotqcd_table_oracle_vs_reference():
+    """the oracle on the reference's shipped 100 000-record HotQCD table
+    (loaded as EquationOfState.cpp:292-327 loads it) equals the reference's
+    own code: steps and freezeout blocks"""
+    if not O.ref_available("table"):
+        pytest.skip("reference build not present")
+    full = HQ.load_full()
+    cfg = hotqcd_glauber()
+    st = vh.glauber_ic(cfg, full)
+    # one thread: the reference's cells-above count (checkForCellsAboveTc,
+    # FreezeOut.cpp:368-378) increments a shared counter inside `omp parallel
+    # for` without a reduction, so with more threads it loses increments
+    ref = O.RefEvent("table", cfg, full, threads=1)
+    orc = O.OracleEvent(cfg, full)
+    ref.set_initial(st)
+    orc.set_initial(st)
+    with tempfile.TemporaryDirectory() as d:
+        for blk in range(4):
+            path = os.path.join(d, f"s{blk}.dat")
+            above_ref = ref.freezeout(path)
+            el_orc, above_orc = orc.freezeout()
+            assert above_ref == above_orc
+            np.testing.assert_array_equal(_parse_surface(path).view(np.uint64), el_orc.view(np.uint64))
+            ref.step(3)
+            assert orc.step(3) == 0
+            for f in FIELDS(orc.nq):
+                assert _same(cfg, ref.field(f), orc.field(f)) == 0, (blk, f)
+
+
+@pytest.mark.skipif(not os.path.exists(HQ.full_table_path()), reason="the reference's EoS file is not here")
+def test_hotqcd_prefix_evolves_like_the_full_table():
+    """the committed 2000-record prefix gives the same evolution as the full
+    table for the test events (energy densities stay inside the prefix), and
+    the prefix equals the first records of the shipped file"""
+    full, pre = HQ.load_full(), HQ.load_prefix()
+    np.testing.assert_array_equal(pre, full[:len(pre)])
+    cfg = hotqcd_glauber()
+    st = vh.glauber_ic(cfg, full)
+    assert np.array_equal(st.e, vh.glauber_ic(cfg, pre).e)
+    a, b = O.OracleEvent(cfg, full), O.OracleEvent(cfg, pre)
+    a.set_initial(st)
+    b.set_initial(st)
+    for n in (2, 8):
+        assert a.step(n) == 0 and b.step(n) == 0
+        e = vh.interior(cfg, a.field(100))
+        assert e.max() * 0.197326938 < pre[-3, 0]
+        for f in FIELDS(a.nq):
+            assert _same(cfg, a.field(f), b.field(f)) == 0, (n, f)
