@@ -371,6 +371,160 @@ __device__ __forceinline__ void flux_slopes_tile(const StageArgs &A, int i0, int
     if (bad) raise_error(A.err, kErrNan, s, A.step);
 }
 
+/* ---------------------------------------------------------------------
+ * The flux along DIR over lines: the lattice is cut into lines along DIR,
+ * and the lines into bundles of W adjacent x-columns (W = 1 for DIR 1,
+ * where a line is a row of contiguous x; W = 4 for DIR 2 and 3, so that a
+ * warp's loads cover whole 32-byte sectors).  Run positions R = pos + nd *
+ * bundle enumerate (position along DIR, bundle); a block takes PB = 128 / W
+ * consecutive run positions times W columns, which may span the end of one
+ * line and the start of the next.  Every thread therefore has a cell (131
+ * cells a line no longer leave 29 of 160 lanes idle as 32-wide tiles do).
+ * Shared memory holds, per component, each line piece the block touches
+ * with its 2-cell halo at both ends (a "slot"), W values per position, and
+ * the half slopes at the same indices.
+ * --------------------------------------------------------------------- */
+template <int DIR>
+struct FluxLines {
+    static constexpr int W = (DIR == 1) ? 1 : 4;
+    static constexpr int PB = 128 / W;
+    /* line pieces one block can touch, for lines of nd cells */
+    static __host__ __device__ int max_slots(int nd) { return (PB - 1) / nd + 2; }
+    /* doubles per component of the staged values (and of the half slopes) */
+    static __host__ __device__ int plane(int nd) { return (PB + 4 * max_slots(nd)) * W; }
+    static __host__ __device__ long long bundles(int nx, int ny, int nz)
+    {
+        const long long nxq = (nx + W - 1) / W;
+        return (DIR == 1) ? (long long)ny * nz : (DIR == 2) ? nxq * nz : nxq * ny;
+    }
+};
+
+template <int NQ, int EOS, int DIR>
+__device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__restrict__ sm)
+{
+    using G = FluxLines<DIR>;
+    constexpr int W = G::W, PB = G::PB;
+    const int nd = (DIR == 1) ? A.nx : (DIR == 2) ? A.ny : A.nz;
+    const int PS = G::plane(nd);
+    double *__restrict__ hs = sm + NQ * PS;
+    const long long sxy = (long long)A.ncx * A.ncy;
+    const long long gst = (DIR == 1) ? 1 : (DIR == 2) ? (long long)A.ncx : sxy;
+    const int nxq = (A.nx + W - 1) / W;
+    const long long nbund = G::bundles(A.nx, A.ny, A.nz);
+    const long long Rtot = (long long)nd * nbund;
+    const long long R0 = (long long)blockIdx.x * PB;
+    const long long b0 = R0 / nd;
+    const int p0 = (int)(R0 - b0 * nd);
+    const int tid = threadIdx.x;
+    /* padded address of bundle b's column w at position -2 along DIR, or -1
+     * if that column is outside the lattice */
+    auto base = [&](long long b, int w) -> long long {
+        if (DIR == 1) {
+            const long long j = b % A.ny, k = b / A.ny;
+            return A.ncx * (j + 2) + sxy * (k + 2);
+        }
+        const long long xq = b % nxq, o = b / nxq;
+        const int x = (int)xq * W + w;
+        if (x >= A.nx) return -1;
+        return (DIR == 2) ? (x + 2) + sxy * (o + 2) : (x + 2) + A.ncx * (o + 2);
+    };
+    /* staging: slot l covers positions [first_l - 2, first_l + len_l + 2) of
+     * bundle b0 + l at shared indices [M_l, M_l + len_l + 4) */
+    const int mlen_max = PS / W;
+    for (int r = tid; r < mlen_max * W; r += 128) {
+        const int m = r / W, w = r - m * W;
+        int l = 0, M = 0, first = p0, left = PB;
+        long long off = -1;
+        for (; l < G::max_slots(nd) && left > 0; ++l) {
+            const int len = (nd - first < left) ? nd - first : left;
+            if (m < M + len + 4) {
+                if (b0 + l < nbund) {
+                    const long long bb = base(b0 + l, w);
+                    if (bb >= 0) off = bb + (long long)(first + (m - M)) * gst;
+                }
+                break;
+            }
+            M += len + 4;
+            left -= len;
+            first = 0;
+        }
+        if (off >= 0) {
+#pragma unroll 1
+            for (int n = 0; n < NQ; ++n) cp_async8(sm + n * PS + r, A.qin + n * A.L + off);
+        }
+    }
+    cp_async_wait_all();
+    __syncthreads();
+    const double th = A.theta;
+    for (int r = tid + W; r < (mlen_max - 1) * W; r += 128) {
+#pragma unroll 1
+        for (int n = 0; n < NQ; ++n) {
+            const double *q = sm + n * PS + r;
+            hs[n * PS + r] = approx_deriv(th, q[-W], q[0], q[W]) / 2;
+        }
+    }
+    __syncthreads();
+    /* this thread's cell */
+    const int w = tid % W, pr = tid / W;
+    const long long R = R0 + pr;
+    if (R >= Rtot) return;
+    const long long b = R / nd;
+    const int pos = (int)(R - b * nd);
+    const long long bb = base(b, w);
+    if (bb < 0) return;
+    const long long s = bb + (long long)(pos + 2) * gst;
+    const int ts = ((int)(R - R0) + 2 + 4 * (int)(b - b0)) * W + w;
+    constexpr int tst = W;
+    const QTile qt{sm, PS};
+    const double ePrev = __ldg(A.ein + s);
+    bool bad = false;
+    /* states m = 0..3: forward face R, L; backward face R, L */
+    double ut0 = 0, ut1 = 0, ut2 = 0, ut3 = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0;
+#pragma unroll 1
+    for (int mm = 0; mm < 4; ++mm) {
+        const int o = (mm == 0) ? ts + tst : (mm == 3) ? ts - tst : ts;
+        const bool minus = (mm & 1) == 0;        /* R states subtract the half slope */
+        double st[9];
+#pragma unroll
+        for (int c = 0; c < 9; ++c) {
+            const int n = (c < 8) ? c : 14;
+            if (n >= NQ) { st[c] = 0; continue; }
+            const double qv = sm[n * PS + o], hv = hs[n * PS + o];
+            st[c] = minus ? qv - hv : qv + hv;
+        }
+        const Prim Pm = infer<EOS, true>(A.eos, A.t, st[0] - st[4], st[1] - st[5], st[2] - st[6], st[3] - st[7],
+                                         st[8], ePrev, bad);
+        const double vm = (DIR == 1) ? Pm.ux : (DIR == 2) ? Pm.uy : Pm.un;
+        if (mm == 0) { ut0 = Pm.ut; v0 = vm; }
+        else if (mm == 1) { ut1 = Pm.ut; v1 = vm; }
+        else if (mm == 2) { ut2 = Pm.ut; v2 = vm; }
+        else { ut3 = Pm.ut; v3 = vm; }
+    }
+    const double y0 = 1.0 / ut0, y1 = 1.0 / ut1, y2 = 1.0 / ut2, y3 = 1.0 / ut3;
+    const double af = fmax(fabs(div_rcp(v1, ut1, y1)), fabs(div_rcp(v0, ut0, y0)));
+    const double ab = fmax(fabs(div_rcp(v3, ut3, y3)), fabs(div_rcp(v2, ut2, y2)));
+    const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
+    const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
+    double S[4];
+    dir_sources_t<NQ>(A, qt, ts, tst, s, d, DIR, S);
+#pragma unroll 1
+    for (int n = 0; n < NQ; ++n) {
+        const double *q = sm + n * PS + ts, *h = hs + n * PS + ts;
+        const double Rf = q[tst] - h[tst], Lf = q[0] + h[0], Rb = q[0] - h[0], Lb = q[-tst] + h[-tst];
+        double rf = div_rcp(v0 * Rf, ut0, y0) + div_rcp(v1 * Lf, ut1, y1) - af * (Rf - Lf);
+        rf /= 2;
+        double rb = div_rcp(v2 * Rb, ut2, y2) + div_rcp(v3 * Lb, ut3, y3) - ab * (Rb - Lb);
+        rb /= 2;
+        double r = -rf;
+        r = r + rb;
+        r = div_rcp(r, d, yd);
+        if (n < 4) r += (n == 0) ? S[0] : (n == 1) ? S[1] : (n == 2) ? S[2] : S[3];
+        r *= A.dt;
+        A.qout[n * A.L + s] += r;
+    }
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+}
+
 /* eulerStepKernelX/Y/Z (FullyDiscreteKurganovTadmorScheme.cpp:300-634), the
  * axes in the reference's order x, y, eta. */
 template <int NQ, int EOS, bool HAS_Z>

@@ -13,7 +13,9 @@
 namespace vh {
 
 #ifndef VH_STAGE_MIN_BLOCKS
-#define VH_STAGE_MIN_BLOCKS 4   /* 128 registers: 16 warps/SM; measured faster than 2-3 blocks at 168-255 */
+#define VH_STAGE_MIN_BLOCKS 4   /* 128 registers: 16 warps/SM; measured faster than 2-3 blocks at 168-255
+                                   (the source kernel, which spills 224 bytes at 128: 0.78 ms per launch
+                                   against 0.89 at 3 blocks and 168 registers) */
 #endif
 
 /* interior cell (i, j, k) of this thread, at padded index s */
@@ -23,6 +25,23 @@ __device__ __forceinline__ bool stage_cell(const StageArgs &A, int &i, int &j, i
     j = blockIdx.y * blockDim.y + threadIdx.y + 2;
     k = blockIdx.z + 2;
     if (i >= A.nx + 2 || j >= A.ny + 2) return false;
+    s = i + (long long)A.ncx * j + (long long)A.ncx * A.ncy * k;
+    return true;
+}
+
+/* the same for a 1-D grid over all nx*ny*nz interior cells, x fastest: no
+ * lane idles at the end of a row (the per-cell phases need no tile) */
+__device__ __forceinline__ bool stage_cell_flat(const StageArgs &A, int &i, int &j, int &k, long long &s)
+{
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nxy = (long long)A.nx * A.ny;
+    if (c >= nxy * A.nz) return false;
+    k = (int)(c / nxy);
+    const int r = (int)(c - (long long)k * nxy);
+    j = r / A.nx;
+    i = r - j * A.nx + 2;
+    j += 2;
+    k += 2;
     s = i + (long long)A.ncx * j + (long long)A.ncx * A.ncy * k;
     return true;
 }
@@ -45,7 +64,7 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_source_kernel(con
 {
     int i, j, k;
     long long s;
-    if (!stage_cell(A, i, j, k, s)) return;
+    if (!stage_cell_flat(A, i, j, k, s)) return;
     source_phase<NQ, EOS, MIXED>(A, s);
 }
 
@@ -125,13 +144,47 @@ static void launch_flux_slopes(const StageArgs &a, dim3 grid, dim3 block, cudaSt
     kt_flux_slopes_kernel<NQ, EOS, DIR><<<grid, block, bytes, s>>>(a);
 }
 
-/* FP64 flux form of the phase-split stage: VH_FLUX_FORM=slopes (default) or
- * staged (every cell computing its own slopes, flux_staged_tile) */
+/* the flux over line pieces (flux_lines_block): a 1-D grid of 128-thread
+ * blocks, dynamic shared memory 2 * NQ * FluxLines::plane(nd) doubles */
+template <int NQ, int EOS, int DIR, int MB>
+__global__ void __launch_bounds__(128, MB) kt_flux_lines_kernel(const __grid_constant__ StageArgs A)
+{
+    extern __shared__ double smd[];
+    flux_lines_block<NQ, EOS, DIR>(A, smd);
+}
+
+template <int NQ, int EOS, int DIR, int MB>
+static void launch_flux_lines(const StageArgs &a, cudaStream_t s)
+{
+    using G = FluxLines<DIR>;
+    const int nd = (DIR == 1) ? a.nx : (DIR == 2) ? a.ny : a.nz;
+    const size_t bytes = sizeof(double) * 2 * NQ * (size_t)G::plane(nd);
+    static size_t attr_bytes = 0;
+    if (bytes > attr_bytes) {
+        cudaFuncSetAttribute(kt_flux_lines_kernel<NQ, EOS, DIR, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)bytes);
+        cudaFuncSetAttribute(kt_flux_lines_kernel<NQ, EOS, DIR, MB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             100);
+        attr_bytes = bytes;
+    }
+    const long long runs = (long long)nd * G::bundles(a.nx, a.ny, a.nz);
+    const unsigned blocks = (unsigned)((runs + G::PB - 1) / G::PB);
+    kt_flux_lines_kernel<NQ, EOS, DIR, MB><<<blocks, 128, bytes, s>>>(a);
+}
+
+/* FP64 flux form of the phase-split stage: VH_FLUX_FORM=lines (default:
+ * line pieces, 5 blocks per SM at 96 registers), lines4 (4 blocks per SM,
+ * up to 128 registers), slopes (32 x 4 tiles with shared half slopes) or
+ * staged (32 x 4 tiles, every cell computing its own slopes).  Measured on
+ * the 131x131x61 Glauber event (ms per x/y/eta launch): lines 0.75/0.86/0.87,
+ * lines4 0.89/0.98/0.99, slopes 0.98/1.00/1.03, staged 1.10/1.09/1.12. */
 static inline int flux_form()
 {
     static int f = [] {
         const char *e = getenv("VH_FLUX_FORM");
-        return (e && e[0] == 's' && e[1] == 't') ? 0 : 1;
+        if (!e) return 3;
+        if (e[0] == 'l') return e[5] == '4' ? 2 : 3;
+        return (e[0] == 's' && e[1] == 't') ? 0 : 1;
     }();
     return f;
 }
@@ -170,12 +223,16 @@ static inline dim3 face_grid(const StageArgs &a)
     return dim3((a.nx + kFaceTX - 1) / kFaceTX, a.ny, (a.nz + kFaceTY - 2) / (kFaceTY - 1));
 }
 
-template <int NQ, int EOS, bool HAS_Z, bool STAGE2>
+/* MIXED is part of the kernel's name although the body is the same: the
+ * FP64 and the mixed translation units compile it with different
+ * floating-point flags, and one name for two different device functions
+ * would leave it to the runtime which of the two a launch runs */
+template <int NQ, int EOS, bool HAS_Z, bool STAGE2, bool MIXED>
 __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_final_kernel(const __grid_constant__ StageArgs A)
 {
     int i, j, k;
     long long s;
-    if (!stage_cell(A, i, j, k, s)) return;
+    if (!stage_cell_flat(A, i, j, k, s)) return;
     final_body<NQ, EOS, HAS_Z, STAGE2>(A, i, j, k, s);
 }
 
@@ -224,7 +281,8 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
         mark(5);
         return;
     }
-    kt_source_kernel<NQ, EOS, MIXED><<<grid, block, 0, s>>>(a);
+    const dim3 gflat((unsigned)(((long long)a.nx * a.ny * a.nz + 127) / 128));
+    kt_source_kernel<NQ, EOS, MIXED><<<gflat, 128, 0, s>>>(a);
     mark(0);
     if constexpr (MIXED) {
         const dim3 fb(kFaceTX, kFaceTY, 1);
@@ -235,11 +293,25 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
         if (z) { kt_flux_face_kernel<NQ, EOS, 3><<<face_grid<3>(a), fb, 0, s>>>(a); mark(3); }
     } else if (flux_staged() && flux_form() != 0) {
         const dim3 g3((a.nx + 31) / 32, a.ny, (a.nz + 3) / 4);
-        launch_flux_slopes<NQ, EOS, 1>(a, grid, block, s);
-        mark(1);
-        launch_flux_slopes<NQ, EOS, 2>(a, grid, block, s);
-        mark(2);
-        if (z) { launch_flux_slopes<NQ, EOS, 3>(a, g3, block, s); mark(3); }
+        if (flux_form() == 2) {
+            launch_flux_lines<NQ, EOS, 1, 4>(a, s);
+            mark(1);
+            launch_flux_lines<NQ, EOS, 2, 4>(a, s);
+            mark(2);
+            if (z) { launch_flux_lines<NQ, EOS, 3, 4>(a, s); mark(3); }
+        } else if (flux_form() == 3) {
+            launch_flux_lines<NQ, EOS, 1, 5>(a, s);
+            mark(1);
+            launch_flux_lines<NQ, EOS, 2, 5>(a, s);
+            mark(2);
+            if (z) { launch_flux_lines<NQ, EOS, 3, 5>(a, s); mark(3); }
+        } else {
+            launch_flux_slopes<NQ, EOS, 1>(a, grid, block, s);
+            mark(1);
+            launch_flux_slopes<NQ, EOS, 2>(a, grid, block, s);
+            mark(2);
+            if (z) { launch_flux_slopes<NQ, EOS, 3>(a, g3, block, s); mark(3); }
+        }
     } else if (flux_staged()) {
         const dim3 g3((a.nx + 31) / 32, a.ny, (a.nz + 3) / 4);
         kt_flux_staged_kernel<NQ, EOS, 1><<<grid, block, 0, s>>>(a);
@@ -254,10 +326,10 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
         mark(2);
         if (z) { kt_flux_kernel<NQ, EOS, 3, MIXED><<<grid, block, 0, s>>>(a); mark(3); }
     }
-    if (z && st2) kt_final_kernel<NQ, EOS, true, true><<<grid, block, 0, s>>>(a);
-    else if (z) kt_final_kernel<NQ, EOS, true, false><<<grid, block, 0, s>>>(a);
-    else if (st2) kt_final_kernel<NQ, EOS, false, true><<<grid, block, 0, s>>>(a);
-    else kt_final_kernel<NQ, EOS, false, false><<<grid, block, 0, s>>>(a);
+    if (z && st2) kt_final_kernel<NQ, EOS, true, true, MIXED><<<gflat, 128, 0, s>>>(a);
+    else if (z) kt_final_kernel<NQ, EOS, true, false, MIXED><<<gflat, 128, 0, s>>>(a);
+    else if (st2) kt_final_kernel<NQ, EOS, false, true, MIXED><<<gflat, 128, 0, s>>>(a);
+    else kt_final_kernel<NQ, EOS, false, false, MIXED><<<gflat, 128, 0, s>>>(a);
     mark(4);
 }
 

@@ -206,3 +206,27 @@ def test_reference_pressure_of_the_initial_state_equals_the_library():
     st = O.glauber_state(cfg, ref.pressure)
     g = vh.glauber_config(15, 13, 5)
     assert _same_bits(st.p, vh.glauber_ic(g, rows).p)
+
+
+def test_no_kernel_name_in_two_floating_point_modes():
+    """the mixed-precision translation unit (vh_mixed.cu: FMA contraction,
+    fast FP32 division) and the FP64 ones (vh_kt.cu, vh_batch.cu: no
+    contraction) must not instantiate a kernel of the same name: two device
+    functions behind one launch stub leave it to the runtime which one runs
+    (a template without the precision among its parameters did, and the
+    mixed results then differed between processes)"""
+    import subprocess
+    build = os.path.join(ROOT, "cpu-vh_b200", "_build")
+    if not os.path.exists(os.path.join(build, "vh_mixed.o")):
+        pytest.skip("library objects not built here")
+
+    def kernels(obj):
+        out = subprocess.run(["nm", "-C", os.path.join(build, obj)], capture_output=True, text=True, check=True).stdout
+        return {ln.split(" ", 2)[2] for ln in out.splitlines()
+                if " W " in ln and "_kernel" in ln and ln.split(" ", 2)[2].startswith("void vh::")}
+
+    mixed = kernels("vh_mixed.o")
+    assert mixed, "no kernels found in vh_mixed.o"
+    for obj in ("vh_kt.o", "vh_batch.o"):
+        both = mixed & kernels(obj)
+        assert not both, (obj, sorted(both)[:5])
