@@ -109,10 +109,13 @@ void pool_live(int dev, int delta)
     if (P.live == 0 && P.holds == 0 && P.pool) cudaMemPoolTrimTo(P.pool, 0);
 }
 
-/* an event buffer, ordered on the event's stream.  VH_POISON_ALLOC=1 fills
- * every new buffer with all-ones bytes (a NaN in every double) before the
- * library's own initialisation, so that a value read before any kernel
- * wrote it shows up in the parity tests (a diagnostic, off by default). */
+/* an event buffer, ordered on the event's stream.  A diagnostic, off by
+ * default: VH_POISON_ALLOC=1 fills every new buffer with all-ones bytes (a
+ * NaN in every double), =2 with 0x7E bytes (1.4e301 in every double, 2.1e38
+ * in every float: finite, so fmin/fmax-based limiters and wave speeds do not
+ * discard it as they discard a NaN), before the library's own
+ * initialisation, so that a value read before any kernel wrote it changes the
+ * results the tests compare. */
 cudaError_t ev_alloc(vh_event *ev, void *ptr, size_t bytes)
 {
     cudaMemPool_t pool = nullptr;
@@ -121,7 +124,8 @@ cudaError_t ev_alloc(vh_event *ev, void *ptr, size_t bytes)
     e = cudaMallocFromPoolAsync(reinterpret_cast<void **>(ptr), bytes, pool, ev->stream);
     if (e == cudaSuccess) {
         const char *p = getenv("VH_POISON_ALLOC");
-        if (p && p[0] == '1') e = cudaMemsetAsync(*reinterpret_cast<void **>(ptr), 0xFF, bytes, ev->stream);
+        if (p && (p[0] == '1' || p[0] == '2'))
+            e = cudaMemsetAsync(*reinterpret_cast<void **>(ptr), p[0] == '1' ? 0xFF : 0x7E, bytes, ev->stream);
     }
     return e;
 }

@@ -574,6 +574,8 @@ def run_like_server(cfg: VhConfig, rows, st, max_steps: int = 0):
             zero += na == 0
         if zero >= 3 or (max_steps and steps >= max_steps):
             break
+    if status == VH_OK:
+        status = ev.status()[0]        # errors of the steps after the last block
     ev.close()
     return steps, (np.concatenate(parts) if parts else np.zeros((0, VH_FO_COLUMNS))), status
 
