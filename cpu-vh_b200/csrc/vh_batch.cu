@@ -65,11 +65,28 @@ __global__ void batch_prep_kernel(const __grid_constant__ BatchPrep P)
     const BatchMember &M = P.mem[e];
     const int n = P.nstep[e];
     StageArgs a = M.base, b = M.base;
+    /* an inactive member is not advanced: every tile of it is skipped, the
+     * phase kernels testing nx before any access (the state pointers of
+     * M.base are null) */
     if (!M.active || n >= M.tcap) {
-        a.nx = 0;                      /* every tile of the member is skipped */
+        a.nx = 0;
         b.nx = 0;
         P.args[e] = a;
         P.args[P.nmem + e] = b;
+        return;
+    }
+    /* a member whose device has flagged an error is not computed either --
+     * its state is invalid (the reference exits at its first NaN), and in
+     * garbage cells the root solves would run their 10^4 Newton and 10^6
+     * bisection iterations every step until the host reads the error -- but
+     * its step count advances as the host counts it, so that the buffer
+     * roles of host and device stay the same */
+    if (M.base.err.code && *M.base.err.code != 0) {
+        a.nx = 0;
+        b.nx = 0;
+        P.args[e] = a;
+        P.args[P.nmem + e] = b;
+        if (P.advance) P.nstep[e] = n + 1;
         return;
     }
     const long long L = M.base.L;

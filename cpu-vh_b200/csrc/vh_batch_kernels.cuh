@@ -76,6 +76,10 @@ __global__ void __launch_bounds__(kBatchFaceTX * kBatchFaceTY, 2) kt_batch_face_
             __syncthreads();
             cur = tile.x;
         }
+        /* an inactive member (nx = 0, and no state pointers in its
+         * arguments): skip its tiles -- flux_faces_tile would otherwise take
+         * the x face at index 2 for a valid face (uniform over the block) */
+        if (sA.nx == 0) continue;
         flux_faces_tile<NQ, EOS, DIR, kBatchFaceTX, kBatchFaceTY>(sA, tile.y, tile.z, tile.w, sm);
     }
 }

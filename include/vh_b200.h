@@ -250,7 +250,11 @@ typedef struct vh_batch_tuning {
 int vh_batch_create(vh_event *const *events, int n_events, vh_batch **out);
 int vh_batch_destroy(vh_batch *b);
 int vh_batch_size(vh_batch *b, int *n_events);
-/* nsteps RK2 steps of every active member (autotunes on the first call). */
+/* nsteps RK2 steps of every active member (autotunes on the first call).
+ * A member whose device has flagged an error (vh_event_status) is no longer
+ * computed by later steps (its state is invalid, as the reference's would be
+ * at its exit): its error stays, its energy density stays that of the
+ * failing step, and its step count advances with the batch. */
 int vh_batch_step(vh_batch *b, int nsteps);
 /* An inactive member is skipped (its tiles do no work) until re-activated. */
 int vh_batch_set_active(vh_batch *b, int member, int active);

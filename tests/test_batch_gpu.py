@@ -106,13 +106,20 @@ def test_mixed_2d_3d_batch_and_interleaved_single_steps():
     assert evs[0].progress()[0] == 7 and evs[1].progress()[0] == 5
 
 
-def test_inactive_member_is_frozen():
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_inactive_member_is_frozen(precision):
+    """an inactive member does not move (its tiles are skipped in every phase,
+    the mixed face-once flux included) and resumes where it stopped: its
+    state equals that of the same event stepped as often in a batch of its
+    own, and the other members equal a batch without it"""
     rows = vh.synthetic_eos_table()
     cfgs, ics = _hotspot_members([17, 25, 21], rows, seed0=21)
+    if precision == "mixed":
+        cfgs = [c.copy(precision=vh.VH_PREC_MIXED) for c in cfgs]
     evs = _events(cfgs, ics, rows)
-    ref = _events(cfgs, ics, rows)
     b = vh.Batch(evs)
     b.step(2)
+    evs[1].sync()
     before = evs[1].field(vh.VH_F_E).copy()
     b.set_active(1, False)
     b.step(3)
@@ -121,12 +128,22 @@ def test_inactive_member_is_frozen():
     assert evs[1].progress()[0] == 2
     b.set_active(1, True)
     b.step(1)
-    for r, n in zip(ref, [6, 3, 6]):
-        r.step(n)
-    for c, e, r in zip(cfgs, evs, ref):
+    ref_a = _events([cfgs[0], cfgs[2]], [ics[0], ics[2]], rows)
+    ref_b = _events([cfgs[1]], [ics[1]], rows)
+    ba, bb = vh.Batch(ref_a), vh.Batch(ref_b)
+    ba.step(6)
+    bb.step(3)
+    for c, e, r in ((cfgs[0], evs[0], ref_a[0]), (cfgs[1], evs[1], ref_b[0]), (cfgs[2], evs[2], ref_a[1])):
         e.sync()
         r.sync()
+        assert e.status()[0] == 0
         assert not _compare(c, e, r)
+    if precision == "fp64":
+        singles = _events(cfgs, ics, rows)
+        for c, e, r, n in zip(cfgs, evs, singles, [6, 3, 6]):
+            r.step(n)
+            r.sync()
+            assert not _compare(c, e, r)
 
 
 def test_freezeout_of_batched_member():

@@ -54,3 +54,29 @@ def test_failing_batch_member_is_isolated():
     assert evs[1].status()[0] == 0 and ref.status()[0] == 0
     a, r = evs[1].field(vh.VH_F_E), ref.field(vh.VH_F_E)
     assert np.array_equal(a.view(np.uint64), r.view(np.uint64))
+
+
+def test_failed_batch_member_is_not_advanced():
+    """a member whose device flagged an error is no longer computed while the
+    batch goes on (its root solves would otherwise grind on garbage): its
+    error and its energy density stay those of the failing step, and the
+    other members advance as usual"""
+    rows = vh.synthetic_eos_table()
+    cfgs = [vh.hotspot_config(n) for n in (23, 29)]
+    sts = [vh.hotspot_ic(c, rows, seed=80 + i) for i, c in enumerate(cfgs)]
+    evs = [vh.Event(c, rows) for c in cfgs]
+    evs[0].set_initial(_poisoned(cfgs[0], sts[0]))
+    evs[1].set_initial(sts[1])
+    b = vh.Batch(evs)
+    b.step(2)
+    assert evs[0].status()[0] == VH_ERR_NAN
+    rc0, step0, cell0 = evs[0].status()
+    frozen = evs[0].field(vh.VH_F_E).copy()
+    b.step(3)
+    assert evs[0].status() == (rc0, step0, cell0)
+    assert np.array_equal(evs[0].field(vh.VH_F_E).view(np.uint64), frozen.view(np.uint64))
+    ref = vh.Event(cfgs[1], rows)
+    ref.set_initial(sts[1])
+    ref.step(5)
+    assert evs[1].status()[0] == 0
+    assert np.array_equal(evs[1].field(vh.VH_F_E).view(np.uint64), ref.field(vh.VH_F_E).view(np.uint64))
