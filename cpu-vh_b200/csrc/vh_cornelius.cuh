@@ -10,11 +10,12 @@
  * and normals are the outward-oriented sums of their normals.  Every sum runs
  * in the reference's order so the element geometry is identical bit for bit.
  *
- * Storage is fixed-size per thread: lines are kept once (12 doubles each)
- * and polygons/polyhedra refer to them by index.  Capacities are the
- * reference's own array bounds (cornelius.h: 2 lines per square, 8 polygons
- * per cube, 10 polyhedra per hypercube, 24 lines per polygon and 24 polygons
- * per polyhedron); exceeding one raises an error instead of overrunning.
+ * Storage is fixed-size: lines are kept once (12 doubles each) and
+ * polygons/polyhedra refer to them by index, through a WorkRef (a view of
+ * one thread's Work).  Capacities are the reference's own array bounds
+ * (cornelius.h: 2 lines per square, 8 polygons per cube, 10 polyhedra per
+ * hypercube, 24 lines per polygon and 24 polygons per polyhedron); exceeding
+ * one raises an error instead of overrunning.
  *
  * MODIFIED VERSION of the Cornelius subroutine: restated in 2026 as CUDA
  * device code (one thread per cube or hypercube, fixed-size per-thread
@@ -57,13 +58,6 @@ constexpr int kMaxPolyLines = 12; /* lines of one polygon: at most the lines of 
 constexpr int kMaxHedra = 10;     /* Hypercube MAX_POLY, cornelius.cpp:1703 */
 constexpr int kMaxElements = 10;  /* Cornelius MAX_ELEMENTS, cornelius.cpp:2004 */
 
-struct Lines {
-    double p[kMaxLines][2][D];
-    double out[kMaxLines][D];
-    unsigned char flip[kMaxLines];
-    int n;
-};
-
 struct Poly {
     unsigned char line[kMaxPolyLines];
     int nlines, const_i, x1, x2, x3;
@@ -71,15 +65,31 @@ struct Poly {
     bool have_cen;
 };
 
+/* one thread's storage for a whole (hyper)cube */
 struct Work {
-    Lines L;
+    double p[kMaxLines][2][D];
+    double out[kMaxLines][D];
+    unsigned char flip[kMaxLines];
     Poly poly[kMaxPoly];
-    int npoly;
+};
+
+/* a view of line and polygon storage; nl and np count what was appended */
+struct WorkRef {
+    double (*p)[2][D];
+    double (*out)[D];
+    unsigned char *flip;
+    Poly *poly;
+    int nl, np, lcap, pcap;
     bool error;
 };
 
-__device__ __forceinline__ const double *lstart(const Work &w, int l) { return w.L.p[l][w.L.flip[l]]; }
-__device__ __forceinline__ const double *lend(const Work &w, int l) { return w.L.p[l][1 - w.L.flip[l]]; }
+__device__ __forceinline__ WorkRef work_ref(Work &w)
+{
+    return WorkRef{w.p, w.out, w.flip, w.poly, 0, 0, kMaxLines, kMaxPoly, false};
+}
+
+__device__ __forceinline__ const double *lstart(const WorkRef &w, int l) { return w.p[l][w.flip[l]]; }
+__device__ __forceinline__ const double *lend(const WorkRef &w, int l) { return w.p[l][1 - w.flip[l]]; }
 
 /* GeneralElement::check_normal_direction, cornelius.cpp:91-106 */
 __device__ __forceinline__ void orient(double *n, const double *out)
@@ -91,8 +101,8 @@ __device__ __forceinline__ void orient(double *n, const double *out)
 }
 
 /* Square::construct_lines with ends_of_edge and find_outside
- * (cornelius.cpp:1134-1337); appends its lines to w.L. */
-static __device__ void square_lines(Work &w, const double P[2][2], int c0, int c1, double v0_, double v1_, double E0, const double *dx)
+ * (cornelius.cpp:1134-1337); appends its lines to w. */
+static __device__ void square_lines(WorkRef &w, const double P[2][2], int c0, int c1, double v0_, double v1_, double E0, const double *dx)
 {
     int above = 0;
     for (int i = 0; i < 2; i++)
@@ -149,19 +159,19 @@ static __device__ void square_lines(Work &w, const double P[2][2], int c0, int c
     }
     (void)ambiguous;
     for (int k = 0; k < nc / 2; k++) {
-        if (w.L.n >= kMaxLines) { w.error = true; return; }
-        int l = w.L.n++;
+        if (w.nl >= w.lcap) { w.error = true; return; }
+        int l = w.nl++;
         for (int e = 0; e < 2; e++) {
-            w.L.p[l][e][x1] = cuts[2 * k + e][0];
-            w.L.p[l][e][x2] = cuts[2 * k + e][1];
-            w.L.p[l][e][c0] = v0_;
-            w.L.p[l][e][c1] = v1_;
+            w.p[l][e][x1] = cuts[2 * k + e][0];
+            w.p[l][e][x2] = cuts[2 * k + e][1];
+            w.p[l][e][c0] = v0_;
+            w.p[l][e][c1] = v1_;
         }
-        w.L.out[l][x1] = out[k][0];
-        w.L.out[l][x2] = out[k][1];
-        w.L.out[l][c0] = v0_;
-        w.L.out[l][c1] = v1_;
-        w.L.flip[l] = 0;
+        w.out[l][x1] = out[k][0];
+        w.out[l][x2] = out[k][1];
+        w.out[l][c0] = v0_;
+        w.out[l][c1] = v1_;
+        w.flip[l] = 0;
     }
 }
 
@@ -176,7 +186,7 @@ __device__ __forceinline__ void poly_init(Poly &p, int c)
 }
 
 /* Polygon::add_line, cornelius.cpp:436-471 */
-__device__ __forceinline__ bool poly_add_line(Work &w, Poly &p, int l, bool donotcheck)
+__device__ __forceinline__ bool poly_add_line(WorkRef &w, Poly &p, int l, bool donotcheck)
 {
     if (donotcheck || p.nlines == 0) {
         if (p.nlines >= kMaxPolyLines) { w.error = true; return false; }
@@ -187,7 +197,7 @@ __device__ __forceinline__ bool poly_add_line(Work &w, Poly &p, int l, bool dono
     double diff1 = 0, diff2 = 0;
     for (int j = 0; j < D; j++) { diff1 += fabs(p1[j] - p3[j]); diff2 += fabs(p2[j] - p3[j]); }
     if (diff1 < 1e-10 || diff2 < 1e-10) {
-        if (diff2 < 1e-10) w.L.flip[l] ^= 1;
+        if (diff2 < 1e-10) w.flip[l] ^= 1;
         if (p.nlines >= kMaxPolyLines) { w.error = true; return false; }
         p.line[p.nlines++] = (unsigned char)l;
         return true;
@@ -197,7 +207,7 @@ __device__ __forceinline__ bool poly_add_line(Work &w, Poly &p, int l, bool dono
 
 /* Polygon::calculate_centroid, cornelius.cpp:478-551 (pow(x, 2.0) is x*x:
  * the host libm returns the correctly rounded square) */
-static __device__ const double *poly_centroid(Work &w, Poly &p)
+static __device__ const double *poly_centroid(const WorkRef &w, Poly &p)
 {
     if (p.have_cen) return p.cen;
     double mean[D] = {0, 0, 0, 0};
@@ -230,7 +240,7 @@ static __device__ const double *poly_centroid(Work &w, Poly &p)
 }
 
 /* Polygon::calculate_normal, cornelius.cpp:559-617 */
-static __device__ void poly_normal(Work &w, Poly &p, double *normal)
+static __device__ void poly_normal(const WorkRef &w, Poly &p, double *normal)
 {
     const double *cen = poly_centroid(w, p);
     for (int i = 0; i < D; i++) normal[i] = 0;
@@ -243,7 +253,7 @@ static __device__ void poly_normal(Work &w, Poly &p, double *normal)
         n[p.x2] = -0.5 * (a[p.x1] * b[p.x3] - a[p.x3] * b[p.x1]);
         n[p.x3] = 0.5 * (a[p.x1] * b[p.x2] - a[p.x2] * b[p.x1]);
         n[p.const_i] = 0;
-        for (int j = 0; j < D; j++) vout[j] = w.L.out[p.line[i]][j] - cen[j];
+        for (int j = 0; j < D; j++) vout[j] = w.out[p.line[i]][j] - cen[j];
         orient(n, vout);
         for (int j = 0; j < D; j++) acc[i][j] = n[j];
     }
@@ -254,13 +264,13 @@ static __device__ void poly_normal(Work &w, Poly &p, double *normal)
 /* Cube::split_to_squares + construct_polygons + check_ambiguous
  * (cornelius.cpp:1502-1650).  Returns the cube's number of lines; its
  * polygons are appended to w.poly, and *ambiguous reports the cube flag. */
-static __device__ int cube_polygons(Work &w, const double cube[2][2][2], int const_i, double const_v, double E0,
+static __device__ int cube_polygons(WorkRef &w, const double cube[2][2][2], int const_i, double const_v, double E0,
                              const double *dx, bool *ambiguous)
 {
     int x1 = -1, x2 = -1, x3 = -1;
     for (int i = 0; i < D; i++)
         if (i != const_i) { if (x1 < 0) x1 = i; else if (x2 < 0) x2 = i; else x3 = i; }
-    const int first = w.L.n;
+    const int first = w.nl;
     int amb = 0;
     for (int i = 0; i < D; i++) {
         if (i == const_i) continue;
@@ -269,13 +279,13 @@ static __device__ int cube_polygons(Work &w, const double cube[2][2][2], int con
             for (int a = 0; a < 2; a++)
                 for (int b = 0; b < 2; b++)
                     sq[a][b] = (i == x1) ? cube[j][a][b] : (i == x2) ? cube[a][j][b] : cube[a][b][j];
-            int before = w.L.n;
+            int before = w.nl;
             square_lines(w, sq, const_i, i, const_v, j * dx[i], E0, dx);
-            if (w.L.n - before == 2) amb++;   /* two lines <=> four cuts: Square::ambiguous */
+            if (w.nl - before == 2) amb++;   /* two lines <=> four cuts: Square::ambiguous */
             if (w.error) return 0;
         }
     }
-    const int nlines = w.L.n - first;
+    const int nlines = w.nl - first;
     *ambiguous = false;
     if (nlines == 0) return 0;
     if (amb == 0 && nlines == 6) amb++;
@@ -285,20 +295,20 @@ static __device__ int cube_polygons(Work &w, const double cube[2][2][2], int con
         int used = 0;
         for (int i = 0; i < nlines; i++) not_used[i] = true;
         do {
-            if (nlines - used < 3 || w.npoly >= kMaxPoly) { w.error = true; return nlines; }
-            Poly &p = w.poly[w.npoly];
+            if (nlines - used < 3 || w.np >= w.pcap) { w.error = true; return nlines; }
+            Poly &p = w.poly[w.np];
             poly_init(p, const_i);
             for (int i = 0; i < nlines; i++)
                 if (not_used[i] && poly_add_line(w, p, first + i, false)) { not_used[i] = false; used++; i = 0; }
             if (w.error) return nlines;
-            w.npoly++;
+            w.np++;
         } while (used < nlines);
     } else {
-        if (w.npoly >= kMaxPoly) { w.error = true; return nlines; }
-        Poly &p = w.poly[w.npoly];
+        if (w.np >= w.pcap) { w.error = true; return nlines; }
+        Poly &p = w.poly[w.np];
         poly_init(p, const_i);
         for (int i = 0; i < nlines; i++) poly_add_line(w, p, first + i, true);
-        w.npoly++;
+        w.np++;
     }
     return nlines;
 }
@@ -306,7 +316,7 @@ static __device__ int cube_polygons(Work &w, const double cube[2][2][2], int con
 /* Cornelius::find_surface_3d for a cube whose corner (i,j,k) spans
  * (tau, x, y); dx3 = {dtau, dx, dy} (cornelius.cpp:2161-2237, init :2087).
  * Element geometry is 4-vectors with component 0 unused. */
-static __device__ int surface_3d(Work &w, const double cube[2][2][2], double E0, const double *dx3,
+static __device__ int surface_3d(Work &wk, const double cube[2][2][2], double E0, const double *dx3,
                           double cen[][D], double nor[][D])
 {
     int above = 0;
@@ -314,21 +324,21 @@ static __device__ int surface_3d(Work &w, const double cube[2][2][2], double E0,
         if (cube[i][j][k] >= E0) above++;
     if (above == 0 || above == 8) return 0;
     const double dx[D] = {1, dx3[0], dx3[1], dx3[2]};
-    w.L.n = 0; w.npoly = 0; w.error = false;
+    WorkRef w = work_ref(wk);
     bool amb;
     cube_polygons(w, cube, 0, 0, E0, dx, &amb);
     if (w.error) return -1;
-    if (w.npoly > kMaxElements) { w.error = true; return -1; }
-    for (int i = 0; i < w.npoly; i++) {
+    if (w.np > kMaxElements) { w.error = true; return -1; }
+    for (int i = 0; i < w.np; i++) {
         poly_normal(w, w.poly[i], nor[i]);
         const double *c = poly_centroid(w, w.poly[i]);
         for (int j = 0; j < D; j++) cen[i][j] = c[j];
     }
-    return w.npoly;
+    return w.np;
 }
 
 /* Polyhedron::lines_equal, cornelius.cpp:786-802 */
-__device__ __forceinline__ bool lines_equal(const Work &w, int l1, int l2)
+__device__ __forceinline__ bool lines_equal(const WorkRef &w, int l1, int l2)
 {
     const double *p11 = lstart(w, l1), *p12 = lend(w, l1), *p21 = lstart(w, l2);
     double diff1 = 0, diff2 = 0;
@@ -361,7 +371,7 @@ struct Hedron {
 };
 
 /* Polyhedron::add_polygon, cornelius.cpp:743-774 */
-__device__ __forceinline__ bool hedron_add(Work &w, Hedron &h, int pi, bool donocheck)
+__device__ __forceinline__ bool hedron_add(WorkRef &w, Hedron &h, int pi, bool donocheck)
 {
     const Poly &p = w.poly[pi];
     if (donocheck || h.npoly == 0) {
@@ -385,7 +395,7 @@ __device__ __forceinline__ bool hedron_add(Work &w, Hedron &h, int pi, bool dono
 }
 
 /* Polyhedron::calculate_centroid and calculate_normal, cornelius.cpp:842-987 */
-static __device__ void hedron_geometry(Work &w, const Hedron &h, double *centroid, double *normal)
+static __device__ void hedron_geometry(const WorkRef &w, const Hedron &h, double *centroid, double *normal)
 {
     double mean[D] = {0, 0, 0, 0};
     for (int i = 0; i < h.npoly; i++) {
@@ -425,7 +435,7 @@ static __device__ void hedron_geometry(Work &w, const Hedron &h, double *centroi
             double a[D], b[D], c[D], n[D], vout[D];
             for (int k = 0; k < D; k++) { a[k] = p1[k] - centroid[k]; b[k] = p2[k] - centroid[k]; c[k] = cent[k] - centroid[k]; }
             tetravolume(a, b, c, n);
-            for (int k = 0; k < D; k++) vout[k] = w.L.out[p.line[j]][k] - centroid[k];
+            for (int k = 0; k < D; k++) vout[k] = w.out[p.line[j]][k] - centroid[k];
             orient(n, vout);
             for (int k = 0; k < D; k++) normal[k] += n[k];
         }
@@ -434,14 +444,14 @@ static __device__ void hedron_geometry(Work &w, const Hedron &h, double *centroi
 
 /* Cornelius::find_surface_4d with the Hypercube construction
  * (cornelius.cpp:1778-1970, :2248-2287). */
-static __device__ int surface_4d(Work &w, const double h[2][2][2][2], double E0, const double *dx,
+static __device__ int surface_4d(Work &wk, const double h[2][2][2][2], double E0, const double *dx,
                           double cen[][D], double nor[][D])
 {
     int above = 0;
     for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) for (int k = 0; k < 2; k++) for (int l = 0; l < 2; l++)
         if (h[i][j][k][l] >= E0) above++;
     if (above == 0 || above == 16) return 0;
-    w.L.n = 0; w.npoly = 0; w.error = false;
+    WorkRef w = work_ref(wk);
     int nlines_total = 0, ambiguous = 0;
     for (int i = 0; i < D; i++)
         for (int j = 0; j < 2; j++) {
@@ -462,7 +472,7 @@ static __device__ int surface_4d(Work &w, const double h[2][2][2][2], double E0,
     }
     Hedron hed[kMaxHedra];
     int nh = 0;
-    const int npolys = w.npoly;
+    const int npolys = w.np;
     if (ambiguous > 0) {
         bool not_used[kMaxPoly];
         int used = 0;
