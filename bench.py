@@ -60,10 +60,19 @@ def phase_words(nq):
 
 
 # DRAM bytes per launch (dram__bytes_read.sum + dram__bytes_write.sum) from the
-# ncu captures kept in profiles/kt_stage_kernels_glauber_131x131x61.md and
-# profiles/kt_flux_face_kernel_glauber_131x131x61_mixed.md
-NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 387.84e6, ("glauber_3p1d", "fp64", "source"): 336.17e6,
+# ncu captures kept in profiles/kt_flux_lines_kernel_glauber_131x131x61.md
+# (FP64: mean of the x, y, eta launches) and
+# profiles/kt_flux_face_kernel_glauber_131x131x61_mixed.md (mixed)
+NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 381.0e6, ("glauber_3p1d", "fp64", "source"): 333.8e6,
                ("glauber_3p1d", "mixed", "flux"): 388.30e6, ("glauber_3p1d", "mixed", "source"): 322.01e6}
+
+
+# FP64 pipe use of the dominant kernel from the same captures: mean over the
+# x, y, eta launches of sm__pipe_fp64_cycles_active (% of peak sustained),
+# the launch's duration under ncu (ms) and its FP64-pipe warp instructions.
+# The fraction of the FP64 pipe's peak at live speed is that percentage
+# scaled by the ratio of the durations.
+NCU_FP64 = {("glauber_3p1d", "fp64", "flux"): (29.18, 0.586, 94.8e6)}
 
 
 # batched flux launches: DRAM bytes per cell from ncu captures of the same
@@ -74,14 +83,16 @@ NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 387.84e6, ("glauber_3p1d", "fp6
 NCU_TRAFFIC_PER_CELL = {("fp64", "flux"): 371.7, ("mixed", "flux"): 371.6}
 
 
-# steps of the mixed-precision error report: the Gubser event to its end
+# steps of the mixed-precision error report: the Gubser event's 300 steps
 # (tau = 4 fm/c); the Glauber event to tau = 12.6 fm/c (800 steps) -- at step
 # 909 its FP64 evolution, bit-identical to the reference's, trips the
-# reference's NaN guard (EnergyMomentumTensor.cpp:197-203) in the dilute edge
+# reference's NaN guard (EnergyMomentumTensor.cpp:197-203) in the dilute
+# edge.  No cell is above e_F after about step 150 (Gubser) and 400
+# (Glauber): the reference's stop rule would end the events there.
 PRECISION_STEPS = {"gubser_2p1d": 300, "glauber_3p1d": 800}
 
 
-KERNEL_NAMES = {"source": "kt_source_kernel", "flux": "kt_flux_staged_kernel (x, y, eta)",
+KERNEL_NAMES = {"source": "kt_source_kernel", "flux": "kt_flux_lines_kernel (x, y, eta)",
                 "final": "kt_final_kernel", "fused": "kt_stage_kernel"}
 
 
@@ -104,6 +115,10 @@ def parse():
                     help="--precision mixed: steps of the error report (0: the workload's whole event)")
     ap.add_argument("--fo-blocks", type=int, default=4,
                     help="freezeout blocks timed after the steps (0: none), one per fo_factor steps")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="glauber_3p1d FP64 line without its batch / precision / serve records")
+    ap.add_argument("--serve-events", type=int, default=24,
+                    help="events of the serve record of the default line (each run to the stop rule)")
     return ap.parse_args()
 
 
@@ -184,26 +199,63 @@ def precision_report(cfg, rows, st, steps, ev_mixed=None):
         e.sync()
         return e
 
+    e_F = vh.eos_eval(cfg, rows, 3, cfg.T_freezeout_GeV / 0.197326938)
+
     def errs(a_ev, b_ev):
+        """relative L-inf / L2 over the interior, and over the cells above e_F
+        (the fluid that has not frozen out yet) of the FP64 run b_ev"""
         out = {}
+        hot = vh.interior(cfg, b_ev.field(vh.VH_F_E)).ravel() > e_F
         for name, fid in fields:
             a = vh.interior(cfg, a_ev.field(fid)).ravel()
             b = vh.interior(cfg, b_ev.field(fid)).ravel()
             d = a - b
             out[name] = {"linf": float(np.max(np.abs(d)) / max(np.max(np.abs(b)), 1e-300)),
                          "l2": float(np.linalg.norm(d) / max(np.linalg.norm(b), 1e-300))}
+            if hot.any():
+                out[name]["linf_above_eF"] = float(np.max(np.abs(d[hot])) / max(np.max(np.abs(b[hot])), 1e-300))
+                out[name]["l2_above_eF"] = float(np.linalg.norm(d[hot]) / max(np.linalg.norm(b[hot]), 1e-300))
+        out["cells_above_eF"] = int(hot.sum())
         return out
 
-    ref = run(st)
     bumped = vh.InitialState(st.e * (1 + 2.0 ** -50), st.p, st.u, st.pi, st.Pi)
-    floor = run(bumped)
     own = ev_mixed is None
     if own:
-        ev_mixed = run(st, vh.VH_PREC_MIXED)
-    rep = {"steps": steps, "tau_fm": cfg.t0 + steps * cfg.dt, "mixed_vs_fp64": errs(ev_mixed, ref),
-           "fp64_sensitivity": errs(floor, ref)}
-    for e in (ref, floor) + ((ev_mixed,) if own else ()):
-        e.close()
+        # the three runs side by side, compared at eight points of the event:
+        # while fluid is above e_F, the error there is the one that reaches
+        # the freezeout surface
+        def make(ic, prec=vh.VH_PREC_FP64):
+            e = vh.Event(cfg.copy(precision=prec), rows)
+            e.set_initial(ic)
+            return e
+        ref, floor, ev_mixed = make(st), make(bumped), make(st, vh.VH_PREC_MIXED)
+        marks, done = [], 0
+        for k in range(1, 9):
+            n = steps * k // 8 - done
+            for e in (ref, floor, ev_mixed):
+                e.step(n)
+                e.sync()
+            done += n
+            marks.append({"step": done, "mixed_vs_fp64": errs(ev_mixed, ref), "fp64_sensitivity": errs(floor, ref)})
+        rep = {"steps": steps, "tau_fm": cfg.t0 + steps * cfg.dt, "mixed_vs_fp64": marks[-1]["mixed_vs_fp64"],
+               "fp64_sensitivity": marks[-1]["fp64_sensitivity"]}
+        for key in ("mixed_vs_fp64", "fp64_sensitivity"):
+            hot = [m[key]["e"].get("linf_above_eF") for m in marks if "linf_above_eF" in m[key]["e"]]
+            rep[key]["e_linf_above_eF_max_over_event"] = max(hot) if hot else None
+        rep["checkpoints"] = [{"step": m["step"], "cells_above_eF": m["mixed_vs_fp64"]["cells_above_eF"],
+                               "e_linf_mixed": m["mixed_vs_fp64"]["e"]["linf"],
+                               "e_linf_above_eF_mixed": m["mixed_vs_fp64"]["e"].get("linf_above_eF"),
+                               "e_linf_fp64_sensitivity": m["fp64_sensitivity"]["e"]["linf"],
+                               "e_linf_above_eF_fp64_sensitivity": m["fp64_sensitivity"]["e"].get("linf_above_eF")}
+                              for m in marks]
+        for e in (ref, floor, ev_mixed):
+            e.close()
+    else:
+        ref, floor = run(st), run(bumped)
+        rep = {"steps": steps, "tau_fm": cfg.t0 + steps * cfg.dt, "mixed_vs_fp64": errs(ev_mixed, ref),
+               "fp64_sensitivity": errs(floor, ref)}
+        for e in (ref, floor):
+            e.close()
 
     # freezeout over the same steps, a block every fo_factor steps as run()
     # does: element count and the sums of d sigma_mu over all elements
@@ -273,11 +325,22 @@ def pct(xs, q):
 
 
 def run_serve(args, rank):
+    line = serve_record(args.events, args.rate, args.max_steps, args.precision)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def serve_record(n_events, rate, max_steps, precision):
     """The event server under a Poisson stream, next to the same stream served
     one event at a time by the plain FP64 path (FCFS queue over the measured
-    per-event service times)."""
+    per-event service times).  max_steps 0: every event runs to the
+    reference's stop rule (three freezeout blocks with no cell above e_F,
+    HydroPlugin.cpp:267-281) or to a device error."""
     import numpy as np
     import vh
+    from types import SimpleNamespace
+    args = SimpleNamespace(events=n_events, rate=rate, max_steps=max_steps, precision=precision)
     stream, rows, desc = serve_stream(args.events, args.rate)
     mixed = args.precision == "mixed"
     prec = vh.VH_PREC_MIXED if mixed else vh.VH_PREC_FP64
@@ -340,9 +403,9 @@ def run_serve(args, rank):
                                   "events_with_device_error": serial_bad,
                                   "how": "each event alone through vh_event_step/freezeout (FP64), same cadence "
                                          "and step cap; FCFS queue over the measured service times"}}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    return 0
+    line["server_vs_serial_events_per_s"] = line["value"] / line["serial_plain_fp64"]["events_per_s"]
+    line["steps_per_event"] = {"mean": float(np.mean([d.steps for d in done])), "max": int(max(d.steps for d in done))}
+    return line
 
 
 def measured_peaks():
@@ -583,6 +646,136 @@ def run_reference(args):
     return 0
 
 
+def batch_record(torch, n_events=256, steps=10, warmup=3, error_steps=EVENT_STEPS):
+    """The batched workload in FP64 and in mixed precision against the plain
+    single-event FP64 path, and the error of every member over its whole
+    event (error_steps RK2 steps) against the FP64 path, next to the FP64
+    path's own sensitivity (initial e scaled by 1 + 2^-50)."""
+    import numpy as np
+    import vh
+    cfgs, rows, ics, desc = batch_workload(n_events)
+    Ntot = sum(c.nx * c.ny * c.nz for c in cfgs)
+    rec = {"workload": desc, "events": n_events, "cells": Ntot, "steps": steps, "warmup": warmup,
+           "event_steps": EVENT_STEPS}
+
+    def make(prec, states):
+        out = []
+        for c, st in zip(cfgs, states):
+            e = vh.Event(c.copy(precision=prec), rows)
+            e.set_initial(st)
+            out.append(e)
+        return out
+
+    def close(evs, b):
+        b.close()
+        for e in evs:
+            e.close()
+
+    def timed(prec):
+        evs = make(prec, ics)
+        b = vh.Batch(evs)
+        tune = b.autotune()
+        stream = torch.cuda.ExternalStream(b.stream())
+        b.step(warmup)
+        for e in evs:
+            e.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        b.step(steps)
+        e1.record(stream)
+        e1.synchronize()
+        for e in evs:
+            vh.check(e.status()[0], "batched steps")
+        ms = e0.elapsed_time(e1) / steps
+        launches = b.launches_per_step()
+        close(evs, b)
+        return {"ms_per_step": ms, "cell_updates_per_s": Ntot / (ms / 1e3),
+                "events_per_s": n_events / (ms / 1e3 * EVENT_STEPS), "gpu_launches_per_step": launches,
+                "tuning": tune.describe()}
+
+    t_mark = [time.perf_counter()]
+
+    def mark(what):
+        now = time.perf_counter()
+        print(f"[bench] batch record: {what} {now - t_mark[0]:.1f} s", file=sys.stderr, flush=True)
+        t_mark[0] = now
+
+    mark("workload")
+    rec["fp64"] = timed(vh.VH_PREC_FP64)
+    mark("fp64 batch")
+    rec["mixed"] = timed(vh.VH_PREC_MIXED)
+    mark("mixed batch")
+    # the plain single-event FP64 path, one event at a time
+    t_solo, s0, s1 = 0.0, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for c, st in zip(cfgs, ics):
+        e = vh.Event(c, rows)
+        e.set_initial(st)
+        es = torch.cuda.ExternalStream(e.stream())
+        e.step(1)
+        s0.record(es)
+        e.step(steps)
+        s1.record(es)
+        s1.synchronize()
+        t_solo += s0.elapsed_time(s1)
+        e.close()
+    solo_ms = t_solo / steps
+    rec["plain_single_event_fp64"] = {"ms_per_step_all_events": solo_ms, "cell_updates_per_s": Ntot / (solo_ms / 1e3),
+                                      "events_per_s": n_events / (solo_ms / 1e3 * EVENT_STEPS),
+                                      "how": f"vh_event_step, one event at a time, {steps} steps each after 1, "
+                                             "CUDA events per event"}
+    mark("plain path")
+    rec["fp64_batch_vs_plain"] = solo_ms / rec["fp64"]["ms_per_step"]
+    rec["mixed_batch_vs_plain"] = solo_ms / rec["mixed"]["ms_per_step"]
+
+    # every member over its whole event: mixed vs FP64 and FP64 vs itself perturbed
+    def run_all(prec, states):
+        """error_steps steps; a member whose device flags an error (the
+        reference's NaN guard) is no longer computed by the batch"""
+        evs = make(prec, states)
+        b = vh.Batch(evs)
+        b.step(error_steps)
+        for e in evs:
+            e.status()
+        return evs, b
+
+    e_F = vh.eos_eval(cfgs[0], rows, 3, cfgs[0].T_freezeout_GeV / 0.197326938)
+    ref_evs, rb = run_all(vh.VH_PREC_FP64, ics)
+    mix_evs, mb = run_all(vh.VH_PREC_MIXED, ics)
+    bumped = [vh.InitialState(st.e * (1 + 2.0 ** -50), st.p, st.u, st.pi, st.Pi) for st in ics]
+    bmp_evs, bb = run_all(vh.VH_PREC_FP64, bumped)
+    per = {"mixed_vs_fp64": {"linf": [], "linf_above_eF": []}, "fp64_sensitivity": {"linf": [], "linf_above_eF": []}}
+    errored = {"fp64": 0, "mixed": 0, "fp64_perturbed": 0}
+    for c, r, m, q in zip(cfgs, ref_evs, mix_evs, bmp_evs):
+        st = {"fp64": r.status()[0], "mixed": m.status()[0], "fp64_perturbed": q.status()[0]}
+        for k, v in st.items():
+            errored[k] += v != 0
+        if any(st.values()):
+            continue            # a device error (the reference's NaN guard) before the last step
+        b = vh.interior(c, r.field(vh.VH_F_E)).ravel()
+        hot = b > e_F
+        for key, ev in (("mixed_vs_fp64", m), ("fp64_sensitivity", q)):
+            d = vh.interior(c, ev.field(vh.VH_F_E)).ravel() - b
+            per[key]["linf"].append(float(np.max(np.abs(d)) / np.max(np.abs(b))))
+            per[key]["linf_above_eF"].append(float(np.max(np.abs(d[hot])) / np.max(np.abs(b[hot]))) if hot.any()
+                                             else 0.0)
+    close(ref_evs, rb)
+    close(mix_evs, mb)
+    close(bmp_evs, bb)
+    mark("whole-event errors")
+    compared = len(per["mixed_vs_fp64"]["linf"])
+    err = {"steps": error_steps, "field": "e", "members_compared": compared,
+           "members_with_device_error": errored,
+           "note": "members whose run in any of the three modes flagged a device error (the reference's NaN "
+                   "guard, EnergyMomentumTensor.cpp:197-203, reached in the dilute edge of lumpy events) "
+                   "within the steps are not compared"}
+    for key, v in per.items():
+        err[key] = {k: {"max": float(np.max(x)), "median": float(np.median(x)),
+                        "members_within_1e-4": int(np.sum(np.asarray(x) <= 1e-4))} for k, x in v.items()}
+    rec["precision_error"] = err
+    return rec
+
+
 def run_batch(args, torch, world, rank, barrier, max_over_ranks):
     """All events of the batched workload advanced by one vh_batch: one launch
     per RK phase for every event, CUDA-graph replay, autotuned launch shapes."""
@@ -646,7 +839,8 @@ def run_batch(args, torch, world, rank, barrier, max_over_ranks):
                 for c, st, e in list(zip(cfgs, ics, evs))[:4]]
         prec = {"members": "the first 4 events of the batch, worst case over them", "steps": reps[0]["steps"]}
         for key in ("mixed_vs_fp64", "fp64_sensitivity"):
-            prec[key] = {f: {m: max(r[key][f][m] for r in reps) for m in ("linf", "l2")} for f in reps[0][key]}
+            prec[key] = {f: {m: max(r[key][f][m] for r in reps) for m in ("linf", "l2")} for f in reps[0][key]
+                         if isinstance(reps[0][key][f], dict)}
 
     # the plain single-event FP64 path on the same events, one event at a time
     solo_steps = max(1, min(args.steps, 10))
@@ -906,6 +1100,15 @@ def main():
                                      "FP64/FP32 issue latency (memory and barrier stalls), not HBM"},
                 "phases_ms_per_step": {k: t / args.steps for k, (t, _) in phases.items()},
                 "clocks": clk, "gpu_launches": ev.launches_per_step() * args.steps}
+        fp = NCU_FP64.get((args.workload, args.precision, dom))
+        if fp:
+            pct, t_ncu_ms, inst = fp
+            line["roofline_fp64_pipe"] = {
+                "kernel": line["roofline"]["kernel"], "frac": pct / 100.0 * t_ncu_ms / (launch_s * 1e3),
+                "fp64_warp_instructions_per_launch": inst,
+                "achieved_warp_instructions_per_s": inst / launch_s,
+                "how": f"ncu sm__pipe_fp64_cycles_active {pct:.1f} % of peak over the captured launch "
+                       f"({t_ncu_ms:.3f} ms under ncu), scaled to the live launch duration"}
         if prec:
             line["precision_error"] = prec
         if fo:
@@ -914,8 +1117,34 @@ def main():
             line["e2e"] = e2e
         if base:
             line["cpu_baseline"] = {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")}
-        print(json.dumps(line), flush=True)
     ev.close()
+    if rank == 0 and world == 1 and args.workload == "glauber_3p1d" and not mixed and not args.no_extras:
+        # the other targets of the benchmark's configurations, each a record
+        # of its own: batched events (FP64, mixed) against the plain path; the
+        # mixed-precision error of whole events; the event server on a sample
+        # of the served mix with every event run to the stop rule
+        secs = {}
+        t0 = time.perf_counter()
+        line["batch"] = batch_record(torch)
+        secs["batch"] = time.perf_counter() - t0
+        print(f"[bench] batch record {secs['batch']:.1f} s", file=sys.stderr, flush=True)
+        t0 = time.perf_counter()
+        gc = vh.gubser_config()
+        line["precision"] = {
+            "gubser_2p1d": precision_report(gc, None, vh.gubser_ic(gc), PRECISION_STEPS["gubser_2p1d"]),
+            "glauber_3p1d": precision_report(cfg, rows, st, PRECISION_STEPS["glauber_3p1d"])}
+        secs["precision"] = time.perf_counter() - t0
+        print(f"[bench] precision record {secs['precision']:.1f} s", file=sys.stderr, flush=True)
+        if args.serve_events > 0:
+            t0 = time.perf_counter()
+            line["serve"] = serve_record(args.serve_events, 30.0, 0, "mixed")
+            line["serve"]["note"] = (f"a sample of {args.serve_events} events of the served mix (the "
+                                     "configuration names 10,000), arrivals at 30/s (saturating), every event "
+                                     "to the stop rule")
+            secs["serve"] = time.perf_counter() - t0
+        line["extras_seconds"] = secs
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     R.close()
     return 0
 
