@@ -375,7 +375,7 @@ __device__ __forceinline__ void flux_slopes_tile(const StageArgs &A, int i0, int
  * The flux along DIR over lines: the lattice is cut into lines along DIR,
  * and the lines into bundles of W adjacent x-columns (W = 1 for DIR 1,
  * where a line is a row of contiguous x; W = 4 for DIR 2 and 3, so that a
- * warp's loads cover whole 32-byte sectors).  Run positions R = pos + nd *
+ * warp's loads cover whole 32-byte sectors; 8 columns measured slower).  Run positions R = pos + nd *
  * bundle enumerate (position along DIR, bundle); a block takes PB = 128 / W
  * consecutive run positions times W columns, which may span the end of one
  * line and the start of the next.  Every thread therefore has a cell (131
@@ -399,7 +399,7 @@ struct FluxLines {
     }
 };
 
-template <int NQ, int EOS, int DIR>
+template <int NQ, int EOS, int DIR, int UNR = 1>
 __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__restrict__ sm)
 {
     using G = FluxLines<DIR>;
@@ -507,7 +507,7 @@ __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__r
     const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
     double S[4];
     dir_sources_t<NQ>(A, qt, ts, tst, s, d, DIR, S);
-#pragma unroll 1
+#pragma unroll UNR
     for (int n = 0; n < NQ; ++n) {
         const double *q = sm + n * PS + ts, *h = hs + n * PS + ts;
         const double Rf = q[tst] - h[tst], Lf = q[0] + h[0], Rb = q[0] - h[0], Lb = q[-tst] + h[-tst];

@@ -146,14 +146,14 @@ static void launch_flux_slopes(const StageArgs &a, dim3 grid, dim3 block, cudaSt
 
 /* the flux over line pieces (flux_lines_block): a 1-D grid of 128-thread
  * blocks, dynamic shared memory 2 * NQ * FluxLines::plane(nd) doubles */
-template <int NQ, int EOS, int DIR, int MB>
+template <int NQ, int EOS, int DIR, int MB, int UNR>
 __global__ void __launch_bounds__(128, MB) kt_flux_lines_kernel(const __grid_constant__ StageArgs A)
 {
     extern __shared__ double smd[];
-    flux_lines_block<NQ, EOS, DIR>(A, smd);
+    flux_lines_block<NQ, EOS, DIR, UNR>(A, smd);
 }
 
-template <int NQ, int EOS, int DIR, int MB>
+template <int NQ, int EOS, int DIR, int MB, int UNR = 1>
 static void launch_flux_lines(const StageArgs &a, cudaStream_t s)
 {
     using G = FluxLines<DIR>;
@@ -161,23 +161,25 @@ static void launch_flux_lines(const StageArgs &a, cudaStream_t s)
     const size_t bytes = sizeof(double) * 2 * NQ * (size_t)G::plane(nd);
     static size_t attr_bytes = 0;
     if (bytes > attr_bytes) {
-        cudaFuncSetAttribute(kt_flux_lines_kernel<NQ, EOS, DIR, MB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(kt_flux_lines_kernel<NQ, EOS, DIR, MB, UNR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)bytes);
-        cudaFuncSetAttribute(kt_flux_lines_kernel<NQ, EOS, DIR, MB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        cudaFuncSetAttribute(kt_flux_lines_kernel<NQ, EOS, DIR, MB, UNR>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              100);
         attr_bytes = bytes;
     }
     const long long runs = (long long)nd * G::bundles(a.nx, a.ny, a.nz);
     const unsigned blocks = (unsigned)((runs + G::PB - 1) / G::PB);
-    kt_flux_lines_kernel<NQ, EOS, DIR, MB><<<blocks, 128, bytes, s>>>(a);
+    kt_flux_lines_kernel<NQ, EOS, DIR, MB, UNR><<<blocks, 128, bytes, s>>>(a);
 }
 
 /* FP64 flux form of the phase-split stage: VH_FLUX_FORM=lines (default:
- * line pieces, 5 blocks per SM at 96 registers), lines4 (4 blocks per SM,
- * up to 128 registers), slopes (32 x 4 tiles with shared half slopes) or
- * staged (32 x 4 tiles, every cell computing its own slopes).  Measured on
- * the 131x131x61 Glauber event (ms per x/y/eta launch): lines 0.75/0.86/0.87,
- * lines4 0.89/0.98/0.99, slopes 0.98/1.00/1.03, staged 1.10/1.09/1.12. */
+ * line pieces, 5 blocks per SM at 96 registers, the component loop unrolled
+ * by 3), lines4 (4 blocks per SM, up to 128 registers, loop rolled), slopes
+ * (32 x 4 tiles with shared half slopes) or staged (32 x 4 tiles, every cell
+ * computing its own slopes).  Measured on the 131x131x61 Glauber event (ms
+ * per step of the x/y/eta launches, two each): lines 0.74/0.85/0.86 (0.75/
+ * 0.86/0.87 with the loop rolled), lines4 0.89/0.98/0.99, slopes
+ * 0.98/1.00/1.03, staged 1.10/1.09/1.12. */
 static inline int flux_form()
 {
     static int f = [] {
@@ -300,11 +302,11 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
             mark(2);
             if (z) { launch_flux_lines<NQ, EOS, 3, 4>(a, s); mark(3); }
         } else if (flux_form() == 3) {
-            launch_flux_lines<NQ, EOS, 1, 5>(a, s);
+            launch_flux_lines<NQ, EOS, 1, 5, 3>(a, s);
             mark(1);
-            launch_flux_lines<NQ, EOS, 2, 5>(a, s);
+            launch_flux_lines<NQ, EOS, 2, 5, 3>(a, s);
             mark(2);
-            if (z) { launch_flux_lines<NQ, EOS, 3, 5>(a, s); mark(3); }
+            if (z) { launch_flux_lines<NQ, EOS, 3, 5, 3>(a, s); mark(3); }
         } else {
             launch_flux_slopes<NQ, EOS, 1>(a, grid, block, s);
             mark(1);
