@@ -115,6 +115,7 @@ static inline vh::DevEos dev_eos(const vh_event *ev)
     E.pq.hb0 = ev->powf.hb0;
     E.pq.hb1 = ev->powf.hb1;
     E.pq.miss = ev->powf_miss;
+    E.stop = ev->err;
     return E;
 }
 

@@ -27,6 +27,7 @@ struct DevEos {
     double inv_spacing;       /* RN(1/e_spacing), for div_rcp */
     double cs2_third_hi;      /* eos_cs2 is exactly 1/3 for e <= this (HostEos::cs2_third_bound) */
     PowfTab pq;               /* host-exact powf(x, 0.25) */
+    const int *stop;          /* the event's device error code (or null): see e_bisect_table */
 };
 
 struct DevErr {
@@ -124,11 +125,17 @@ __device__ __forceinline__ double approx_deriv(double th, double x, double y, do
 /* -------------------------------------------------------- inversion */
 /* EnergyMomentumTensor.cpp:48-111: the bisection the tabulated-EoS root solve
  * falls back to when Newton has not converged in 10^4 iterations.  Out of
- * line: no workload here reaches it, and every caller shares one copy. */
+ * line: no valid state here reaches it, and every caller shares one copy.
+ * Once the event's device has flagged an error, the bisection gives up after
+ * 64 iterations: the state is then invalid (the reference exits at its first
+ * NaN), and the cells of a garbage state would each spend its 10^6
+ * iterations before the host reads the error.  The flag is read through L2
+ * (another block may have just set it). */
 static __device__ __noinline__ double e_bisect_table(const DevEos &E, double ePrev, double M0, double M, double Pi)
 {
     double e_lo = 0.0, e_mid = ePrev, e_hi = 2.0 * (ePrev + 1.0);
     for (int j = 0; j < 1000000; ++j) {                            /* MAX_ITERS_BI */
+        if ((j & 63) == 63 && E.stop && *(const volatile int *)E.stop != 0) return ePrev;
         double p_lo = eos_p<1>(E, e_lo), p_mid = eos_p<1>(E, e_mid), p_hi = eos_p<1>(E, e_hi);
         double c_lo = p_lo / e_lo, c_mid = p_mid / e_mid, c_hi = p_hi / e_hi;
         double A_lo = M0 * (1.0 - c_lo) + Pi, A_mid = M0 * (1.0 - c_mid) + Pi, A_hi = M0 * (1.0 - c_hi) + Pi;

@@ -1057,6 +1057,85 @@ __device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int 
     if constexpr (DIR != 1) __syncthreads();
 }
 
+/* The face-once flux over line pieces (mixed precision, single events):
+ * the faces of each line along DIR (nd + 1 of them, face f between cells
+ * f - 1 and f) enumerated like FluxLines' cells, R = f + (nd + 1) * bundle,
+ * one face per thread, the W columns of a bundle side by side.  A block
+ * takes PB consecutive faces and updates the cells of all but its last face
+ * (the next block starts there: blocks overlap by one face), so no lane
+ * idles at line ends and only one face in PB is computed twice.  The face
+ * arithmetic, the next face through shared memory and the recomputation
+ * across the root solve's e <= 0.1 branch are those of flux_faces_tile, so
+ * a cell's update is the same.  sm: NQ * 128 doubles. */
+template <int NQ, int EOS, int DIR>
+__device__ __forceinline__ void flux_faces_lines(const StageArgs &A, double *__restrict__ sm)
+{
+    using G = FluxLines<DIR>;
+    constexpr int W = G::W, PB = G::PB;
+    const int nd = (DIR == 1) ? A.nx : (DIR == 2) ? A.ny : A.nz;
+    const int nf = nd + 1;
+    const long long sxy = (long long)A.ncx * A.ncy;
+    const long long st = (DIR == 1) ? 1 : (DIR == 2) ? (long long)A.ncx : sxy;
+    const int nxq = (A.nx + W - 1) / W;
+    const long long Rtot = (long long)nf * G::bundles(A.nx, A.ny, A.nz);
+    const int tid = threadIdx.x, w = tid % W, pr = tid / W;
+    const long long R = (long long)blockIdx.x * (PB - 1) + pr;
+    bool face_ok = R < Rtot;
+    int f = 0;
+    long long s = 0;
+    if (face_ok) {
+        const long long b = R / nf;
+        f = (int)(R - b * nf);
+        long long base;
+        if (DIR == 1) {
+            const long long j = b % A.ny, k = b / A.ny;
+            base = A.ncx * (j + 2) + sxy * (k + 2);
+        } else {
+            const long long xq = b % nxq, o = b / nxq;
+            const int x = (int)xq * W + w;
+            face_ok = x < A.nx;
+            base = (DIR == 2) ? (x + 2) + sxy * (o + 2) : (x + 2) + A.ncx * (o + 2);
+        }
+        s = base + (long long)(f + 2) * st;       /* the face's upper cell (a ghost for f = nd) */
+    }
+    bool bad = false;
+    double H[NQ];
+    if (face_ok) {
+        face_H_m<NQ, EOS>(A, s - st, st, DIR, __ldg(A.ein + s), H, bad);
+    } else {
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) H[n] = 0.0;
+    }
+#pragma unroll
+    for (int n = 0; n < NQ; ++n) sm[n * 128 + tid] = H[n];
+    __syncthreads();
+    if (face_ok && f < nd && pr < PB - 1) {
+        const int nxt = tid + W;                  /* face f + 1 of the same line */
+        const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
+        const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
+        double r[NQ];
+        const double e_self = __ldg(A.ein + s), e_next = __ldg(A.ein + s + st);
+        if ((e_self <= 0.1) != (e_next <= 0.1)) {
+            double F[NQ];
+            face_H_m<NQ, EOS>(A, s, st, DIR, e_self, F, bad);
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) r[n] = H[n] - F[n];
+        } else {
+#pragma unroll
+            for (int n = 0; n < NQ; ++n) r[n] = H[n] - sm[n * 128 + nxt];
+        }
+        double S[4];
+        dir_sources<NQ>(A, s, st, d, DIR, S);
+#pragma unroll
+        for (int n = 0; n < 4; ++n) r[n] = (r[n] * yd + S[n]) * A.dt;
+#pragma unroll
+        for (int n = 4; n < NQ; ++n) r[n] *= yd * A.dt;
+#pragma unroll
+        for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] += r[n];
+    }
+    if (bad) raise_error(A.err, kErrNan, s, A.step);
+}
+
 /* ---------------------------------------------------------------------
  * Face-parallel stage for small lattices.  A single event of ~10^4 cells is
  * latency-bound: one thread per cell carries the whole stage.  Here each cell

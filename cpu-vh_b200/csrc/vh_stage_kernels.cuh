@@ -137,7 +137,7 @@ static void launch_flux_slopes(const StageArgs &a, dim3 grid, dim3 block, cudaSt
         cudaFuncSetAttribute(kt_flux_slopes_kernel<NQ, EOS, DIR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)bytes);
         cudaFuncSetAttribute(kt_flux_slopes_kernel<NQ, EOS, DIR>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             100);
+                             (int)((VH_STAGE_MIN_BLOCKS * (bytes + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024)));
         return true;
     }();
     (void)attr;
@@ -163,8 +163,13 @@ static void launch_flux_lines(const StageArgs &a, cudaStream_t s)
     if (bytes > attr_bytes) {
         cudaFuncSetAttribute(kt_flux_lines_kernel<NQ, EOS, DIR, MB, UNR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)bytes);
+        /* shared memory for MB resident blocks (1 KB reserved per block) out
+         * of 228 KB, and the rest of the SM's 256 KB left to L1, which holds
+         * the EoS table of the root solves; VH_CARVEOUT overrides (percent) */
+        int pct = (int)((MB * (bytes + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
+        if (const char *e = getenv("VH_CARVEOUT")) pct = atoi(e);
         cudaFuncSetAttribute(kt_flux_lines_kernel<NQ, EOS, DIR, MB, UNR>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             100);
+                             pct);
         attr_bytes = bytes;
     }
     const long long runs = (long long)nd * G::bundles(a.nx, a.ny, a.nz);
@@ -177,9 +182,11 @@ static void launch_flux_lines(const StageArgs &a, cudaStream_t s)
  * by 3), lines4 (4 blocks per SM, up to 128 registers, loop rolled), slopes
  * (32 x 4 tiles with shared half slopes) or staged (32 x 4 tiles, every cell
  * computing its own slopes).  Measured on the 131x131x61 Glauber event (ms
- * per step of the x/y/eta launches, two each): lines 0.74/0.85/0.86 (0.75/
- * 0.86/0.87 with the loop rolled), lines4 0.89/0.98/0.99, slopes
- * 0.98/1.00/1.03, staged 1.10/1.09/1.12. */
+ * per step of the x/y/eta launches, two each): lines 0.74/0.77/0.78 (0.74/
+ * 0.85/0.87 with the shared-memory carveout at its maximum, which left L1
+ * 28 KB for the EoS table and the loads; 0.75/0.86/0.87 with the loop
+ * rolled), lines4 0.89/0.98/0.99, slopes 0.98/1.00/1.03, staged
+ * 1.10/1.09/1.12. */
 static inline int flux_form()
 {
     static int f = [] {
@@ -215,6 +222,40 @@ __global__ void __launch_bounds__(kFaceTX * kFaceTY, 2) kt_flux_face_kernel(cons
     else if (DIR == 2) { i0 = blockIdx.x * kFaceTX; j0 = blockIdx.y * (kFaceTY - 1); k0 = blockIdx.z; }
     else { i0 = blockIdx.x * kFaceTX; j0 = blockIdx.y; k0 = blockIdx.z * (kFaceTY - 1); }
     flux_faces_tile<NQ, EOS, DIR, kFaceTX, kFaceTY>(A, i0, j0, k0, sm);
+}
+
+/* the face-once flux over line pieces (flux_faces_lines), 128 threads */
+template <int NQ, int EOS, int DIR, int MB>
+__global__ void __launch_bounds__(128, MB) kt_flux_face_lines_kernel(const __grid_constant__ StageArgs A)
+{
+    __shared__ double sm[NQ * 128];
+    flux_faces_lines<NQ, EOS, DIR>(A, sm);
+}
+
+template <int NQ, int EOS, int DIR, int MB>
+static void launch_flux_face_lines(const StageArgs &a, cudaStream_t s)
+{
+    using G = FluxLines<DIR>;
+    const int nd = (DIR == 1) ? a.nx : (DIR == 2) ? a.ny : a.nz;
+    const long long faces = (long long)(nd + 1) * G::bundles(a.nx, a.ny, a.nz);
+    const unsigned blocks = (unsigned)((faces + G::PB - 2) / (G::PB - 1));
+    kt_flux_face_lines_kernel<NQ, EOS, DIR, MB><<<blocks, 128, 0, s>>>(a);
+}
+
+/* mixed-precision flux form of the phase-split stage: VH_FACE_FORM=lines
+ * (default: faces over line pieces along y and eta, 32 x 8 face tiles along
+ * x, where a warp passes each face to the next lane by shuffle) or tiles
+ * (32 x 8 face tiles along every axis).  131x131x61 Glauber event, ms per
+ * step x/y/eta: lines 0.646/0.658/0.715, tiles 0.646/0.723/0.747; along x
+ * line pieces measured 0.712 (a block barrier for the next face where the
+ * tile's warp uses a shuffle), at 3 blocks per SM y/eta 0.744/0.803 */
+static inline int face_form()
+{
+    static int f = [] {
+        const char *e = getenv("VH_FACE_FORM");
+        return (e && e[0] == 't') ? 0 : 4;
+    }();
+    return f;
 }
 
 template <int DIR>
@@ -287,12 +328,21 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
     kt_source_kernel<NQ, EOS, MIXED><<<gflat, 128, 0, s>>>(a);
     mark(0);
     if constexpr (MIXED) {
-        const dim3 fb(kFaceTX, kFaceTY, 1);
-        kt_flux_face_kernel<NQ, EOS, 1><<<face_grid<1>(a), fb, 0, s>>>(a);
-        mark(1);
-        kt_flux_face_kernel<NQ, EOS, 2><<<face_grid<2>(a), fb, 0, s>>>(a);
-        mark(2);
-        if (z) { kt_flux_face_kernel<NQ, EOS, 3><<<face_grid<3>(a), fb, 0, s>>>(a); mark(3); }
+        if (face_form() != 0) {
+            const dim3 fb(kFaceTX, kFaceTY, 1);
+            kt_flux_face_kernel<NQ, EOS, 1><<<face_grid<1>(a), fb, 0, s>>>(a);
+            mark(1);
+            launch_flux_face_lines<NQ, EOS, 2, 4>(a, s);
+            mark(2);
+            if (z) { launch_flux_face_lines<NQ, EOS, 3, 4>(a, s); mark(3); }
+        } else {
+            const dim3 fb(kFaceTX, kFaceTY, 1);
+            kt_flux_face_kernel<NQ, EOS, 1><<<face_grid<1>(a), fb, 0, s>>>(a);
+            mark(1);
+            kt_flux_face_kernel<NQ, EOS, 2><<<face_grid<2>(a), fb, 0, s>>>(a);
+            mark(2);
+            if (z) { kt_flux_face_kernel<NQ, EOS, 3><<<face_grid<3>(a), fb, 0, s>>>(a); mark(3); }
+        }
     } else if (flux_staged() && flux_form() != 0) {
         const dim3 g3((a.nx + 31) / 32, a.ny, (a.nz + 3) / 4);
         if (flux_form() == 2) {

@@ -214,3 +214,24 @@ def test_mixed_results_same_in_every_process_and_with_poisoned_memory():
         out.append([ln for ln in r.stdout.splitlines() if ln.startswith("HASH")][-1])
     assert out[0].split()[1] == "0", out[0]
     assert len(set(out)) == 1, out
+
+
+def test_mixed_face_forms_agree():
+    """the face-once flux over line pieces (along y and eta, the default) and
+    over 32 x 8 face tiles (VH_FACE_FORM=tiles) compute every face and every
+    cell update with the same arithmetic: the same bits (child processes:
+    the form is chosen once per process)"""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    child = _REPRO.split("# an autotuned batch")[0] + 'print("HASH", rc, h.hexdigest())\n'
+    out = []
+    for form in ("tiles", "lines"):
+        env = dict(os.environ, VH_FACE_FORM=form,
+                   PYTHONPATH=os.pathsep.join([os.path.join(root, "cpu-vh_b200"), root]))
+        env.pop("VH_POISON_ALLOC", None)
+        r = subprocess.run([sys.executable, "-c", child], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out.append([ln for ln in r.stdout.splitlines() if ln.startswith("HASH")][-1])
+    assert out[0].split()[1] == "0" and out[0] == out[1], out
