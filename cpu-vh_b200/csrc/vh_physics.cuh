@@ -50,15 +50,27 @@ static __device__ __noinline__ double div_ieee(double a, double b) { return a / 
  * Handbook of Floating-Point Arithmetic, ch. 4): q0 = RN(a*y) is within one
  * ulp of a/b, r = a - q0*b is exact with an FMA, and RN(q0 + r*y) = RN(a/b).
  * One reciprocal then serves every division by the same b at the cost of a
- * multiply and two FMAs each -- bit-identical to `a / b`.  Zero, non-finite,
- * huge or near-subnormal operands, where the exactness argument needs more
- * care, take the IEEE division. */
+ * multiply and two FMAs each -- bit-identical to `a / b`.  The range test
+ * (|a|, |y| >= 2^-960 and 2^-960 <= |q0| < 2^1000) reads the high words
+ * with integer operations.  A zero numerator over a finite b gives q0 = a * y =
+ * +-0 with the sign of a XOR the sign of b, which is a / b exactly (zero
+ * numerators are common: velocity and viscous components that are still
+ * exactly 0).  Non-finite, huge or near-subnormal operands, where the
+ * exactness argument needs more care, take the IEEE division. */
 __device__ __forceinline__ double div_rcp(double a, double b, double y)
 {
+    constexpr unsigned kLo = 0x03f00000u;      /* high word of 2^-960 */
+    constexpr unsigned kHi = 0x7e700000u;      /* high word of 2^1000 */
     const double q0 = a * y;
-    if (!(fabs(q0) >= 0x1p-960 && fabs(q0) <= 0x1p1000 && fabs(a) >= 0x1p-960)) return div_ieee(a, b);
-    const double r = fma(-q0, b, a);
-    return fma(r, y, q0);
+    const unsigned ha = (unsigned)__double2hiint(a) & 0x7fffffffu;
+    const unsigned hq = (unsigned)__double2hiint(q0) & 0x7fffffffu;
+    const unsigned hy = (unsigned)__double2hiint(y) & 0x7fffffffu;
+    if (ha >= kLo && hq >= kLo && hq < kHi && hy >= kLo) {
+        const double r = fma(-q0, b, a);
+        return fma(r, y, q0);
+    }
+    if ((ha | (unsigned)__double2loint(a)) == 0u && hq < 0x7ff00000u) return q0;
+    return div_ieee(a, b);
 }
 
 /* ------------------------------------------------------------------ EoS */
@@ -257,9 +269,11 @@ __device__ __forceinline__ double dvr(double a, double b, double y) { return div
 __device__ __forceinline__ float dvr(float a, float, float y) { return a * y; }
 
 /* SourceTerms.cpp:55-313, the right-hand side of the pi^{mu nu} (and Pi)
- * relaxation equations divided by u^tau. */
+ * relaxation equations divided by u^tau.  yt = RN(1/t); every division by
+ * t, 2t, t^2 and 5 goes through the shared reciprocal (dvr: the same
+ * quotient in FP64, a product in FP32). */
 template <typename R, int EOS, bool BULK>
-__device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, R *rhs, R t, double e_d, double p_d,
+__device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, R *rhs, R t, R yt, double e_d, double p_d,
     double ut_d, double ux_d, double uy_d, double un_d, double utp, double uxp, double uyp, double unp,
     const R *pv, R Pi,
     R dxut, R dyut, R dnut, R dxux, R dyux, R dnux,
@@ -272,17 +286,18 @@ __device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, R *rhs, R t, double e
     const R pixy = pv[5], pixn = pv[6], piyy = pv[7], piyn = pv[8], pinn = pv[9];
     R T = R(eos_T<EOS>(E, e_d));
     R taupiInv = T / 5 / d_etabar;
-    R beta_pi = (e + p) / 5;
+    R beta_pi = dvr(e + p, R(5), R(0.2));
     R cs2 = R(eos_cs2<EOS>(E, e_d));
     R a = R(1.0) / R(3.0) - cs2;
     R a2 = a * a;
     R beta_Pi = 15 * a2 * (e + p);
-    R lambda_Pipi = 8 * a / 5;
+    R lambda_Pipi = dvr(8 * a, R(5), R(0.2));
     R tauPiInv = R(0.0);
     /* in FP64 for both precisions: zeta/s underflows FP32 far from its peak
      * while a2 = 0 for both EoS kinds, and 0/0 must not appear */
     if (BULK) tauPiInv = R(15 * double(a2) * double(T) / zeta_over_s(Z, double(T)));
     R ut2 = ut * ut, un2 = un * un, t2 = t * t, t3 = t * t2;
+    const R yt2 = R(1.0) / t2, y2t = yt * R(0.5);   /* RN(1/t^2); RN(1/(2t)) = RN(1/t) / 2 */
     const R kThird = R(1.0) / R(3.0), yut = R(1.0) / ut, ydt = R(1.0) / d_dt;
     R dtut = dvr(R(ut_d - utp), d_dt, ydt), dtux = dvr(R(ux_d - uxp), d_dt, ydt), dtuy = dvr(R(uy_d - uyp), d_dt, ydt), dtun = dvr(R(un_d - unp), d_dt, ydt);
     R Dut = ut * dtut + ux * dxut + uy * dyut + un * dnut + t * un * un;
@@ -290,30 +305,30 @@ __device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, R *rhs, R t, double e
     R Dux = -DuxUpper;
     R DuyUpper = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
     R Duy = -DuyUpper;
-    R DunUpper = ut * dtun + ux * dxun + uy * dyun + un * dnun + 2 * ut * un / t;
+    R DunUpper = ut * dtun + ux * dxun + uy * dyun + un * dnun + dvr(2 * ut * un, t, yt);
     R Dun = -t2 * DunUpper;
     R dut = Dut - t * un * un;
     R dux = ut * dtux + ux * dxux + uy * dyux + un * dnux;
     R duy = ut * dtuy + ux * dxuy + uy * dyuy + un * dnuy;
     R dun = ut * dtun + ux * dxun + uy * dyun + un * dnun;
-    R theta = ut / t + dtut + dxux + dyuy + dnun;
+    R theta = dvr(ut, t, yt) + dtut + dxux + dyuy + dnun;
     R stt = -t * ut * un2 + (dtut - ut * dut) + dvr((ut2 - 1) * theta, R(3.0), kThird);
     R stx = -(t * un2 * ux) / R(2.0) + (dtux - dxut) / R(2.0) - (ux * dut + ut * dux) / R(2.0) + dvr(ut * ux * theta, R(3.0), kThird);
     R sty = -(t * un2 * uy) / R(2.0) + (dtuy - dyut) / R(2.0) - (uy * dut + ut * duy) / R(2.0) + dvr(ut * uy * theta, R(3.0), kThird);
-    R stn = -un * (R(2.0) * ut2 + t2 * un2) / (R(2.0) * t) + (dtun - dnut / t2) / R(2.0) - (un * dut + ut * dun) / R(2.0) + dvr(ut * un * theta, R(3.0), kThird);
+    R stn = dvr(-un * (R(2.0) * ut2 + t2 * un2), R(2.0) * t, y2t) + (dtun - dvr(dnut, t2, yt2)) / R(2.0) - (un * dut + ut * dun) / R(2.0) + dvr(ut * un * theta, R(3.0), kThird);
     R sxx = -(dxux + ux * dux) + dvr((R(1.0) + ux * ux) * theta, R(3.0), kThird);
     R sxy = -(dxuy + dyux) / R(2.0) - (uy * dux + ux * duy) / R(2.0) + dvr(ux * uy * theta, R(3.0), kThird);
-    R sxn = -ut * ux * un / t - (dxun + dnux / t2) / R(2.0) - (un * dux + ux * dun) / R(2.0) + dvr(ux * un * theta, R(3.0), kThird);
+    R sxn = dvr(-ut * ux * un, t, yt) - (dxun + dvr(dnux, t2, yt2)) / R(2.0) - (un * dux + ux * dun) / R(2.0) + dvr(ux * un * theta, R(3.0), kThird);
     R syy = -(dyuy + uy * duy) + dvr((R(1.0) + uy * uy) * theta, R(3.0), kThird);
-    R syn = -ut * uy * un / t - (dyun + dnuy / t2) / R(2.0) - (un * duy + uy * dun) / R(2.0) + dvr(uy * un * theta, R(3.0), kThird);
-    R snn = -ut * (R(1.0) + R(2.0) * t2 * un2) / t3 - dnun / t2 - un * dun + dvr((R(1.0) / t2 + un2) * theta, R(3.0), kThird);
+    R syn = dvr(-ut * uy * un, t, yt) - (dyun + dvr(dnuy, t2, yt2)) / R(2.0) - (un * duy + uy * dun) / R(2.0) + dvr(uy * un * theta, R(3.0), kThird);
+    R snn = -ut * (R(1.0) + R(2.0) * t2 * un2) / t3 - dvr(dnun, t2, yt2) - un * dun + dvr((yt2 + un2) * theta, R(3.0), kThird);
     R wtx = (-dtux - dxut + ut * dux - ux * dut - t * un2 * ux) / R(2.0);
     R wty = (-dtuy - dyut + ut * duy - uy * dut - t * un2 * uy) / R(2.0);
     R wtn = (-t2 * dtun - R(2.0) * t * un - dnut - ut * Dun - t2 * un * dut - t3 * un * un2) / R(2.0);
     R wxy = (dxuy - dyux + ux * duy - uy * dux) / R(2.0);
     R wxn = (t2 * dxun - dnux - ux * Dun - t2 * un * dux) / R(2.0);
     R wyn = (t2 * dyun - dnuy - uy * Dun - t2 * un * duy) / R(2.0);
-    R wxt = wtx, wyt = wty, wnt = wtn / t2, wyx = -wxy, wnx = -wxn / t2, wny = -wyn / t2;
+    R wxt = wtx, wyt = wty, wnt = dvr(wtn, t2, yt2), wyx = -wxy, wnx = dvr(-wxn, t2, yt2), wny = dvr(-wyn, t2, yt2);
     R I1tt = R(2.0) * ut * (pitt * Dut + pitx * Dux + pity * Duy + pitn * Dun);
     R I1tx = (pitt * ux + pitx * ut) * Dut + (pitx * ux + pixx * ut) * Dux + (pity * ux + pixy * ut) * Duy + (pitn * ux + pixn * ut) * Dun;
     R I1ty = (pitt * uy + pity * ut) * Dut + (pitx * uy + pixy * ut) * Dux + (pity * uy + piyy * ut) * Duy + (pitn * uy + piyn * ut) * Dun;
@@ -347,7 +362,7 @@ __device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, R *rhs, R t, double e
     R I4xn = (pitx * stn + pitn * stx) / R(2.0) - (pixx * sxn + pixn * sxx) / R(2.0) - (pixy * syn + piyn * sxy) / R(2.0) - t2 * (pixn * snn + pinn * sxn) / R(2.0) + dvr((ux * un) * ps, R(3.0), kThird);
     R I4yy = (pity * sty - pixy * sxy - piyy * syy - t2 * piyn * syn) + dvr((R(1.0) + uy2) * ps, R(3.0), kThird);
     R I4yn = (pity * stn + pitn * sty) / R(2.0) - (pixy * sxn + pixn * sxy) / R(2.0) - (piyy * syn + piyn * syy) / R(2.0) - t2 * (piyn * snn + pinn * syn) / R(2.0) + dvr((uy * un) * ps, R(3.0), kThird);
-    R I4nn = (pitn * stn - pixn * sxn - piyn * syn - t2 * pinn * snn) + dvr((R(1.0) / t2 + un2) * ps, R(3.0), kThird);
+    R I4nn = (pitn * stn - pixn * sxn - piyn * syn - t2 * pinn * snn) + dvr((yt2 + un2) * ps, R(3.0), kThird);
     R Itt = I1tt + delta_pipi * I2tt - I3tt + tau_pipi * I4tt - lambda_piPi * Pi * stt;
     R Itx = I1tx + delta_pipi * I2tx - I3tx + tau_pipi * I4tx - lambda_piPi * Pi * stx;
     R Ity = I1ty + delta_pipi * I2ty - I3ty + tau_pipi * I4ty - lambda_piPi * Pi * sty;
@@ -361,13 +376,13 @@ __device__ void pimunu_rhs(const DevEos &E, const Zeta &Z, R *rhs, R t, double e
     R dpitt = R(2.0) * beta_pi * stt - pitt * taupiInv - Itt - R(2.0) * un * t * pitn;
     R dpitx = R(2.0) * beta_pi * stx - pitx * taupiInv - Itx - un * t * pixn;
     R dpity = R(2.0) * beta_pi * sty - pity * taupiInv - Ity - un * t * piyn;
-    R dpitn = R(2.0) * beta_pi * stn - pitn * taupiInv - Itn - un * t * pinn - (ut * pitn + un * pitt) / t;
+    R dpitn = R(2.0) * beta_pi * stn - pitn * taupiInv - Itn - un * t * pinn - dvr(ut * pitn + un * pitt, t, yt);
     R dpixx = R(2.0) * beta_pi * sxx - pixx * taupiInv - Ixx;
     R dpixy = R(2.0) * beta_pi * sxy - pixy * taupiInv - Ixy;
-    R dpixn = R(2.0) * beta_pi * sxn - pixn * taupiInv - Ixn - (ut * pixn + un * pitx) / t;
+    R dpixn = R(2.0) * beta_pi * sxn - pixn * taupiInv - Ixn - dvr(ut * pixn + un * pitx, t, yt);
     R dpiyy = R(2.0) * beta_pi * syy - piyy * taupiInv - Iyy;
-    R dpiyn = R(2.0) * beta_pi * syn - piyn * taupiInv - Iyn - (ut * piyn + un * pity) / t;
-    R dpinn = R(2.0) * beta_pi * snn - pinn * taupiInv - Inn - 2 * (ut * pinn + un * pitn) / t;
+    R dpiyn = R(2.0) * beta_pi * syn - piyn * taupiInv - Iyn - dvr(ut * piyn + un * pity, t, yt);
+    R dpinn = R(2.0) * beta_pi * snn - pinn * taupiInv - Inn - dvr(2 * (ut * pinn + un * pitn), t, yt);
     rhs[0] = dvr(dpitt, ut, yut) + pitt * dkvk;
     rhs[1] = dvr(dpitx, ut, yut) + pitx * dkvk;
     rhs[2] = dvr(dpity, ut, yut) + pity * dkvk;

@@ -604,7 +604,7 @@ __device__ __forceinline__ void source_update(const StageArgs &A, long long s, d
     S[1] = s1 - div_rcp(Qv[1], t, yt) - dxp + dkvk * Qv[5];
     S[2] = s2 - div_rcp(Qv[2], t, yt) - dyp + dkvk * Qv[6];
     S[3] = s3 - div_rcp(3 * Qv[3], t, yt) - dnp / A.t2pow + dkvk * Qv[7];
-    pimunu_rhs<double, EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, e, p, ut, ux, uy, un,
+    pimunu_rhs<double, EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, yt, e, p, ut, ux, uy, un,
                               __ldg(A.upin + s), __ldg(A.upin + L + s), __ldg(A.upin + 2 * L + s), __ldg(A.upin + 3 * L + s),
                               Qv + 4, Pi, dxut, dyut, dnut, dxux, dyux, dnux, dxuy, dyuy, dnuy, dxun, dyun, dnun, dkvk,
                               A.etabar, A.dt);
@@ -886,7 +886,7 @@ __device__ __forceinline__ void source_update_m(const StageArgs &A, long long s,
     float pvf[10];
 #pragma unroll
     for (int n = 0; n < 10; ++n) pvf[n] = (float)Qv[4 + n];
-    pimunu_rhs<float, EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, e, p, utd, uxd, uyd, und,
+    pimunu_rhs<float, EOS, NQ == 15>(A.eos, A.zeta, S + 4, t, yt, e, p, utd, uxd, uyd, und,
                                      __ldg(A.upin + s), __ldg(A.upin + L + s), __ldg(A.upin + 2 * L + s), __ldg(A.upin + 3 * L + s),
                                      pvf, Pi, dxut, dyut, dnut, dxux, dyux, dnux, dxuy, dyuy, dnuy, dxun, dyun, dnun, dkvk,
                                      (float)A.etabar, (float)A.dt);
