@@ -201,6 +201,24 @@ __device__ __forceinline__ void cp_async8(double *smem, const double *gmem)
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+/* hint: bring the line holding *p into L2 */
+__device__ __forceinline__ void prefetch_l2(const double *p)
+{
+    asm volatile("prefetch.global.L2 [%0];\n" ::"l"(__cvta_generic_to_global(p)));
+}
+
+/* the values a flux launch along dir reads for cell s only after its root
+ * solves -- the accumulator it adds to, u^tau and u^dir of the direction
+ * sources -- requested into L2 when the block starts (no registers held) */
+template <int NQ>
+__device__ __forceinline__ void prefetch_flux_cell(const StageArgs &A, long long s, int dir)
+{
+#pragma unroll 1
+    for (int n = 0; n < NQ; ++n) prefetch_l2(A.qout + n * A.L + s);
+    prefetch_l2(A.uin + s);
+    prefetch_l2(A.uin + dir * A.L + s);
+}
+
 /* One block of the staged flux along DIR: TX x TY cells (x by y for DIR 1
  * and 2, x by eta for DIR 3, at the block's fixed third coordinate) and the
  * 2-cell halo along DIR, all NQ components, copied asynchronously into sm
@@ -428,6 +446,22 @@ __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__r
         if (x >= A.nx) return -1;
         return (DIR == 2) ? (x + 2) + sxy * (o + 2) : (x + 2) + A.ncx * (o + 2);
     };
+    /* this thread's cell (valid: inside the lattice) */
+    const int w = tid % W, pr = tid / W;
+    const long long R = R0 + pr;
+    long long b = 0, bb = -1;
+    int pos = 0;
+    if (R < Rtot) {
+        b = R / nd;
+        pos = (int)(R - b * nd);
+        bb = base(b, w);
+    }
+    const bool valid = bb >= 0;
+    const long long s = valid ? bb + (long long)(pos + 2) * gst : 0;
+    if (valid) {
+        prefetch_flux_cell<NQ>(A, s, DIR);
+        prefetch_l2(A.ein + s);
+    }
     /* staging: slot l covers positions [first_l - 2, first_l + len_l + 2) of
      * bundle b0 + l at shared indices [M_l, M_l + len_l + 4) */
     const int mlen_max = PS / W;
@@ -464,15 +498,7 @@ __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__r
         }
     }
     __syncthreads();
-    /* this thread's cell */
-    const int w = tid % W, pr = tid / W;
-    const long long R = R0 + pr;
-    if (R >= Rtot) return;
-    const long long b = R / nd;
-    const int pos = (int)(R - b * nd);
-    const long long bb = base(b, w);
-    if (bb < 0) return;
-    const long long s = bb + (long long)(pos + 2) * gst;
+    if (!valid) return;
     const int ts = ((int)(R - R0) + 2 + 4 * (int)(b - b0)) * W + w;
     constexpr int tst = W;
     const QTile qt{sm, PS};
@@ -1009,6 +1035,7 @@ __device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int 
     bool bad = false;
     double H[NQ];
     if (face_ok) {
+        prefetch_flux_cell<NQ>(A, s, DIR);
         face_H_m<NQ, EOS>(A, s - st, st, DIR, __ldg(A.ein + s), H, bad);
         if constexpr (DIR != 1) {
 #pragma unroll
@@ -1101,6 +1128,7 @@ __device__ __forceinline__ void flux_faces_lines(const StageArgs &A, double *__r
     bool bad = false;
     double H[NQ];
     if (face_ok) {
+        prefetch_flux_cell<NQ>(A, s, DIR);
         face_H_m<NQ, EOS>(A, s - st, st, DIR, __ldg(A.ein + s), H, bad);
     } else {
 #pragma unroll
