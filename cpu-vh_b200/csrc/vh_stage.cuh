@@ -201,6 +201,15 @@ __device__ __forceinline__ void cp_async8(double *smem, const double *gmem)
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+/* Programmatic dependent launch (kernels launched with
+ * cudaLaunchAttributeProgrammaticStreamSerialization).  pdl_trigger lets the
+ * next kernel on the stream start once every block of this one has issued
+ * it; pdl_wait returns once the previous kernel on the stream has completed
+ * and its writes are visible.  A kernel launched without the attribute
+ * passes both at once. */
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory"); }
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;\n" ::: "memory"); }
+
 /* hint: bring the line holding *p into L2 */
 __device__ __forceinline__ void prefetch_l2(const double *p)
 {
@@ -417,9 +426,13 @@ struct FluxLines {
     }
 };
 
-template <int NQ, int EOS, int DIR, int UNR = 1>
+template <int NQ, int EOS, int DIR, int UNR = 1, bool PDL = false>
 __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__restrict__ sm)
 {
+    /* with PDL, only the update of the accumulator (written by the previous
+     * phase) waits for the previous kernel; the staged stencil, e and u are
+     * the stage's inputs, complete before the stage's first kernel started */
+    if (PDL) pdl_trigger();
     using G = FluxLines<DIR>;
     constexpr int W = G::W, PB = G::PB;
     const int nd = (DIR == 1) ? A.nx : (DIR == 2) ? A.ny : A.nz;
@@ -533,6 +546,7 @@ __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__r
     const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
     double S[4];
     dir_sources_t<NQ>(A, qt, ts, tst, s, d, DIR, S);
+    if (PDL) pdl_wait();
 #pragma unroll UNR
     for (int n = 0; n < NQ; ++n) {
         const double *q = sm + n * PS + ts, *h = hs + n * PS + ts;
@@ -1013,9 +1027,10 @@ __device__ __forceinline__ void face_H_m(const StageArgs &A, long long b, long l
 
 /* one tile of the face-once flux along DIR; (i0, j0, k0) interior coordinates
  * of the block's first face-owning cell; sm holds NQ * TX * TY doubles */
-template <int NQ, int EOS, int DIR, int TX, int TY>
+template <int NQ, int EOS, int DIR, int TX, int TY, bool PDL = false>
 __device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int j0, int k0, double *__restrict__ sm)
 {
+    if (PDL) pdl_trigger();   /* see flux_lines_block */
     const int tx = threadIdx.x, ty = threadIdx.y, tid = tx + TX * ty;
     const int i = i0 + tx + 2;
     const int j = (DIR == 3) ? j0 + 2 : j0 + ty + 2;
@@ -1077,6 +1092,7 @@ __device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int 
         for (int n = 0; n < 4; ++n) r[n] = (r[n] * yd + S[n]) * A.dt;
 #pragma unroll
         for (int n = 4; n < NQ; ++n) r[n] *= yd * A.dt;
+        if (PDL) pdl_wait();
 #pragma unroll
         for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] += r[n];
     }
@@ -1094,9 +1110,10 @@ __device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int 
  * arithmetic, the next face through shared memory and the recomputation
  * across the root solve's e <= 0.1 branch are those of flux_faces_tile, so
  * a cell's update is the same.  sm: NQ * 128 doubles. */
-template <int NQ, int EOS, int DIR>
+template <int NQ, int EOS, int DIR, bool PDL = false>
 __device__ __forceinline__ void flux_faces_lines(const StageArgs &A, double *__restrict__ sm)
 {
+    if (PDL) pdl_trigger();   /* see flux_lines_block */
     using G = FluxLines<DIR>;
     constexpr int W = G::W, PB = G::PB;
     const int nd = (DIR == 1) ? A.nx : (DIR == 2) ? A.ny : A.nz;
@@ -1158,6 +1175,7 @@ __device__ __forceinline__ void flux_faces_lines(const StageArgs &A, double *__r
         for (int n = 0; n < 4; ++n) r[n] = (r[n] * yd + S[n]) * A.dt;
 #pragma unroll
         for (int n = 4; n < NQ; ++n) r[n] *= yd * A.dt;
+        if (PDL) pdl_wait();
 #pragma unroll
         for (int n = 0; n < NQ; ++n) A.qout[n * A.L + s] += r[n];
     }

@@ -62,6 +62,8 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_stage_kernel(cons
 template <int NQ, int EOS, bool MIXED>
 __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_source_kernel(const __grid_constant__ StageArgs A)
 {
+    pdl_wait();       /* reads the previous stage's results: wait, then let the flux start */
+    pdl_trigger();
     int i, j, k;
     long long s;
     if (!stage_cell_flat(A, i, j, k, s)) return;
@@ -129,6 +131,36 @@ __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_flux_slopes_kerne
     flux_slopes_tile<NQ, EOS, DIR, TX, TY>(A, i0, j0, k0, smd);
 }
 
+/* The phase-split stage's kernels go out with programmatic dependent
+ * launch: each flux kernel starts its staging and root solves while the
+ * previous phase drains and waits only before adding to the accumulator
+ * (flux_lines_block); the source and finalize kernels wait at their start.
+ * VH_PDL=0 launches them in plain stream order. */
+static inline bool pdl_enabled()
+{
+    static int on = [] {
+        const char *e = getenv("VH_PDL");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return on == 1;
+}
+
+template <typename... P>
+static void launch_pdl(void (*kernel)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, const StageArgs &a)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, kernel, a);
+}
+
 template <int NQ, int EOS, int DIR>
 static void launch_flux_slopes(const StageArgs &a, dim3 grid, dim3 block, cudaStream_t s)
 {
@@ -150,7 +182,7 @@ template <int NQ, int EOS, int DIR, int MB, int UNR>
 __global__ void __launch_bounds__(128, MB) kt_flux_lines_kernel(const __grid_constant__ StageArgs A)
 {
     extern __shared__ double smd[];
-    flux_lines_block<NQ, EOS, DIR, UNR>(A, smd);
+    flux_lines_block<NQ, EOS, DIR, UNR, true>(A, smd);
 }
 
 template <int NQ, int EOS, int DIR, int MB, int UNR = 1>
@@ -174,7 +206,7 @@ static void launch_flux_lines(const StageArgs &a, cudaStream_t s)
     }
     const long long runs = (long long)nd * G::bundles(a.nx, a.ny, a.nz);
     const unsigned blocks = (unsigned)((runs + G::PB - 1) / G::PB);
-    kt_flux_lines_kernel<NQ, EOS, DIR, MB, UNR><<<blocks, 128, bytes, s>>>(a);
+    launch_pdl(kt_flux_lines_kernel<NQ, EOS, DIR, MB, UNR>, dim3(blocks), dim3(128), bytes, s, a);
 }
 
 /* FP64 flux form of the phase-split stage: VH_FLUX_FORM=lines (default:
@@ -221,7 +253,7 @@ __global__ void __launch_bounds__(kFaceTX * kFaceTY, 2) kt_flux_face_kernel(cons
     if (DIR == 1) { i0 = blockIdx.x * (kFaceTX - 1); j0 = blockIdx.y * kFaceTY; k0 = blockIdx.z; }
     else if (DIR == 2) { i0 = blockIdx.x * kFaceTX; j0 = blockIdx.y * (kFaceTY - 1); k0 = blockIdx.z; }
     else { i0 = blockIdx.x * kFaceTX; j0 = blockIdx.y; k0 = blockIdx.z * (kFaceTY - 1); }
-    flux_faces_tile<NQ, EOS, DIR, kFaceTX, kFaceTY>(A, i0, j0, k0, sm);
+    flux_faces_tile<NQ, EOS, DIR, kFaceTX, kFaceTY, true>(A, i0, j0, k0, sm);
 }
 
 /* the face-once flux over line pieces (flux_faces_lines), 128 threads */
@@ -229,7 +261,7 @@ template <int NQ, int EOS, int DIR, int MB>
 __global__ void __launch_bounds__(128, MB) kt_flux_face_lines_kernel(const __grid_constant__ StageArgs A)
 {
     __shared__ double sm[NQ * 128];
-    flux_faces_lines<NQ, EOS, DIR>(A, sm);
+    flux_faces_lines<NQ, EOS, DIR, true>(A, sm);
 }
 
 template <int NQ, int EOS, int DIR, int MB>
@@ -239,7 +271,7 @@ static void launch_flux_face_lines(const StageArgs &a, cudaStream_t s)
     const int nd = (DIR == 1) ? a.nx : (DIR == 2) ? a.ny : a.nz;
     const long long faces = (long long)(nd + 1) * G::bundles(a.nx, a.ny, a.nz);
     const unsigned blocks = (unsigned)((faces + G::PB - 2) / (G::PB - 1));
-    kt_flux_face_lines_kernel<NQ, EOS, DIR, MB><<<blocks, 128, 0, s>>>(a);
+    launch_pdl(kt_flux_face_lines_kernel<NQ, EOS, DIR, MB>, dim3(blocks), dim3(128), 0, s, a);
 }
 
 /* mixed-precision flux form of the phase-split stage: VH_FACE_FORM=lines
@@ -273,6 +305,8 @@ static inline dim3 face_grid(const StageArgs &a)
 template <int NQ, int EOS, bool HAS_Z, bool STAGE2, bool MIXED>
 __global__ void __launch_bounds__(128, VH_STAGE_MIN_BLOCKS) kt_final_kernel(const __grid_constant__ StageArgs A)
 {
+    pdl_wait();       /* reads the accumulated update */
+    pdl_trigger();
     int i, j, k;
     long long s;
     if (!stage_cell_flat(A, i, j, k, s)) return;
@@ -325,23 +359,23 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
         return;
     }
     const dim3 gflat((unsigned)(((long long)a.nx * a.ny * a.nz + 127) / 128));
-    kt_source_kernel<NQ, EOS, MIXED><<<gflat, 128, 0, s>>>(a);
+    launch_pdl(kt_source_kernel<NQ, EOS, MIXED>, gflat, dim3(128), 0, s, a);
     mark(0);
     if constexpr (MIXED) {
         if (face_form() != 0) {
             const dim3 fb(kFaceTX, kFaceTY, 1);
-            kt_flux_face_kernel<NQ, EOS, 1><<<face_grid<1>(a), fb, 0, s>>>(a);
+            launch_pdl(kt_flux_face_kernel<NQ, EOS, 1>, face_grid<1>(a), fb, 0, s, a);
             mark(1);
             launch_flux_face_lines<NQ, EOS, 2, 4>(a, s);
             mark(2);
             if (z) { launch_flux_face_lines<NQ, EOS, 3, 4>(a, s); mark(3); }
         } else {
             const dim3 fb(kFaceTX, kFaceTY, 1);
-            kt_flux_face_kernel<NQ, EOS, 1><<<face_grid<1>(a), fb, 0, s>>>(a);
+            launch_pdl(kt_flux_face_kernel<NQ, EOS, 1>, face_grid<1>(a), fb, 0, s, a);
             mark(1);
-            kt_flux_face_kernel<NQ, EOS, 2><<<face_grid<2>(a), fb, 0, s>>>(a);
+            launch_pdl(kt_flux_face_kernel<NQ, EOS, 2>, face_grid<2>(a), fb, 0, s, a);
             mark(2);
-            if (z) { kt_flux_face_kernel<NQ, EOS, 3><<<face_grid<3>(a), fb, 0, s>>>(a); mark(3); }
+            if (z) { launch_pdl(kt_flux_face_kernel<NQ, EOS, 3>, face_grid<3>(a), fb, 0, s, a); mark(3); }
         }
     } else if (flux_staged() && flux_form() != 0) {
         const dim3 g3((a.nx + 31) / 32, a.ny, (a.nz + 3) / 4);
@@ -378,10 +412,10 @@ static void launch_stage_t(const StageArgs &a, cudaStream_t s, StageMarks *m)
         mark(2);
         if (z) { kt_flux_kernel<NQ, EOS, 3, MIXED><<<grid, block, 0, s>>>(a); mark(3); }
     }
-    if (z && st2) kt_final_kernel<NQ, EOS, true, true, MIXED><<<gflat, 128, 0, s>>>(a);
-    else if (z) kt_final_kernel<NQ, EOS, true, false, MIXED><<<gflat, 128, 0, s>>>(a);
-    else if (st2) kt_final_kernel<NQ, EOS, false, true, MIXED><<<gflat, 128, 0, s>>>(a);
-    else kt_final_kernel<NQ, EOS, false, false, MIXED><<<gflat, 128, 0, s>>>(a);
+    if (z && st2) launch_pdl(kt_final_kernel<NQ, EOS, true, true, MIXED>, gflat, dim3(128), 0, s, a);
+    else if (z) launch_pdl(kt_final_kernel<NQ, EOS, true, false, MIXED>, gflat, dim3(128), 0, s, a);
+    else if (st2) launch_pdl(kt_final_kernel<NQ, EOS, false, true, MIXED>, gflat, dim3(128), 0, s, a);
+    else launch_pdl(kt_final_kernel<NQ, EOS, false, false, MIXED>, gflat, dim3(128), 0, s, a);
     mark(4);
 }
 
