@@ -647,7 +647,8 @@ int vh_event_freezeout_launch(vh_event *ev)
     fo_args(ev, a);
     vh::launch_freezeout(a, ev->stream);
     CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaMemcpyAsync(ev->fo_hdr, ev->fo_scratch + ev->fo_scratch_ints - 2, 2 * sizeof(int),
+    /* header words 1 and 2: cells above e_F, elements */
+    CUDA_TRY(cudaMemcpyAsync(ev->fo_hdr, ev->fo_scratch + ev->fo_scratch_ints - vh::kFoHeaderInts + 1, 2 * sizeof(int),
                              cudaMemcpyDeviceToHost, ev->stream));
     CUDA_TRY(cudaEventRecord(ev->fo_done, ev->stream));
     ev->fo_pending = true;

@@ -59,7 +59,7 @@ constexpr int kMaxHedra = 10;     /* Hypercube MAX_POLY, cornelius.cpp:1703 */
 constexpr int kMaxElements = 10;  /* Cornelius MAX_ELEMENTS, cornelius.cpp:2004 */
 
 struct Poly {
-    unsigned char line[kMaxPolyLines];
+    unsigned short line[kMaxPolyLines];   /* line indices (a block's shared pool may hold 512) */
     int nlines, const_i, x1, x2, x3;
     double cen[D];
     bool have_cen;
@@ -98,6 +98,32 @@ __device__ __forceinline__ void orient(double *n, const double *out)
     for (int i = 0; i < D; i++) dot += out[i] * n[i];
     if (dot < 0)
         for (int i = 0; i < D; i++) n[i] = -n[i];
+}
+
+/* The number of edge cuts square_lines finds (0, 2 or 4; anything else is
+ * its error), from the same comparisons, without computing the cuts: a
+ * cube's line count before its lines are built. */
+__device__ __forceinline__ int square_cut_count(const double P[2][2], double E0)
+{
+    int above = 0;
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++)
+            if (P[i][j] >= E0) above++;
+    if (above == 0 || above == 4) return 0;
+    int nc = 0;
+    if ((P[0][0] - E0) * (P[1][0] - E0) < 0) nc++;
+    else if (P[0][0] == E0 && P[1][0] < E0) nc++;
+    else if (P[1][0] == E0 && P[0][0] < E0) nc++;
+    if ((P[0][0] - E0) * (P[0][1] - E0) < 0) nc++;
+    else if (P[0][0] == E0 && P[0][1] < E0) nc++;
+    else if (P[0][1] == E0 && P[0][0] < E0) nc++;
+    if ((P[1][0] - E0) * (P[1][1] - E0) < 0) nc++;
+    else if (P[1][0] == E0 && P[1][1] < E0) nc++;
+    else if (P[1][1] == E0 && P[1][0] < E0) nc++;
+    if ((P[0][1] - E0) * (P[1][1] - E0) < 0) nc++;
+    else if (P[0][1] == E0 && P[1][1] < E0) nc++;
+    else if (P[1][1] == E0 && P[0][1] < E0) nc++;
+    return nc;
 }
 
 /* Square::construct_lines with ends_of_edge and find_outside
@@ -190,7 +216,7 @@ __device__ __forceinline__ bool poly_add_line(WorkRef &w, Poly &p, int l, bool d
 {
     if (donotcheck || p.nlines == 0) {
         if (p.nlines >= kMaxPolyLines) { w.error = true; return false; }
-        p.line[p.nlines++] = (unsigned char)l;
+        p.line[p.nlines++] = (unsigned short)l;
         return true;
     }
     const double *p1 = lstart(w, l), *p2 = lend(w, l), *p3 = lend(w, p.line[p.nlines - 1]);
@@ -199,7 +225,7 @@ __device__ __forceinline__ bool poly_add_line(WorkRef &w, Poly &p, int l, bool d
     if (diff1 < 1e-10 || diff2 < 1e-10) {
         if (diff2 < 1e-10) w.flip[l] ^= 1;
         if (p.nlines >= kMaxPolyLines) { w.error = true; return false; }
-        p.line[p.nlines++] = (unsigned char)l;
+        p.line[p.nlines++] = (unsigned short)l;
         return true;
     }
     return false;
@@ -311,6 +337,32 @@ static __device__ int cube_polygons(WorkRef &w, const double cube[2][2][2], int 
         w.np++;
     }
     return nlines;
+}
+
+/* cube_polygons' line count and square ambiguity count (squares with two
+ * lines) from the corner comparisons alone; err as square_lines would set
+ * it.  cube_polygons then finds exactly this many lines. */
+__device__ __forceinline__ int cube_line_count(const double cube[2][2][2], int const_i, double E0, int &amb, bool &err)
+{
+    int x1 = -1, x2 = -1;
+    for (int i = 0; i < D; i++)
+        if (i != const_i) { if (x1 < 0) x1 = i; else if (x2 < 0) x2 = i; }
+    int n = 0;
+    amb = 0;
+    for (int i = 0; i < D; i++) {
+        if (i == const_i) continue;
+        for (int j = 0; j < 2; j++) {
+            double sq[2][2];
+            for (int a = 0; a < 2; a++)
+                for (int b = 0; b < 2; b++)
+                    sq[a][b] = (i == x1) ? cube[j][a][b] : (i == x2) ? cube[a][j][b] : cube[a][b][j];
+            const int nc = square_cut_count(sq, E0);
+            if (nc != 0 && nc != 2 && nc != 4) err = true;
+            n += nc / 2;
+            if (nc == 4) amb++;
+        }
+    }
+    return n;
 }
 
 /* Cornelius::find_surface_3d for a cube whose corner (i,j,k) spans

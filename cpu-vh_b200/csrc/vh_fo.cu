@@ -36,8 +36,9 @@ size_t freezeout_scratch_ints(int nx, int ny, int nz)
 {
     long long nc = cube_count(nx, ny, nz);
     long long nb = (nc + 1 + kScanChunk - 1) / kScanChunk + 1;
-    /* flags/offsets, list, counts/offsets, block sums, header (n_straddle, n_above, n_total) */
-    return (size_t)((nc + 1) + nc + (nc + 1) + nb + 3);
+    /* flags/offsets, list, counts/offsets, block sums, header (n_straddle,
+     * n_above, n_total) */
+    return (size_t)((nc + 1) + nc + (nc + 1) + nb + kFoHeaderInts);
 }
 
 struct FoScratch {
@@ -259,6 +260,310 @@ __global__ void __launch_bounds__(128) fo_count_kernel(const __grid_constant__ F
     }
 }
 
+/* ---------------------------------------------- count, 4D, grouped lanes
+ * The per-thread count above leaves ~4 warps per SM on a 131x131x61 event
+ * (one thread per crossed hypercube, ~17 k of them), each thread a long
+ * serial chain through the work area in local memory.  Here eight lanes take
+ * one hypercube and a 128-thread block sixteen:
+ *   cubes     lane c builds the c-th of the hypercube's eight 3-cubes
+ *             (surface_4d's order), its lines and polygons and the polygon
+ *             centroids, into a pool in shared memory; the pool is allotted
+ *             by a block-wide scan of the line and polygon counts known from
+ *             the corner comparisons (cube_line_count), so lines and polygons
+ *             keep the reference's order and indices stay in it;
+ *   hedra     one lane per hypercube assembles the polyhedra (all polygons in
+ *             one when nothing is ambiguous, the reference's search loop
+ *             otherwise);
+ *   geometry  the sums of Polyhedron::calculate_centroid/normal in rounds of
+ *             eight tetrahedra, one per lane, each term added to the running
+ *             sums in the reference's order through width-8 shuffles.
+ * Every value is computed by the same expression as in surface_4d, in the
+ * same order: the elements are bit-identical.  A block whose hypercubes need
+ * more than the pool holds takes them in rounds (one hypercube, at most 96
+ * lines, always fits): no hypercube is left to a slower path, whose serial
+ * latency alone would be that of the whole per-thread count. */
+constexpr int kG4 = 16;                     /* hypercubes per 128-thread block */
+constexpr int kPoolLines = 512, kPoolPolys = 128;
+
+struct Count4Shared {
+    double p[kPoolLines][2][4];
+    double out[kPoolLines][4];
+    unsigned char flip[kPoolLines];
+    cor::Poly poly[kPoolPolys];
+    unsigned short tl[kPoolLines];           /* tetrahedra of the polyhedron being measured: its line */
+    unsigned char tp[kPoolLines];            /*   and the polygon the line belongs to */
+    cor::Hedron hed[kG4][cor::kMaxHedra];
+    int lbase[128], pbase[128], nl[128], np[128];
+    unsigned char amb[128], err[128];
+    int nh[kG4];
+    int wsum[4];
+    int next_l, next_p;                      /* the next round's pool offsets */
+};
+
+/* the centroid and normal of polyhedron h (Polyhedron::calculate_centroid and
+ * calculate_normal, cornelius.cpp:842-987), its tetrahedra listed in
+ * S.tl/S.tp from index base; the eight lanes of gmask cooperate */
+__device__ void hedron_geometry_group(const cor::WorkRef &w, Count4Shared &S, int base, int T, int q,
+                                      unsigned gmask, double *centroid, double *normal)
+{
+    double mean[4] = {0, 0, 0, 0};
+    for (int r = 0; r < T; r += 8) {
+        const int t = r + q;
+        double s[4] = {0, 0, 0, 0};
+        if (t < T) {
+            const int l = S.tl[base + t];
+            const double *p1 = cor::lstart(w, l), *p2 = cor::lend(w, l);
+            for (int k = 0; k < 4; k++) s[k] = p1[k] + p2[k];
+        }
+        for (int u = 0; u < 8; u++) {
+            double v[4];
+            for (int k = 0; k < 4; k++) v[k] = __shfl_sync(gmask, s[k], u, 8);
+            if (r + u < T)
+                for (int k = 0; k < 4; k++) mean[k] += v[k];
+        }
+    }
+    for (int j = 0; j < 4; j++) mean[j] = mean[j] / (double)(2.0 * T);
+    double up[4] = {0, 0, 0, 0}, down = 0;
+    for (int r = 0; r < T; r += 8) {
+        const int t = r + q;
+        double s[5] = {0, 0, 0, 0, 0};
+        if (t < T) {
+            const int l = S.tl[base + t];
+            const double *cent = S.poly[S.tp[base + t]].cen;
+            const double *p1 = cor::lstart(w, l), *p2 = cor::lend(w, l);
+            double cm[4], a4[4], b4[4], c4[4], n[4];
+            for (int k = 0; k < 4; k++) cm[k] = (p1[k] + p2[k] + cent[k] + mean[k]) / 4.0;
+            for (int k = 0; k < 4; k++) { a4[k] = p1[k] - mean[k]; b4[k] = p2[k] - mean[k]; c4[k] = cent[k] - mean[k]; }
+            cor::tetravolume(a4, b4, c4, n);
+            double V = 0;
+            for (int k = 0; k < 4; k++) V += n[k] * n[k];
+            V = sqrt(V);
+            for (int k = 0; k < 4; k++) s[k] = cm[k] * V;
+            s[4] = V;
+        }
+        for (int u = 0; u < 8; u++) {
+            double v[5];
+            for (int k = 0; k < 5; k++) v[k] = __shfl_sync(gmask, s[k], u, 8);
+            if (r + u < T) {
+                for (int k = 0; k < 4; k++) up[k] += v[k];
+                down += v[4];
+            }
+        }
+    }
+    for (int i = 0; i < 4; i++) centroid[i] = up[i] / down;
+    for (int i = 0; i < 4; i++) normal[i] = 0;
+    for (int r = 0; r < T; r += 8) {
+        const int t = r + q;
+        double n[4] = {0, 0, 0, 0};
+        if (t < T) {
+            const int l = S.tl[base + t];
+            const double *cent = S.poly[S.tp[base + t]].cen;
+            const double *p1 = cor::lstart(w, l), *p2 = cor::lend(w, l);
+            double a4[4], b4[4], c4[4], vout[4];
+            for (int k = 0; k < 4; k++) { a4[k] = p1[k] - centroid[k]; b4[k] = p2[k] - centroid[k]; c4[k] = cent[k] - centroid[k]; }
+            cor::tetravolume(a4, b4, c4, n);
+            for (int k = 0; k < 4; k++) vout[k] = w.out[l][k] - centroid[k];
+            cor::orient(n, vout);
+        }
+        for (int u = 0; u < 8; u++) {
+            double v[4];
+            for (int k = 0; k < 4; k++) v[k] = __shfl_sync(gmask, n[k], u, 8);
+            if (r + u < T)
+                for (int k = 0; k < 4; k++) normal[k] += v[k];
+        }
+    }
+}
+
+__global__ void __launch_bounds__(128, 3) fo_count4_kernel(const __grid_constant__ FoArgs a, FoScratch sc)
+{
+    extern __shared__ __align__(16) unsigned char count4_smem[];
+    Count4Shared &S = *reinterpret_cast<Count4Shared *>(count4_smem);
+    const int tid = threadIdx.x, g = tid >> 3, q = tid & 7, lane = tid & 31, wid = tid >> 5;
+    const unsigned gmask = 0xFFu << (lane & ~7);
+    const int nst = sc.hdr[0];
+    /* the uncrossed entries of the counts the offsets are scanned from */
+    for (long long i = nst + (long long)blockIdx.x * 128 + tid; i < sc.nc; i += (long long)gridDim.x * 128)
+        sc.counts[i] = 0;
+    const double dx[4] = {a.dtau_c, a.dx, a.dy, a.dz};
+    const double E0 = a.eF;
+    const cor::WorkRef pool{S.p, S.out, S.flip, S.poly, 0, 0, kPoolLines, kPoolPolys, false};
+    for (long long hb = blockIdx.x; hb * kG4 < nst; hb += gridDim.x) {
+        const long long hidx = hb * kG4 + g;
+        const bool valid = hidx < nst;
+        /* this lane's 3-cube: axis ci held at cj (surface_4d's enumeration) */
+        const int ci = q >> 1, cj = q & 1;
+        double cu[2][2][2];
+        int nlc = 0, ambsq = 0, npm = 0, below = 0;
+        bool errc = false;
+        if (valid) {
+            int ix, iy, iz;
+            cube_coords(a, sc.list[hidx], ix, iy, iz);
+            for (int A = 0; A < 2; A++)
+                for (int B = 0; B < 2; B++)
+                    for (int C = 0; C < 2; C++) {
+                        const int t = (ci == 0) ? cj : A;
+                        const int bx = (ci == 0) ? A : (ci == 1) ? cj : B;
+                        const int by = (ci <= 1) ? B : (ci == 2) ? cj : C;
+                        const int bz = (ci <= 2) ? C : cj;
+                        cu[A][B][C] = slab(a, t, 0, ix + bx, iy + by, iz + bz);
+                        if (cu[A][B][C] < E0) below++;
+                    }
+            nlc = cor::cube_line_count(cu, ci, E0, ambsq, errc);
+            if (nlc > 0) {
+                const bool ambc = ambsq > 0 || nlc == 6;     /* cube_polygons' ambiguity */
+                npm = ambc ? (nlc > 3 ? nlc - 2 : 1) : 1;    /* the most polygons it can make */
+            }
+        }
+        /* block-wide exclusive scan of the line and polygon counts, in lane
+         * order (hypercube order, then surface_4d's cube order) */
+        const int packed = nlc | (npm << 16);
+        int incl = packed;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (lane == 31) S.wsum[wid] = incl;
+        __syncthreads();
+        int before = 0;
+        for (int k = 0; k < wid; k++) before += S.wsum[k];
+        const int excl = before + incl - packed;
+        const int lb = excl & 0xffff, pb = excl >> 16;
+        /* the group's range: from its first cube's start to its last cube's end */
+        const int g_lbeg = __shfl_sync(0xffffffffu, lb, lane & ~7);
+        const int g_pbeg = __shfl_sync(0xffffffffu, pb, lane & ~7);
+        const int g_lend = __shfl_sync(0xffffffffu, lb + nlc, (lane & ~7) + 7);
+        const int g_pend = __shfl_sync(0xffffffffu, pb + npm, (lane & ~7) + 7);
+        /* rounds: each takes the next run of groups whose ranges fit the pool
+         * from offset (off_l, off_p); one hypercube (at most 96 lines and 80
+         * polygons reserved) always fits alone, so every round advances */
+        int off_l = 0, off_p = 0;
+        bool done = !valid;
+        for (;;) {
+            const bool mine = !done && g_lend - off_l <= kPoolLines && g_pend - off_p <= kPoolPolys;
+            if (tid == 0) { S.next_l = 1 << 30; S.next_p = 1 << 30; }
+            /* cubes: lines, polygons, polygon centroids */
+            int npc = 0;
+            bool ambb = false, errb = errc;
+            const int rl = lb - off_l, rp = pb - off_p;
+            if (mine && nlc > 0 && !errc) {
+                cor::WorkRef w{S.p, S.out, S.flip, S.poly, rl, rp, rl + nlc, rp + npm, false};
+                const int n = cor::cube_polygons(w, cu, ci, cj * dx[ci], E0, dx, &ambb);
+                if (w.error || n != nlc || w.nl != rl + nlc) errb = true;
+                else {
+                    npc = w.np - rp;
+                    for (int k = rp; k < w.np; k++) cor::poly_centroid(w, S.poly[k]);
+                }
+            }
+            S.lbase[tid] = rl;
+            S.pbase[tid] = rp;
+            S.nl[tid] = nlc;
+            S.np[tid] = npc;
+            S.amb[tid] = (nlc > 0 && ambb) ? 1 : 0;
+            S.err[tid] = errb ? 1 : 0;
+            __syncthreads();
+            if (mine) {
+                const int g0 = g * 8;
+                int gnl = 0, gnp = 0, gamb = 0;
+                bool gerr = false;
+                for (int c = 0; c < 8; c++) {
+                    gnl += S.nl[g0 + c];
+                    gnp += S.np[g0 + c];
+                    gamb += S.amb[g0 + c];
+                    gerr |= S.err[g0 + c] != 0;
+                }
+                if (gnp > cor::kMaxPoly) gerr = true;             /* the per-thread work area's polygon cap */
+                /* surface_4d: 24 lines and 2 (or 14) corners below make it ambiguous */
+                int points = __shfl_sync(gmask, below, 0, 8) + __shfl_sync(gmask, below, 1, 8);
+                if (points > 8) points = 16 - points;
+                const bool ambiguous = gamb > 0 || (gnl == 24 && points == 2);
+                if (q == 0) {
+                    int nh = 0;
+                    if (!gerr) {
+                        cor::WorkRef w = pool;
+                        unsigned char list[cor::kMaxPoly];
+                        int npolys = 0;
+                        for (int c = 0; c < 8; c++)
+                            for (int k = 0; k < S.np[g0 + c]; k++) list[npolys++] = (unsigned char)(S.pbase[g0 + c] + k);
+                        cor::Hedron *hed = S.hed[g];
+                        if (ambiguous) {
+                            bool not_used[cor::kMaxPoly];
+                            int used = 0;
+                            for (int i = 0; i < npolys; i++) not_used[i] = true;
+                            do {
+                                if (nh >= cor::kMaxHedra) { w.error = true; break; }
+                                hed[nh].npoly = 0; hed[nh].ntet = 0;
+                                for (int i = 0; i < npolys; i++)
+                                    if (not_used[i] && cor::hedron_add(w, hed[nh], list[i], false)) { not_used[i] = false; used++; i = 0; }
+                                if (w.error) break;
+                                nh++;
+                            } while (used < npolys);
+                        } else {
+                            hed[0].npoly = 0; hed[0].ntet = 0;
+                            for (int i = 0; i < npolys; i++) cor::hedron_add(w, hed[0], list[i], true);
+                            nh = 1;
+                        }
+                        if (w.error) nh = -1;
+                    } else {
+                        nh = -1;
+                    }
+                    S.nh[g] = nh;
+                }
+                __syncwarp(gmask);
+                const int nh = S.nh[g];
+                const int base = S.lbase[g0];
+                for (int hh = 0; hh < nh; hh++) {
+                    const cor::Hedron &h = S.hed[g][hh];
+                    if (q == 0) {
+                        int t = 0;
+                        for (int i = 0; i < h.npoly; i++) {
+                            const cor::Poly &pg = S.poly[h.poly[i]];
+                            for (int j = 0; j < pg.nlines; j++) { S.tl[base + t] = pg.line[j]; S.tp[base + t] = h.poly[i]; t++; }
+                        }
+                    }
+                    __syncwarp(gmask);
+                    double cen[4], nor[4];
+                    hedron_geometry_group(pool, S, base, h.ntet, q, gmask, cen, nor);
+                    if (q == 0 && hidx < a.slot_cap) {
+                        double *o = a.slots + hidx * kSlotDoubles + 8 * hh;
+                        for (int d = 0; d < 4; d++) { o[d] = cen[d]; o[4 + d] = nor[d]; }
+                    }
+                    __syncwarp(gmask);
+                }
+                if (q == 0) {
+                    int ne = nh;
+                    if (ne < 0) { raise_error(a.err, 5, sc.list[hidx], a.n); ne = 0; }
+                    sc.counts[hidx] = ne;
+                }
+                done = true;
+            } else if (!done && q == 0) {
+                atomicMin(&S.next_l, g_lbeg);
+                atomicMin(&S.next_p, g_pbeg);
+            }
+            __syncthreads();
+            if (S.next_l == (1 << 30)) break;                    /* every group of the block is done */
+            off_l = S.next_l;
+            off_p = S.next_p;
+            __syncthreads();                                     /* next_l / next_p are reset next round */
+        }
+    }
+}
+
+static void launch_count4(const FoArgs &a, FoScratch sc, cudaStream_t st)
+{
+    static int blocks = [] {
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaFuncSetAttribute(fo_count4_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Count4Shared));
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fo_count4_kernel, 128, sizeof(Count4Shared));
+        return sms * (per_sm > 0 ? per_sm : 1);
+    }();
+    const long long need = (sc.nc + kG4 - 1) / kG4;
+    const unsigned grid = (unsigned)(need < blocks ? (need > 0 ? need : 1) : blocks);
+    fo_count4_kernel<<<grid, 128, sizeof(Count4Shared), st>>>(a, sc);
+}
+
 /* FreezeOut.cpp:40-55 */
 __device__ __forceinline__ double interp3(double x0, double x1, double x2, double a000, double a100, double a010,
                                           double a001, double a110, double a101, double a011, double a111)
@@ -362,7 +667,7 @@ void launch_freezeout(const FoArgs &a, cudaStream_t st)
 {
     FoScratch sc = carve(a);
     const long long N = (long long)a.nx * a.ny * a.nz;
-    cudaMemsetAsync(sc.hdr, 0, 3 * sizeof(int), st);
+    cudaMemsetAsync(sc.hdr, 0, kFoHeaderInts * sizeof(int), st);
     fo_gather_kernel<<<(unsigned)((N + 255) / 256), 256, 0, st>>>(a, sc.hdr + 1);
     const unsigned gc = (unsigned)((sc.nc + 255) / 256);
     fo_classify_kernel<<<gc, 256, 0, st>>>(a, sc);
@@ -370,7 +675,8 @@ void launch_freezeout(const FoArgs &a, cudaStream_t st)
     fo_compact_kernel<<<gc, 256, 0, st>>>(sc);
     fo_header_kernel<<<1, 1, 0, st>>>(sc);
     const unsigned gk = (unsigned)((sc.nc + 127) / 128);
-    fo_count_kernel<<<gk, 128, 0, st>>>(a, sc);
+    if (a.nz > 1) launch_count4(a, sc, st);
+    else fo_count_kernel<<<gk, 128, 0, st>>>(a, sc);
     exclusive_scan(sc.counts, sc.nc, sc.bsum, sc.hdr + 2, st);
     launch_freezeout_emit(a, st);
 }

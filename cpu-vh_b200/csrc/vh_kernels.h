@@ -140,6 +140,9 @@ struct FoArgs {
 /* doubles of one crossed cube's element slot: up to 10 elements (Cornelius
  * MAX_ELEMENTS), centroid and normal (4 + 4) each */
 constexpr int kFoSlotDoubles = 80;
+/* the freezeout scratch ends with its header: crossed cubes, cells above
+ * e_F, elements */
+constexpr int kFoHeaderInts = 3;
 
 /* Runs the whole freezeout block; returns the number of elements through
  * *a.n_total (device) and leaves elements in a.elems. */
