@@ -106,12 +106,18 @@ __device__ __forceinline__ double slab(const FoArgs &a, int which, int v, int ix
 }
 
 /* ----------------------------------------------------------- classify */
+/* threads run over the cubes in the slab's memory order (x fastest, so a
+ * warp's corner loads are contiguous); each flag goes to the cube's index
+ * in the reference's order (cube_coords) */
 __global__ void fo_classify_kernel(const __grid_constant__ FoArgs a, FoScratch sc)
 {
-    const long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (c >= sc.nc) return;
-    int ix, iy, iz;
-    cube_coords(a, c, ix, iy, iz);
+    const long long m = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (m >= sc.nc) return;
+    const int mz = a.nz > 1 ? a.nz - 1 : 1;
+    const int ix = (int)(m % (a.nx - 1));
+    const int iy = (int)((m / (a.nx - 1)) % (a.ny - 1));
+    const int iz = (int)(m / ((long long)(a.nx - 1) * (a.ny - 1)));
+    const long long c = iz + (long long)mz * (iy + (long long)(a.ny - 1) * ix);
     const bool four = a.nz > 1;
     int above = 0;
     for (int t = 0; t < 2; t++)
