@@ -112,6 +112,36 @@ BatchKernel batch_kernel(int nq, int eos_kind, int phase, bool st2, int zm, bool
     return mixed ? batch_kernel_mixed(nq, eos_kind, phase, st2, zm) : batch_kernel_of<false>(nq, eos_kind, phase, st2, zm);
 }
 
+template <int NQ, int EOS>
+static BatchKernel batch_lines_t(int dir)
+{
+    return dir == 1 ? kt_batch_lines_kernel<NQ, EOS, 1> : dir == 2 ? kt_batch_lines_kernel<NQ, EOS, 2>
+                                                              : kt_batch_lines_kernel<NQ, EOS, 3>;
+}
+
+BatchKernel batch_lines_kernel(int nq, int eos_kind, int dir)
+{
+    if (nq == 15) return eos_kind == 1 ? batch_lines_t<15, 1>(dir) : batch_lines_t<15, 0>(dir);
+    return eos_kind == 1 ? batch_lines_t<14, 1>(dir) : batch_lines_t<14, 0>(dir);
+}
+
+size_t batch_lines_smem(int nq, int dir, int nd)
+{
+    const int plane = dir == 1 ? FluxLines<1>::plane(nd) : dir == 2 ? FluxLines<2>::plane(nd) : FluxLines<3>::plane(nd);
+    return sizeof(double) * 2 * (size_t)nq * plane;
+}
+
+int batch_lines_per_block(int dir) { return dir == 1 ? FluxLines<1>::PB : dir == 2 ? FluxLines<2>::PB : FluxLines<3>::PB; }
+
+long long batch_line_blocks(int dir, int nx, int ny, int nz)
+{
+    const int nd = dir == 1 ? nx : dir == 2 ? ny : nz;
+    const long long bund = dir == 1 ? FluxLines<1>::bundles(nx, ny, nz) : dir == 2 ? FluxLines<2>::bundles(nx, ny, nz)
+                                                                        : FluxLines<3>::bundles(nx, ny, nz);
+    const int pb = batch_lines_per_block(dir);
+    return ((long long)nd * bund + pb - 1) / pb;
+}
+
 /* resident 128-thread blocks per SM of a batch kernel (persistent grid size) */
 static int resident_blocks(BatchKernel k)
 {
@@ -167,6 +197,9 @@ struct vh_batch {
     std::map<int, Tiles> tiles;      /* key: tile_x */
     int4 *ftiles[3] = {};            /* mixed precision: face tiles per axis */
     int n_ftiles[3] = {};
+    int4 *ltiles[3] = {};            /* FP64: line blocks (member, block) per axis */
+    int n_ltiles[3] = {};
+    size_t lsmem[3] = {};            /* their dynamic shared memory */
     bool tuned = false;
     vh_batch_tuning tune{};
     cudaGraph_t graph = nullptr;
@@ -241,6 +274,45 @@ int build_face_tiles(vh_batch *b)
         if (f[d].empty()) continue;
         BTRY(cudaMalloc(&b->ftiles[d], f[d].size() * sizeof(int4)));
         BTRY(cudaMemcpy(b->ftiles[d], f[d].data(), f[d].size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
+    return VH_OK;
+}
+
+/* FP64 batches run their flux over line pieces (the single-event form);
+ * VH_BATCH_LINES=0 keeps the per-cell flux of kt_batch_kernel */
+bool batch_lines_on()
+{
+    static int on = [] {
+        const char *e = getenv("VH_BATCH_LINES");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return on == 1;
+}
+
+/* FP64: the line blocks of kt_batch_lines_kernel per axis, every member's
+ * blocks in member order (eta: the 3+1D members) */
+int build_line_tiles(vh_batch *b)
+{
+    std::vector<int4> f[3];
+    for (size_t m = 0; m < b->mem.size(); ++m) {
+        const vh_config &c = b->mem[m]->cfg;
+        for (int d = 1; d <= (c.nz > 1 ? 3 : 2); ++d) {
+            const long long nb = vh::batch_line_blocks(d, c.nx, c.ny, c.nz);
+            for (long long k = 0; k < nb; ++k) f[d - 1].push_back(make_int4((int)m, (int)k, 0, 0));
+            const int nd = d == 1 ? c.nx : d == 2 ? c.ny : c.nz;
+            b->lsmem[d - 1] = std::max(b->lsmem[d - 1], vh::batch_lines_smem(b->nq, d, nd));
+        }
+    }
+    for (int d = 0; d < 3; ++d) {
+        b->n_ltiles[d] = (int)f[d].size();
+        if (f[d].empty()) continue;
+        BTRY(cudaMalloc(&b->ltiles[d], f[d].size() * sizeof(int4)));
+        BTRY(cudaMemcpy(b->ltiles[d], f[d].data(), f[d].size() * sizeof(int4), cudaMemcpyHostToDevice));
+        vh::BatchKernel k = vh::batch_lines_kernel(b->nq, b->eos_kind, d + 1);
+        BTRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b->lsmem[d]));
+        /* shared memory for 5 resident blocks, the rest to L1 (the EoS table) */
+        const int pct = (int)((5 * (b->lsmem[d] + sizeof(vh::StageArgs) + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
+        BTRY(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, std::min(pct, 100)));
     }
     return VH_OK;
 }
@@ -323,6 +395,18 @@ void launch_phase(vh_batch *b, int stage, int phase, int tx, int persistent)
     k<<<grid, block, 0, b->stream>>>(B);
 }
 
+/* FP64: one axis of the flux over the line blocks */
+void launch_lines(vh_batch *b, int stage, int dir)
+{
+    vh::BatchLaunch B;
+    B.args = b->d_args + (size_t)stage * b->mem.size();
+    B.tiles = b->ltiles[dir - 1];
+    B.ntiles = b->n_ltiles[dir - 1];
+    if (B.ntiles == 0) return;
+    vh::BatchKernel k = vh::batch_lines_kernel(b->nq, b->eos_kind, dir);
+    k<<<B.ntiles, 128, b->lsmem[dir - 1], b->stream>>>(B);
+}
+
 /* mixed precision: one axis of the face-once flux over the face tiles */
 void launch_face(vh_batch *b, int stage, int dir)
 {
@@ -341,8 +425,9 @@ void launch_stage(vh_batch *b, int stage, const vh_batch_tuning &t, vh::StageMar
     auto run = [&](int phase) {
         /* the split stage's flux is face-once in mixed precision, as on
          * single events (the tile shape of these phases is then unused) */
-        const bool face = b->mixed && phase >= VH_PHASE_FLUX_X && phase <= VH_PHASE_FLUX_ETA;
-        if (face) launch_face(b, stage, phase - VH_PHASE_FLUX_X + 1);
+        const bool flux = phase >= VH_PHASE_FLUX_X && phase <= VH_PHASE_FLUX_ETA;
+        if (flux && b->mixed) launch_face(b, stage, phase - VH_PHASE_FLUX_X + 1);
+        else if (flux && batch_lines_on()) launch_lines(b, stage, phase - VH_PHASE_FLUX_X + 1);
         else launch_phase(b, stage, phase, t.tile_x[phase], t.persistent[phase]);
         if (m) { m->phase[m->n] = phase; cudaEventRecord(m->ev[++m->n], b->stream); }
     };
@@ -498,6 +583,8 @@ int preload(vh_batch *b)
         }
     if (b->mixed)
         for (int d = 1; d <= 3; ++d) BTRY(cudaFuncGetAttributes(&attr, vh::batch_face_kernel_mixed(b->nq, b->eos_kind, d)));
+    else
+        for (int d = 1; d <= 3; ++d) BTRY(cudaFuncGetAttributes(&attr, vh::batch_lines_kernel(b->nq, b->eos_kind, d)));
     return VH_OK;
 }
 
@@ -593,6 +680,7 @@ int vh_batch_create(vh_event *const *events, int n_events, vh_batch **out)
 #undef CTRY
     rc = ensure_times(b, 1024);
     if (rc == VH_OK && b->mixed) rc = build_face_tiles(b);
+    if (rc == VH_OK && !b->mixed) rc = build_line_tiles(b);
     if (rc != VH_OK) { vh_batch_destroy(b); return rc; }
     *out = b;
     return VH_OK;
@@ -605,6 +693,7 @@ int vh_batch_destroy(vh_batch *b)
     drop_graph(b);
     for (auto &kv : b->tiles) { cudaFree(kv.second.all); cudaFree(kv.second.z); }
     for (int4 *f : b->ftiles) cudaFree(f);
+    for (int4 *f : b->ltiles) cudaFree(f);
     for (auto &T : b->ttabs) cudaFree(T.d);
     for (auto &m : b->marks)
         for (cudaEvent_t e : m.ev) cudaEventDestroy(e);

@@ -84,6 +84,32 @@ __global__ void __launch_bounds__(kBatchFaceTX * kBatchFaceTY, 2) kt_batch_face_
     }
 }
 
+/* FP64: the flux along DIR over line pieces of every member, one block per
+ * table entry (member, block index among its line blocks) -- the body of the
+ * single-event kt_flux_lines_kernel, so a member's fluxes equal its
+ * single-event ones.  Dynamic shared memory: 2 * NQ * FluxLines::plane(nd)
+ * doubles for the member with the most. */
+template <int NQ, int EOS, int DIR>
+__global__ void __launch_bounds__(128, 5) kt_batch_lines_kernel(const __grid_constant__ BatchLaunch B)
+{
+    __shared__ __align__(16) StageArgs sA;
+    extern __shared__ double smd[];
+    int cur = -1;
+    for (int t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
+        const int4 tile = __ldg(B.tiles + t);
+        __syncthreads();               /* the previous entry's staged values are read to its end */
+        if (tile.x != cur) {           /* uniform over the block */
+            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(B.args + tile.x);
+            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sA);
+            for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / 8); w += blockDim.x) dst[w] = src[w];
+            __syncthreads();
+            cur = tile.x;
+        }
+        if (sA.nx == 0) continue;      /* an inactive member (uniform over the block) */
+        flux_lines_block<NQ, EOS, DIR, 3, false>(sA, smd, tile.y);
+    }
+}
+
 template <int NQ, int EOS, int PHASE, bool MIXED>
 static BatchKernel batch_kernel_z(bool st2, int zm)
 {

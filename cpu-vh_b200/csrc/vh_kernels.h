@@ -110,6 +110,13 @@ BatchKernel batch_kernel_mixed(int nq, int eos_kind, int phase, bool st2, int zm
 /* mixed precision: the face-once flux along dir (1-3) over face tiles of
  * 32 x 8 faces (block 32 x 8) */
 BatchKernel batch_face_kernel_mixed(int nq, int eos_kind, int dir);
+/* FP64: the flux along dir (1-3) over line blocks (member, block); 128
+ * threads, dynamic shared memory batch_lines_smem(nq, dir, nd) bytes for
+ * the smallest extent nd along dir among the members */
+BatchKernel batch_lines_kernel(int nq, int eos_kind, int dir);
+size_t batch_lines_smem(int nq, int dir, int nd);
+int batch_lines_per_block(int dir);
+long long batch_line_blocks(int dir, int nx, int ny, int nz);
 
 /* ---- freezeout ---- */
 struct FoArgs {

@@ -432,8 +432,9 @@ struct FluxLines {
     }
 };
 
+/* blk: the block's index among the event's line blocks (runs blk * PB on) */
 template <int NQ, int EOS, int DIR, int UNR = 1, bool PDL = false>
-__device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__restrict__ sm)
+__device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__restrict__ sm, long long blk)
 {
     /* with PDL, only the update of the accumulator (written by the previous
      * phase) waits for the previous kernel; the staged stencil, e and u are
@@ -449,7 +450,7 @@ __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__r
     const int nxq = (A.nx + W - 1) / W;
     const long long nbund = G::bundles(A.nx, A.ny, A.nz);
     const long long Rtot = (long long)nd * nbund;
-    const long long R0 = (long long)blockIdx.x * PB;
+    const long long R0 = blk * PB;
     const long long b0 = R0 / nd;
     const int p0 = (int)(R0 - b0 * nd);
     const int tid = threadIdx.x;
@@ -789,6 +790,7 @@ __device__ __forceinline__ void source_body(const StageArgs &A, long long s)
 template <int NQ, int EOS, int DIR>
 __device__ __forceinline__ void flux_body(const StageArgs &A, long long s)
 {
+    prefetch_flux_cell<NQ>(A, s, DIR);
     const double ePrev = __ldg(A.ein + s);
     bool bad = false;
     const long long st = (DIR == 1) ? 1 : (DIR == 2) ? (long long)A.ncx : (long long)A.ncx * A.ncy;

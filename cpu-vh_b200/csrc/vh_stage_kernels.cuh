@@ -182,7 +182,7 @@ template <int NQ, int EOS, int DIR, int MB, int UNR>
 __global__ void __launch_bounds__(128, MB) kt_flux_lines_kernel(const __grid_constant__ StageArgs A)
 {
     extern __shared__ double smd[];
-    flux_lines_block<NQ, EOS, DIR, UNR, true>(A, smd);
+    flux_lines_block<NQ, EOS, DIR, UNR, true>(A, smd, blockIdx.x);
 }
 
 template <int NQ, int EOS, int DIR, int MB, int UNR = 1>
