@@ -142,6 +142,14 @@ long long batch_line_blocks(int dir, int nx, int ny, int nz)
     return ((long long)nd * bund + pb - 1) / pb;
 }
 
+long long batch_face_line_blocks(int dir, int nx, int ny, int nz)
+{
+    const int nd = dir == 2 ? ny : nz;
+    const long long bund = dir == 2 ? FluxLines<2>::bundles(nx, ny, nz) : FluxLines<3>::bundles(nx, ny, nz);
+    const int pb = dir == 2 ? FluxLines<2>::PB : FluxLines<3>::PB;
+    return ((long long)(nd + 1) * bund + pb - 2) / (pb - 1);
+}
+
 /* resident 128-thread blocks per SM of a batch kernel (persistent grid size) */
 static int resident_blocks(BatchKernel k)
 {
@@ -197,6 +205,8 @@ struct vh_batch {
     std::map<int, Tiles> tiles;      /* key: tile_x */
     int4 *ftiles[3] = {};            /* mixed precision: face tiles per axis */
     int n_ftiles[3] = {};
+    int4 *fltiles[3] = {};           /* mixed precision: face line blocks along y, eta */
+    int n_fltiles[3] = {};
     int4 *ltiles[3] = {};            /* FP64: line blocks (member, block) per axis */
     int n_ltiles[3] = {};
     size_t lsmem[3] = {};            /* their dynamic shared memory */
@@ -275,7 +285,33 @@ int build_face_tiles(vh_batch *b)
         BTRY(cudaMalloc(&b->ftiles[d], f[d].size() * sizeof(int4)));
         BTRY(cudaMemcpy(b->ftiles[d], f[d].data(), f[d].size() * sizeof(int4), cudaMemcpyHostToDevice));
     }
+    /* face line blocks along y and eta (the 3+1D members) */
+    std::vector<int4> fl[3];
+    for (size_t m = 0; m < b->mem.size(); ++m) {
+        const vh_config &c = b->mem[m]->cfg;
+        for (int d = 2; d <= (c.nz > 1 ? 3 : 2); ++d) {
+            const long long nb = vh::batch_face_line_blocks(d, c.nx, c.ny, c.nz);
+            for (long long k = 0; k < nb; ++k) fl[d - 1].push_back(make_int4((int)m, (int)k, 0, 0));
+        }
+    }
+    for (int d = 1; d < 3; ++d) {
+        b->n_fltiles[d] = (int)fl[d].size();
+        if (fl[d].empty()) continue;
+        BTRY(cudaMalloc(&b->fltiles[d], fl[d].size() * sizeof(int4)));
+        BTRY(cudaMemcpy(b->fltiles[d], fl[d].data(), fl[d].size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
     return VH_OK;
+}
+
+/* mixed batches run their y and eta flux over face line pieces (the
+ * single-event form); VH_BATCH_FACE_LINES=0 keeps the 32 x 8 face tiles */
+bool batch_face_lines_on()
+{
+    static int on = [] {
+        const char *e = getenv("VH_BATCH_FACE_LINES");
+        return (e && e[0] == '0') ? 0 : 1;
+    }();
+    return on == 1;
 }
 
 /* FP64 batches run their flux over line pieces (the single-event form);
@@ -412,6 +448,14 @@ void launch_face(vh_batch *b, int stage, int dir)
 {
     vh::BatchLaunch B;
     B.args = b->d_args + (size_t)stage * b->mem.size();
+    if (dir >= 2 && batch_face_lines_on()) {
+        B.tiles = b->fltiles[dir - 1];
+        B.ntiles = b->n_fltiles[dir - 1];
+        if (B.ntiles == 0) return;
+        vh::BatchKernel k = vh::batch_face_lines_kernel_mixed(b->nq, b->eos_kind, dir);
+        k<<<B.ntiles, 128, 0, b->stream>>>(B);
+        return;
+    }
     B.tiles = b->ftiles[dir - 1];
     B.ntiles = b->n_ftiles[dir - 1];
     if (B.ntiles == 0) return;
@@ -581,8 +625,10 @@ int preload(vh_batch *b)
             BTRY(cudaFuncGetAttributes(&attr, k));
             vh::resident_blocks(k);
         }
-    if (b->mixed)
+    if (b->mixed) {
         for (int d = 1; d <= 3; ++d) BTRY(cudaFuncGetAttributes(&attr, vh::batch_face_kernel_mixed(b->nq, b->eos_kind, d)));
+        for (int d = 2; d <= 3; ++d) BTRY(cudaFuncGetAttributes(&attr, vh::batch_face_lines_kernel_mixed(b->nq, b->eos_kind, d)));
+    }
     else
         for (int d = 1; d <= 3; ++d) BTRY(cudaFuncGetAttributes(&attr, vh::batch_lines_kernel(b->nq, b->eos_kind, d)));
     return VH_OK;
@@ -694,6 +740,7 @@ int vh_batch_destroy(vh_batch *b)
     for (auto &kv : b->tiles) { cudaFree(kv.second.all); cudaFree(kv.second.z); }
     for (int4 *f : b->ftiles) cudaFree(f);
     for (int4 *f : b->ltiles) cudaFree(f);
+    for (int4 *f : b->fltiles) cudaFree(f);
     for (auto &T : b->ttabs) cudaFree(T.d);
     for (auto &m : b->marks)
         for (cudaEvent_t e : m.ev) cudaEventDestroy(e);

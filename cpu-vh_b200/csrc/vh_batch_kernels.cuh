@@ -110,6 +110,31 @@ __global__ void __launch_bounds__(128, 5) kt_batch_lines_kernel(const __grid_con
     }
 }
 
+/* Mixed precision along y and eta: the face-once flux over line pieces of
+ * every member, one block per entry (member, block index among its face
+ * blocks) -- flux_faces_lines, as the single-event
+ * kt_flux_face_lines_kernel runs it. */
+template <int NQ, int EOS, int DIR>
+__global__ void __launch_bounds__(128, 5) kt_batch_face_lines_kernel(const __grid_constant__ BatchLaunch B)
+{
+    __shared__ __align__(16) StageArgs sA;
+    __shared__ double sm[NQ * 128];
+    int cur = -1;
+    for (int t = blockIdx.x; t < B.ntiles; t += gridDim.x) {
+        const int4 tile = __ldg(B.tiles + t);
+        __syncthreads();               /* the previous entry's faces are read to its end */
+        if (tile.x != cur) {           /* uniform over the block */
+            const unsigned long long *src = reinterpret_cast<const unsigned long long *>(B.args + tile.x);
+            unsigned long long *dst = reinterpret_cast<unsigned long long *>(&sA);
+            for (int w = threadIdx.x; w < (int)(sizeof(StageArgs) / 8); w += blockDim.x) dst[w] = src[w];
+            __syncthreads();
+            cur = tile.x;
+        }
+        if (sA.nx == 0) continue;      /* an inactive member (uniform over the block) */
+        flux_faces_lines<NQ, EOS, DIR, false>(sA, sm, tile.y);
+    }
+}
+
 template <int NQ, int EOS, int PHASE, bool MIXED>
 static BatchKernel batch_kernel_z(bool st2, int zm)
 {

@@ -117,6 +117,10 @@ BatchKernel batch_lines_kernel(int nq, int eos_kind, int dir);
 size_t batch_lines_smem(int nq, int dir, int nd);
 int batch_lines_per_block(int dir);
 long long batch_line_blocks(int dir, int nx, int ny, int nz);
+/* mixed precision along y or eta (dir 2, 3): the face-once flux over face
+ * line blocks (member, block), 128 threads; the blocks of one member */
+BatchKernel batch_face_lines_kernel_mixed(int nq, int eos_kind, int dir);
+long long batch_face_line_blocks(int dir, int nx, int ny, int nz);
 
 /* ---- freezeout ---- */
 struct FoArgs {

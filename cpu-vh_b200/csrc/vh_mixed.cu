@@ -46,4 +46,16 @@ BatchKernel batch_face_kernel_mixed(int nq, int eos_kind, int dir)
     return eos_kind == 1 ? batch_face_t<14, 1>(dir) : batch_face_t<14, 0>(dir);
 }
 
+template <int NQ, int EOS>
+static BatchKernel batch_face_lines_t(int dir)
+{
+    return dir == 3 ? kt_batch_face_lines_kernel<NQ, EOS, 3> : kt_batch_face_lines_kernel<NQ, EOS, 2>;
+}
+
+BatchKernel batch_face_lines_kernel_mixed(int nq, int eos_kind, int dir)
+{
+    if (nq == 15) return eos_kind == 1 ? batch_face_lines_t<15, 1>(dir) : batch_face_lines_t<15, 0>(dir);
+    return eos_kind == 1 ? batch_face_lines_t<14, 1>(dir) : batch_face_lines_t<14, 0>(dir);
+}
+
 } // namespace vh

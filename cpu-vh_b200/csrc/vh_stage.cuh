@@ -1121,7 +1121,7 @@ __device__ __forceinline__ void flux_faces_tile(const StageArgs &A, int i0, int 
  * across the root solve's e <= 0.1 branch are those of flux_faces_tile, so
  * a cell's update is the same.  sm: NQ * 128 doubles. */
 template <int NQ, int EOS, int DIR, bool PDL = false>
-__device__ __forceinline__ void flux_faces_lines(const StageArgs &A, double *__restrict__ sm)
+__device__ __forceinline__ void flux_faces_lines(const StageArgs &A, double *__restrict__ sm, long long blk)
 {
     if (PDL) pdl_trigger();   /* see flux_lines_block */
     using G = FluxLines<DIR>;
@@ -1133,7 +1133,7 @@ __device__ __forceinline__ void flux_faces_lines(const StageArgs &A, double *__r
     const int nxq = (A.nx + W - 1) / W;
     const long long Rtot = (long long)nf * G::bundles(A.nx, A.ny, A.nz);
     const int tid = threadIdx.x, w = tid % W, pr = tid / W;
-    const long long R = (long long)blockIdx.x * (PB - 1) + pr;
+    const long long R = blk * (PB - 1) + pr;
     bool face_ok = R < Rtot;
     int f = 0;
     long long s = 0;

@@ -261,7 +261,7 @@ template <int NQ, int EOS, int DIR, int MB>
 __global__ void __launch_bounds__(128, MB) kt_flux_face_lines_kernel(const __grid_constant__ StageArgs A)
 {
     __shared__ double sm[NQ * 128];
-    flux_faces_lines<NQ, EOS, DIR, true>(A, sm);
+    flux_faces_lines<NQ, EOS, DIR, true>(A, sm, blockIdx.x);
 }
 
 template <int NQ, int EOS, int DIR, int MB>
