@@ -145,8 +145,8 @@ long long batch_line_blocks(int dir, int nx, int ny, int nz)
 long long batch_face_line_blocks(int dir, int nx, int ny, int nz)
 {
     const int nd = dir == 2 ? ny : nz;
-    const long long bund = dir == 2 ? FluxLines<2>::bundles(nx, ny, nz) : FluxLines<3>::bundles(nx, ny, nz);
-    const int pb = dir == 2 ? FluxLines<2>::PB : FluxLines<3>::PB;
+    const long long bund = dir == 2 ? FaceLinesG<2>::bundles(nx, ny, nz) : FaceLinesG<3>::bundles(nx, ny, nz);
+    const int pb = dir == 2 ? FaceLinesG<2>::PB : FaceLinesG<3>::PB;
     return ((long long)(nd + 1) * bund + pb - 2) / (pb - 1);
 }
 

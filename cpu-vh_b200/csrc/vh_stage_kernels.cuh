@@ -199,6 +199,7 @@ static void launch_flux_lines(const StageArgs &a, cudaStream_t s)
          * of 228 KB, and the rest of the SM's 256 KB left to L1, which holds
          * the EoS table of the root solves; VH_CARVEOUT overrides (percent) */
         int pct = (int)((MB * (bytes + 1024) * 100 + 228 * 1024 - 1) / (228 * 1024));
+        if (pct > 100) pct = 100;
         if (const char *e = getenv("VH_CARVEOUT")) pct = atoi(e);
         cudaFuncSetAttribute(kt_flux_lines_kernel<NQ, EOS, DIR, MB, UNR>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              pct);
@@ -267,7 +268,7 @@ __global__ void __launch_bounds__(128, MB) kt_flux_face_lines_kernel(const __gri
 template <int NQ, int EOS, int DIR, int MB>
 static void launch_flux_face_lines(const StageArgs &a, cudaStream_t s)
 {
-    using G = FluxLines<DIR>;
+    using G = FaceLinesG<DIR>;
     const int nd = (DIR == 1) ? a.nx : (DIR == 2) ? a.ny : a.nz;
     const long long faces = (long long)(nd + 1) * G::bundles(a.nx, a.ny, a.nz);
     const unsigned blocks = (unsigned)((faces + G::PB - 2) / (G::PB - 1));
