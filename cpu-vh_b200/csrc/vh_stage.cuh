@@ -456,20 +456,23 @@ __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__r
     const int nxq = (A.nx + W - 1) / W;
     const long long nbund = G::bundles(A.nx, A.ny, A.nz);
     const long long Rtot = (long long)nd * nbund;
+    /* line and bundle indices in 32-bit arithmetic: an event's cell count
+     * is far below 2^31 (its 61 FP64 planes alone would need 1 TB) */
+    const unsigned und = (unsigned)nd;
     const long long R0 = blk * PB;
-    const long long b0 = R0 / nd;
-    const int p0 = (int)(R0 - b0 * nd);
+    const long long b0 = (unsigned)R0 / und;
+    const int p0 = (int)((unsigned)R0 - (unsigned)b0 * und);
     const int tid = threadIdx.x;
     /* padded address of bundle b's column w at position -2 along DIR, or -1
      * if that column is outside the lattice */
     auto base = [&](long long b, int w) -> long long {
         if (DIR == 1) {
-            const long long nyq = (A.ny + W - 1) / W, jq = b % nyq, k = b / nyq;
+            const unsigned nyq = (unsigned)(A.ny + W - 1) / W, k = (unsigned)b / nyq, jq = (unsigned)b - k * nyq;
             const int y = (int)jq * W + w;
             if (y >= A.ny) return -1;
             return A.ncx * (y + 2) + sxy * (k + 2);
         }
-        const long long xq = b % nxq, o = b / nxq;
+        const unsigned o = (unsigned)b / (unsigned)nxq, xq = (unsigned)b - o * (unsigned)nxq;
         const int x = (int)xq * W + w;
         if (x >= A.nx) return -1;
         return (DIR == 2) ? (x + 2) + sxy * (o + 2) : (x + 2) + A.ncx * (o + 2);
@@ -480,8 +483,8 @@ __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__r
     long long b = 0, bb = -1;
     int pos = 0;
     if (R < Rtot) {
-        b = R / nd;
-        pos = (int)(R - b * nd);
+        b = (unsigned)R / und;
+        pos = (int)((unsigned)R - (unsigned)b * und);
         bb = base(b, w);
     }
     const bool valid = bb >= 0;
@@ -1144,16 +1147,17 @@ __device__ __forceinline__ void flux_faces_lines(const StageArgs &A, double *__r
     int f = 0;
     long long s = 0;
     if (face_ok) {
-        const long long b = R / nf;
-        f = (int)(R - b * nf);
+        /* 32-bit index arithmetic, as in flux_lines_block */
+        const unsigned b = (unsigned)R / (unsigned)nf;
+        f = (int)((unsigned)R - b * (unsigned)nf);
         long long base;
         if (DIR == 1) {
-            const long long nyq = (A.ny + W - 1) / W, jq = b % nyq, k = b / nyq;
+            const unsigned nyq = (unsigned)(A.ny + W - 1) / W, k = b / nyq, jq = b - k * nyq;
             const int y = (int)jq * W + w;
             face_ok = y < A.ny;
             base = A.ncx * (y + 2) + sxy * (k + 2);
         } else {
-            const long long xq = b % nxq, o = b / nxq;
+            const unsigned o = b / (unsigned)nxq, xq = b - o * (unsigned)nxq;
             const int x = (int)xq * W + w;
             face_ok = x < A.nx;
             base = (DIR == 2) ? (x + 2) + sxy * (o + 2) : (x + 2) + A.ncx * (o + 2);
