@@ -201,6 +201,9 @@ int vh_event_create(const vh_config *cfg, const double *eos_rows, int eos_nrows,
     if (!cfg || !out) return fail(VH_ERR_ARG, "null argument");
     *out = nullptr;
     if (cfg->nx < 2 || cfg->ny < 2 || cfg->nz < 1) return fail(VH_ERR_ARG, "lattice must be at least 2x2x1");
+    /* the kernels index cells and lines in 32-bit arithmetic */
+    if ((long long)(cfg->nx + 4) * (cfg->ny + 4) * (cfg->nz + 4) >= (1LL << 31))
+        return fail(VH_ERR_ARG, "lattice too large (2^31 padded cells or more)");
     if (!(cfg->dx > 0 && cfg->dy > 0 && cfg->dz > 0 && cfg->dt > 0 && cfg->t0 > 0))
         return fail(VH_ERR_ARG, "spacings and t0 must be positive");
     if (cfg->eos_kind == VH_EOS_TABLE && (!eos_rows || eos_nrows < 2 || eos_nrows > 100000))

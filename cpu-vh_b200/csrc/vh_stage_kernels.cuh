@@ -33,11 +33,12 @@ __device__ __forceinline__ bool stage_cell(const StageArgs &A, int &i, int &j, i
  * lane idles at the end of a row (the per-cell phases need no tile) */
 __device__ __forceinline__ bool stage_cell_flat(const StageArgs &A, int &i, int &j, int &k, long long &s)
 {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long nxy = (long long)A.nx * A.ny;
-    if (c >= nxy * A.nz) return false;
+    /* 32-bit index arithmetic: an event's cell count is far below 2^31 */
+    const unsigned c = blockIdx.x * blockDim.x + threadIdx.x;
+    const unsigned nxy = (unsigned)A.nx * (unsigned)A.ny;
+    if (c >= nxy * (unsigned)A.nz) return false;
     k = (int)(c / nxy);
-    const int r = (int)(c - (long long)k * nxy);
+    const int r = (int)(c - (unsigned)k * nxy);
     j = r / A.nx;
     i = r - j * A.nx + 2;
     j += 2;
