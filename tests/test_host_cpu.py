@@ -38,6 +38,15 @@ def test_event_create_without_device_fails_cleanly():
     assert ei.value.code == 7   # VH_ERR_NODEVICE
 
 
+def test_event_create_rejects_a_lattice_beyond_32_bit_cell_indices():
+    # checked before the device is looked for, so this runs on any host
+    cfg = vh.gubser_config(9, 9)
+    cfg.nx, cfg.ny, cfg.nz = 2000, 2000, 600
+    with pytest.raises(vh.VhError) as ei:
+        vh.Event(cfg)
+    assert ei.value.code == 1   # VH_ERR_ARG
+
+
 class Lat(C.Structure):
     _fields_ = [(n, C.c_int) for n in ("nx", "ny", "nz", "ncx", "ncy", "ncz", "nt", "fo")] + \
                [(n, C.c_double) for n in ("dx", "dy", "dz", "dt", "theta")]
