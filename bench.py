@@ -63,7 +63,7 @@ def phase_words(nq):
 # ncu captures kept in profiles/kt_flux_lines_kernel_glauber_131x131x61.md
 # (FP64: mean of the x, y, eta launches) and
 # profiles/kt_flux_face_kernel_glauber_131x131x61_mixed.md (mixed)
-NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 380.96e6, ("glauber_3p1d", "fp64", "source"): 334.20e6,
+NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 381.57e6, ("glauber_3p1d", "fp64", "source"): 336.57e6,
                ("glauber_3p1d", "mixed", "flux"): 388.30e6, ("glauber_3p1d", "mixed", "source"): 322.01e6}
 
 
@@ -72,7 +72,7 @@ NCU_TRAFFIC = {("glauber_3p1d", "fp64", "flux"): 380.96e6, ("glauber_3p1d", "fp6
 # the launch's duration under ncu (ms) and its FP64-pipe warp instructions.
 # The fraction of the FP64 pipe's peak at live speed is that percentage
 # scaled by the ratio of the durations.
-NCU_FP64 = {("glauber_3p1d", "fp64", "flux"): (26.76, 0.3514, 51.47e6)}
+NCU_FP64 = {("glauber_3p1d", "fp64", "flux"): (27.01, 0.3473, 51.47e6)}
 
 
 # batched flux launches: DRAM bytes per cell from ncu captures of the same
