@@ -159,15 +159,13 @@ __device__ __forceinline__ void face_flux_t(const StageArgs &A, const QTile &qt,
     }
 }
 
-/* dir_sources with q from the tile at ts +- tst and u at the padded cell s */
+/* dir_sources with q from the tile at ts +- tst and u^tau, u^dir of the
+ * padded cell given (dir_sources_t below reads them at s) */
 template <int NQ>
-__device__ __forceinline__ void dir_sources_t(const StageArgs &A, const QTile &qt, int ts, int tst, long long s,
-                                              double d, int dir, double *S)
+__device__ __forceinline__ void dir_sources_uv(const StageArgs &A, const QTile &qt, int ts, int tst, double ut, double v,
+                                               double d, int dir, double *S)
 {
-    const long long L = A.L;
     const double fac = 1 / d / 2;
-    const double ut = __ldg(A.uin + s);
-    const double v = __ldg(A.uin + dir * L + s);
     const double vv = v / ut;
 #define DER(n) ((qt(n, ts + tst) - qt(n, ts - tst)) * fac)
     const double dpitt = DER(4), dpitx = DER(5), dpity = DER(6), dpitn = DER(7);
@@ -191,6 +189,13 @@ __device__ __forceinline__ void dir_sources_t(const StageArgs &A, const QTile &q
         S[2] = dpity * vv - dpiyn;
     }
 #undef DER
+}
+
+template <int NQ>
+__device__ __forceinline__ void dir_sources_t(const StageArgs &A, const QTile &qt, int ts, int tst, long long s,
+                                              double d, int dir, double *S)
+{
+    dir_sources_uv<NQ>(A, qt, ts, tst, __ldg(A.uin + s), __ldg(A.uin + dir * A.L + s), d, dir, S);
 }
 
 /* copy 8 bytes global -> shared without staging through registers */
@@ -489,10 +494,9 @@ __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__r
     }
     const bool valid = bb >= 0;
     const long long s = valid ? bb + (long long)(pos + 2) * gst : 0;
-    if (valid) {
-        prefetch_flux_cell<NQ>(A, s, DIR);
-        prefetch_l2(A.ein + s);
-    }
+    if (valid) prefetch_flux_cell<NQ>(A, s, DIR);
+    /* the root solves' start, read while the stencil is staged */
+    const double ePrev = valid ? __ldg(A.ein + s) : 0.0;
     /* staging: slot l covers positions [first_l - 2, first_l + len_l + 2) of
      * bundle b0 + l at shared indices [M_l, M_l + len_l + 4) */
     const int mlen_max = PS / W;
@@ -533,7 +537,6 @@ __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__r
     const int ts = ((int)(R - R0) + 2 + 4 * (int)(b - b0)) * W + w;
     constexpr int tst = W;
     const QTile qt{sm, PS};
-    const double ePrev = __ldg(A.ein + s);
     bool bad = false;
     /* states m = 0..3: forward face R, L; backward face R, L */
     double ut0 = 0, ut1 = 0, ut2 = 0, ut3 = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0;
@@ -557,13 +560,15 @@ __device__ __forceinline__ void flux_lines_block(const StageArgs &A, double *__r
         else if (mm == 2) { ut2 = Pm.ut; v2 = vm; }
         else { ut3 = Pm.ut; v3 = vm; }
     }
+    /* u of the direction sources, read while the reciprocals run */
+    const double uts = __ldg(A.uin + s), uds = __ldg(A.uin + DIR * A.L + s);
     const double y0 = 1.0 / ut0, y1 = 1.0 / ut1, y2 = 1.0 / ut2, y3 = 1.0 / ut3;
     const double af = fmax(fabs(div_rcp(v1, ut1, y1)), fabs(div_rcp(v0, ut0, y0)));
     const double ab = fmax(fabs(div_rcp(v3, ut3, y3)), fabs(div_rcp(v2, ut2, y2)));
     const double d = (DIR == 1) ? A.dx : (DIR == 2) ? A.dy : A.dz;
     const double yd = (DIR == 1) ? A.inv_dx : (DIR == 2) ? A.inv_dy : A.inv_dz;
     double S[4];
-    dir_sources_t<NQ>(A, qt, ts, tst, s, d, DIR, S);
+    dir_sources_uv<NQ>(A, qt, ts, tst, uts, uds, d, DIR, S);
     if (PDL) pdl_wait();
 #pragma unroll UNR
     for (int n = 0; n < NQ; ++n) {
